@@ -1,0 +1,204 @@
+// Oracle harness: drives the reference ZLLBM solver through its own public API
+// (the same calls examples/lbm/immersed_boundary/cylinder2d/cylinder2d.cpp:14-111
+// makes) on a single uniform level, and dumps every node's populations so the
+// CUDA path can be compared node by node.  Test infrastructure only.
+//
+// usage: zl_ref_run key=value ...
+//   dims=2|3  n=NX,NY[,NZ] (domain size in cells, dx = 1)  steps=K
+//   coll=srt|mrt  nu=<lattice viscosity>  les=0|1
+//   bc=<face>:<bb|per|neq>[:ux,uy[,uz]]  (repeatable; faces xmin xmax ymin ymax zmin zmax)
+//   init=eq|tgv  u0=<TGV amplitude>  rho0=<default density>  vel=ux,uy[,uz] (initial uniform)
+//   out0=<file>  out=<file>  (binary dumps before and after stepping; optional)
+//   timing=1 (print wall-clock seconds of the TimeMarching loop)
+//
+// Dump format (little endian): int32 dims, int32 q, int64 n, then n records of
+// uint64 morton code, int32 flag, int32 pad, double f[q]; records sorted by code.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <string>
+#include <vector>
+#include "./amr_manager.h"
+#include "d2q9_model/lbm_d2q9.h"
+#include "d3q19_model/lbm_d3q19.h"
+
+using namespace rootproject;
+using amrproject::EDomainBoundaryDirection;
+using lbmproject::ELbmBoundaryConditionScheme;
+
+namespace {
+std::vector<double> parse_list(const std::string& s) {
+    std::vector<double> v;
+    std::stringstream ss(s);
+    std::string tok;
+    while (std::getline(ss, tok, ',')) v.push_back(std::atof(tok.c_str()));
+    return v;
+}
+
+struct FaceBc {
+    EDomainBoundaryDirection dir;
+    ELbmBoundaryConditionScheme kind;
+    std::vector<double> vel;
+};
+
+EDomainBoundaryDirection face_of(const std::string& f) {
+    if (f == "xmin") return EDomainBoundaryDirection::kBoundaryXMin;
+    if (f == "xmax") return EDomainBoundaryDirection::kBoundaryXMax;
+    if (f == "ymin") return EDomainBoundaryDirection::kBoundaryYMin;
+    if (f == "ymax") return EDomainBoundaryDirection::kBoundaryYMax;
+    if (f == "zmin") return EDomainBoundaryDirection::kBoundaryZMin;
+    if (f == "zmax") return EDomainBoundaryDirection::kBoundaryZMax;
+    std::fprintf(stderr, "unknown face %s\n", f.c_str());
+    std::exit(2);
+}
+
+ELbmBoundaryConditionScheme kind_of(const std::string& k) {
+    if (k == "bb") return ELbmBoundaryConditionScheme::kBounceBack;
+    if (k == "per") return ELbmBoundaryConditionScheme::kPeriodic;
+    if (k == "neq") return ELbmBoundaryConditionScheme::kNonEqExtrapolation;
+    std::fprintf(stderr, "unknown bc kind %s\n", k.c_str());
+    std::exit(2);
+}
+
+void dump(const std::string& path, int dims, int q, amrproject::GridInfoInterface& grid) {
+    auto& nodes = *dynamic_cast<lbmproject::GridInfoLbmInteface&>(grid).GetPtrToLbmGrid();
+    std::vector<std::pair<uint64_t, lbmproject::GridNodeLbm*>> order;
+    order.reserve(nodes.size());
+    for (auto& it : nodes) order.emplace_back(it.first.to_ullong(), it.second.get());
+    std::sort(order.begin(), order.end(),
+              [](const auto& a, const auto& b) { return a.first < b.first; });
+    FILE* fp = std::fopen(path.c_str(), "wb");
+    if (!fp) { std::perror(path.c_str()); std::exit(3); }
+    int32_t hdr[2] = {dims, q};
+    int64_t n = static_cast<int64_t>(order.size());
+    std::fwrite(hdr, sizeof(hdr), 1, fp);
+    std::fwrite(&n, sizeof(n), 1, fp);
+    for (auto& [code, node] : order) {
+        int32_t fl[2] = {node->flag_status_, 0};
+        std::fwrite(&code, sizeof(code), 1, fp);
+        std::fwrite(fl, sizeof(fl), 1, fp);
+        std::fwrite(node->f_.data(), sizeof(double), q, fp);
+    }
+    std::fclose(fp);
+}
+}  // namespace
+
+int main(int argc, char* argv[]) {
+    std::map<std::string, std::string> kv;
+    std::vector<FaceBc> bcs;
+    for (int i = 1; i < argc; ++i) {
+        std::string a(argv[i]);
+        auto eq = a.find('=');
+        if (eq == std::string::npos) continue;
+        std::string k = a.substr(0, eq), v = a.substr(eq + 1);
+        if (k == "bc") {
+            std::stringstream ss(v);
+            std::string face, kind, vel;
+            std::getline(ss, face, ':');
+            std::getline(ss, kind, ':');
+            std::getline(ss, vel, ':');
+            bcs.push_back({face_of(face), kind_of(kind), vel.empty() ? std::vector<double>{} : parse_list(vel)});
+        } else {
+            kv[k] = v;
+        }
+    }
+    const int dims = kv.count("dims") ? std::atoi(kv["dims"].c_str()) : 2;
+    const std::vector<double> n = parse_list(kv.count("n") ? kv["n"] : "16,16,16");
+    const int steps = kv.count("steps") ? std::atoi(kv["steps"].c_str()) : 1;
+    const std::string coll = kv.count("coll") ? kv["coll"] : "srt";
+    const double nu = kv.count("nu") ? std::atof(kv["nu"].c_str()) : 0.1;
+    const double rho0 = kv.count("rho0") ? std::atof(kv["rho0"].c_str()) : 1.0;
+    const std::string init = kv.count("init") ? kv["init"] : "eq";
+    const double u0 = kv.count("u0") ? std::atof(kv["u0"].c_str()) : 0.05;
+    std::vector<double> vel0 = kv.count("vel") ? parse_list(kv["vel"]) : std::vector<double>(dims, 0.);
+    vel0.resize(dims, 0.);
+
+    amrproject::AmrManager* amr = amrproject::AmrManager::GetInstance();
+    amr->StartupAmrManager(argc, argv);
+    amr->StartupInitialization(dims);
+    amr->ptr_grid_manager_->SetMaxLevel(0);
+    amr->program_name_ = "zl_ref_run";
+    std::vector<double> domain(n.begin(), n.begin() + dims);
+    amr->ptr_grid_manager_->SetDomainSize(domain);
+    amr->ptr_grid_manager_->SetDomainGridSize({1.});
+    amr->SetupInputDependentParameters();
+    lbmproject::SolverCreatorLbmD2Q9 c2;
+    lbmproject::SolverCreatorLbmD3Q19 c3;
+    if (dims == 2) {
+        amr->AddSolverToGridManager(c2);
+    } else {
+        amr->AddSolverToGridManager(c3);
+    }
+    amr->SetSameSolverDependentInfoForAllGrids(amr->ptr_grid_manager_->vec_ptr_solver_.at(0));
+    auto& solver = *dynamic_cast<lbmproject::SolverLbmInterface*>(
+        amr->ptr_grid_manager_->vec_ptr_solver_.at(0).get());
+    for (auto& g : amr->ptr_grid_manager_->vec_ptr_grid_info_) {
+        auto& grid = *dynamic_cast<lbmproject::GridInfoLbmInteface*>(g.get());
+        solver.SetCollisionOperator(grid.GetGridLevel(), coll == "mrt"
+            ? lbmproject::ELbmCollisionOperatorType::kLbmMrt : lbmproject::ELbmCollisionOperatorType::kLbmSrt);
+        for (auto& bc : bcs) {
+            solver.SetDomainBoundaryCondition(bc.dir, bc.kind, &grid.domain_boundary_condition_);
+            std::vector<double> v = bc.vel;
+            v.resize(dims, 0.);
+            grid.domain_boundary_condition_.at(bc.dir)->SetValues(v);
+        }
+    }
+    if (kv.count("les") && kv["les"] == "1") solver.SetLesModel(lbmproject::ELbmLesModelType::kSmagorinsky);
+    solver.SetDefaultViscosity(nu);
+    solver.SetDefaultDensity(rho0);
+    solver.SetDefaultVelocity(vel0);
+    amr->InitializeAllSolvers();
+    amr->SetupMesh(0);
+
+    auto& grid0 = *amr->ptr_grid_manager_->vec_ptr_grid_info_.at(0);
+    const int q = solver.k0NumQ_;
+    if (init == "tgv") {
+        // Taylor-Green vortex written into the public node members after SetupMesh.
+        auto& nodes = *dynamic_cast<lbmproject::GridInfoLbmInteface&>(grid0).GetPtrToLbmGrid();
+        auto* aux3 = dynamic_cast<amrproject::SFBitsetAux3D*>(amr->ptr_grid_manager_.get());
+        auto* aux2 = dynamic_cast<amrproject::SFBitsetAux2D*>(amr->ptr_grid_manager_.get());
+        const double two_pi = 2. * std::acos(-1.);
+        for (auto& it : nodes) {
+            double x, y, z = 0.;
+            if (dims == 3) {
+                std::array<DefAmrLUint, 3> idx;
+                aux3->SFBitsetComputeIndices(it.first, &idx);
+                x = two_pi * (idx[0] - 1) / n[0];
+                y = two_pi * (idx[1] - 1) / n[1];
+                z = two_pi * (idx[2] - 1) / n[2];
+            } else {
+                std::array<DefAmrLUint, 2> idx;
+                aux2->SFBitsetComputeIndices(it.first, &idx);
+                x = two_pi * (idx[0] - 1) / n[0];
+                y = two_pi * (idx[1] - 1) / n[1];
+            }
+            std::vector<double> u(dims);
+            u[0] = u0 * std::sin(x) * std::cos(y) * std::cos(z);
+            u[1] = -u0 * std::cos(x) * std::sin(y) * std::cos(z);
+            if (dims == 3) u[2] = 0.;
+            const double p = (dims == 3)
+                ? rho0 * u0 * u0 / 16. * (std::cos(2. * x) + std::cos(2. * y)) * (std::cos(2. * z) + 2.)
+                : rho0 * u0 * u0 / 4. * (std::cos(2. * x) + std::cos(2. * y));
+            const double rho = rho0 + 3. * p;
+            solver.func_cal_feq_(rho, u, &it.second->f_);
+            it.second->f_collide_ = it.second->f_;
+            it.second->rho_ = rho;
+            it.second->velocity_ = u;
+        }
+    }
+    if (kv.count("out0")) dump(kv["out0"], dims, q, grid0);
+    auto t0 = std::chrono::steady_clock::now();
+    for (int it = 0; it < steps; ++it) amr->TimeMarching(it);
+    auto t1 = std::chrono::steady_clock::now();
+    if (kv.count("out")) dump(kv["out"], dims, q, grid0);
+    if (kv.count("timing")) {
+        const double sec = std::chrono::duration<double>(t1 - t0).count();
+        std::printf("{\"nodes\": %zu, \"steps\": %d, \"seconds\": %.6f}\n", grid0.map_grid_node_.size(), steps, sec);
+    }
+    return 0;
+}
