@@ -1,0 +1,395 @@
+"""Benchmark: D3Q19 MRT Taylor-Green vortex on a periodic 256^3 lattice, one LBM time step per step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--storage f32|f16|bf16|f64] [--impl ours|reference]
+
+Prints one JSON line (rank 0).  ``value`` is whole-job MLUPS over all ranks with the
+populations resident in HBM; ``e2e`` is the same job through the C ABI with host buffers:
+upload of the initial populations from pinned memory, K steps, read-back of density and
+velocity, all inside the timed region.  The lattice (256^3 nodes, 2.55 GB of FP32
+populations) is far larger than L2, so no flush is needed between steps.
+
+Multi-GPU runs are independent replicas (one lattice per rank, no data-path
+collective); ranks only meet at the timing barriers.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "D3Q19 MLUPS & HBM-roofline %; learned vs Smagorinsky LES error at same GPU"
+CELLS = 256          # unique nodes per axis (periodic; the reference stores 257 planes)
+U0 = 0.05
+TAU = 0.55
+NU = (TAU - 0.5) / 3.0
+STORAGE_BYTES = {"f64": 8, "f32": 4, "f16": 2, "bf16": 2}
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ---------------------------------------------------------------- helpers
+def tgv_nodes(cells: int):
+    """Morton codes of the reference's stored nodes (indices 1..cells+1) and TGV feq populations."""
+    import zllbm_b200 as zl
+    n = cells + 1
+    codes = zl.box_codes(3, (1, 1, 1), (n, n, n))
+    ax = 2.0 * np.pi * (np.arange(n) % cells) / cells
+    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    x, y, z = x.ravel(), y.ravel(), z.ravel()
+    ux = U0 * np.sin(x) * np.cos(y) * np.cos(z)
+    uy = -U0 * np.cos(x) * np.sin(y) * np.cos(z)
+    p = U0 * U0 / 16.0 * (np.cos(2 * x) + np.cos(2 * y)) * (np.cos(2 * z) + 2.0)
+    rho = 1.0 + 3.0 * p
+    del x, y, z
+    c = np.array([(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (1, 1, 0),
+                  (-1, 1, 0), (1, -1, 0), (-1, -1, 0), (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1), (0, 1, 1),
+                  (0, -1, 1), (0, 1, -1), (0, -1, -1)], dtype=np.float64)
+    w = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    f = np.empty((codes.size, 19))
+    usq = ux * ux + uy * uy
+    for q in range(19):
+        cu = ux * c[q, 0] + uy * c[q, 1]
+        f[:, q] = w[q] * rho * (1.0 + 3.0 * cu + 4.5 * cu * cu - 1.5 * usq)
+    return codes, f
+
+
+def solver_config(storage: int, device: int):
+    import zllbm_b200 as zl
+    n = CELLS + 1
+    return zl.SolverConfig(lattice=zl.D3Q19, collision=zl.MRT, storage=storage, viscosity=NU, rho0=1.0,
+                           bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(1, 1, 1), domain_max=(n, n, n), device=device)
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(storage: str):
+    """DRAM bytes per launch of the step kernel from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(storage)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        exe = shutil.which("nvidia-smi")
+        if exe:
+            self.proc = subprocess.Popen([exe, f"--id={self.device}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+            time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            time.sleep(0.15)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- distributed plumbing
+def dist_init(gpus: int):
+    if gpus <= 1 or "RANK" not in os.environ:
+        return 0, 1, int(os.environ.get("LOCAL_RANK", 0)), None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    local = int(os.environ.get("LOCAL_RANK", 0))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return dist.get_rank(), dist.get_world_size(), local, dist
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def max_over_ranks(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------- CPU baselines
+def reference_run(cells: int, steps: int, warmup: int, workdir: str):
+    exe = os.path.join(ROOT, "oracle", "_ref", "zl_ref_run")
+    args = [exe, "dims=3", f"n={cells},{cells},{cells}", f"steps={steps}", f"warmup={warmup}", "coll=mrt",
+            f"nu={NU!r}", "init=tgv", f"u0={U0!r}", "timing=1"] + \
+           [f"bc={f}:per" for f in ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")]
+    return subprocess.Popen(args, cwd=workdir, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+
+
+def cpu_baseline_sample(processes: int = 1, cells: int = 48, steps: int = 30, warmup: int = 2):
+    """Time the reference ZLLBM solver (oracle/_ref, built from its own sources) on a TGV
+    subdomain of the same workload; `processes` independent single-rank runs model its MPI
+    scaling across the host cores.  Falls back to the C restatement when the binary is absent."""
+    import tempfile
+    exe = os.path.join(ROOT, "oracle", "_ref", "zl_ref_run")
+    nodes = (cells + 1) ** 3
+    if os.path.exists(exe):
+        with tempfile.TemporaryDirectory() as tmp:
+            dirs = []
+            for i in range(processes):
+                d = os.path.join(tmp, str(i))
+                os.makedirs(d)
+                dirs.append(d)
+            procs = [reference_run(cells, steps, warmup, d) for d in dirs]
+            secs = []
+            for p in procs:
+                out, _ = p.communicate(timeout=1800)
+                if p.returncode != 0:
+                    raise RuntimeError("reference harness failed")
+                secs.append(json.loads(out.strip().splitlines()[-1])["seconds"])
+        wall = max(secs)
+        mlups = processes * nodes * steps / wall / 1e6
+        return {"value": mlups, "unit": "MLUPS", "cores": processes, "kind": "reference",
+                "sample": f"reference ZLLBM TimeMarching, D3Q19 MRT TGV periodic {cells}^3 "
+                          f"({nodes} stored nodes) x {steps} steps after {warmup} warm-up, "
+                          f"{processes} single-rank process(es), max wall {wall:.2f} s"}
+    from oracle.port import MRT, BC_PERIODIC, LevelConfig, Port, tgv_init
+    port = Port()
+    cfg = LevelConfig(dims=3, n=(cells + 1,) * 3, collision=MRT, nu=NU, bc_kind=(BC_PERIODIC,) * 6)
+    f = tgv_init(cfg, U0, port).reshape(-1, 19)
+    fc = f.copy()
+    port.run(cfg, f, fc, warmup)
+    t0 = time.perf_counter()
+    port.run(cfg, f, fc, steps)
+    wall = time.perf_counter() - t0
+    return {"value": nodes * steps / wall / 1e6, "unit": "MLUPS", "cores": 1, "kind": "port",
+            "sample": f"C restatement of the reference step, TGV {cells}^3 x {steps} steps, {wall:.2f} s"}
+
+
+def run_reference_arm(args):
+    rank = int(os.environ.get("RANK", 0))
+    if rank != 0:
+        return 0
+    procs = max(1, min(os.cpu_count() or 1, 64))
+    # bound the sample: about a minute of CPU work per process for K timed steps
+    budget_lups = 60.0 * 0.8e6
+    cells = int(max(16, min(64, round((budget_lups / max(args.steps, 1)) ** (1 / 3)) - 1)))
+    cb = cpu_baseline_sample(processes=procs, cells=cells, steps=args.steps, warmup=args.warmup)
+    out = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": "MLUPS", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "config": {"workload": "D3Q19 MRT Taylor-Green vortex, periodic, u0=0.05, tau=0.55 (sampled subdomain "
+                                  f"{cells}^3 per process on the host cores)", "parallelism": f"{procs} processes"},
+           "cpu_baseline": cb,
+           "e2e": {"value": cb["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- GPU arm
+def time_steps(ctx, steps: int):
+    """Device time of `steps` calls of zl_step_level on the context's stream (CUDA events)."""
+    import torch
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    ctx.synchronize()
+    start.record(stream)
+    for _ in range(steps):
+        ctx.step_level(0)
+    end.record(stream)
+    end.synchronize()
+    return start.elapsed_time(end)
+
+
+def run_ours(args):
+    import torch
+
+    import zllbm_b200 as zl
+    rank, world, local, dist = dist_init(args.gpus)
+    torch.cuda.set_device(local)
+    storage = zl.STORAGE_NAMES[args.storage]
+    elem = STORAGE_BYTES[args.storage]
+    codes, f0 = tgv_nodes(CELLS)
+    nodes = CELLS ** 3
+    alg_bytes = nodes * 2 * 19 * elem  # read + write every population once per update
+
+    ctx = zl.Context(solver_config(storage, local))
+    ctx.set_level_nodes(0, codes)
+    ctx.set_populations(0, codes, f0)
+    for _ in range(args.warmup):
+        ctx.step_level(0)
+    ctx.synchronize()
+
+    barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        ms = time_steps(ctx, args.steps)
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms = max_over_ranks(dist, ms)
+    mass = ctx.conservation(0)[0]
+
+    ms_per_step = ms / args.steps
+    value = world * nodes * args.steps / (ms / 1e3) / 1e6
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    traffic = committed_traffic(args.storage)
+
+    # other storage precisions of the same workload, kernel time only (reported alongside)
+    variants = {}
+    if args.variants and rank == 0:
+        for name in ("f16", "bf16", "f32"):
+            if name == args.storage:
+                continue
+            with zl.Context(solver_config(zl.STORAGE_NAMES[name], local)) as c2:
+                c2.set_level_nodes(0, codes)
+                c2.set_populations(0, codes, f0)
+                for _ in range(args.warmup):
+                    c2.step_level(0)
+                vms = time_steps(c2, args.steps)
+                b = nodes * 2 * 19 * STORAGE_BYTES[name]
+                variants[name] = {"mlups": nodes * args.steps / (vms / 1e3) / 1e6,
+                                  "ms_per_step": vms / args.steps,
+                                  "hbm_gbs": b / (vms / args.steps / 1e3) / 1e9,
+                                  "frac": b / (vms / args.steps / 1e3) / 1e9 / peak}
+    # end to end through the C ABI with host buffers
+    e2e = None
+    if not args.no_e2e:
+        codes_h = torch.from_numpy(codes).pin_memory()
+        f_h = torch.from_numpy(f0).pin_memory()
+        rho_h = torch.empty(codes.size, dtype=torch.float64).pin_memory()
+        u_h = torch.empty((codes.size, 3), dtype=torch.float64).pin_memory()
+        lib = ctx.lib
+        import ctypes
+        u64p, dp = ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)
+        cp = ctypes.cast(codes_h.data_ptr(), u64p)
+        barrier(dist)
+        ctx.synchronize()
+        t0 = time.perf_counter()
+        ctx._check(lib.zl_set_populations(ctx.handle, 0, cp, ctypes.cast(f_h.data_ptr(), dp), codes.size))
+        for _ in range(args.steps):
+            ctx._check(lib.zl_step_level(ctx.handle, 0))
+        ctx._check(lib.zl_get_macros(ctx.handle, 0, cp, ctypes.cast(rho_h.data_ptr(), dp),
+                                     ctypes.cast(u_h.data_ptr(), dp), codes.size))
+        ctx.synchronize()
+        t_e2e = max_over_ranks(dist, time.perf_counter() - t0)
+        h2d = codes.nbytes * 2 + f0.nbytes
+        d2h = rho_h.numel() * 8 + u_h.numel() * 8
+        e2e = {"value": world * nodes * args.steps / t_e2e / 1e6, "unit": "MLUPS",
+               "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
+               "seconds": t_e2e,
+               "includes": "H2D of codes + initial populations (pinned), K steps, D2H of rho and u"}
+    ctx.close()
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_sample(processes=1)
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": f"D3Q19 MRT Taylor-Green vortex, periodic {CELLS}^3 "
+                                   f"(reference stores {CELLS + 1}^3), u0={U0}, tau={TAU}, "
+                                   f"{args.storage} population storage, FP32 collision"
+                                   if args.storage != "f64" else "FP64 collision",
+                       "nodes_per_gpu": nodes, "storage": args.storage, "collision": "MRT",
+                       "l2": f"inputs larger than L2 ({alg_bytes / 2 / 1e9:.2f} GB of populations)",
+                       "parallelism": f"{world} independent replica(s)" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
+                         "kernel": "aa_step_kernel<D3Q19, MRT>"},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": args.steps,
+            "clocks": clocks.summary(),
+            "mass_after": mass,
+        }
+        if variants:
+            out["storage_variants"] = variants
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_BYTES))
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--variants", type=int, default=1)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

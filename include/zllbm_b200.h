@@ -1,0 +1,180 @@
+/*
+ * zllbm_b200 — C ABI of the B200 lattice-Boltzmann time step.
+ *
+ * The library replaces, for one GPU, the per-level time step of the
+ * reference ZLLBM LBM plugin: GridInfoLbmInteface::AdvancingAtCurrentTime
+ * (lbm_project/lbm_grid_interface.cpp:104-153), which collides every node,
+ * pull-streams it through Morton-code hash lookups, applies the domain
+ * boundary conditions and exchanges coarse/fine information.  A host
+ * (the reference's AmrManager / GridManager, or any other caller) keeps
+ * owning the Morton-coded node sets; it hands each level's codes over once,
+ * then calls zl_step_level (or zl_advance) where the reference called
+ * AdvancingAtCurrentTime.
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Arrays passed in are copied; the caller
+ *    keeps ownership.  Pointers are HOST pointers unless a name says _device.
+ *  - Populations use the reference's direction order (d2q9_model/lbm_d2q9.h:53-61,
+ *    d3q19_model/lbm_d3q19.h:18-85) and are exchanged in the order of the
+ *    Morton codes the caller passes, q fastest (node-major, like GridNodeLbm::f_).
+ *  - Every call returns 0 on success or a negative ZL_E* code; zl_last_error
+ *    gives the message.  This replaces the reference's LogError + MPI_Abort
+ *    (amr_project/io/log_write.cpp:143-182): a C++ wrapper maps a non-zero
+ *    return to LogManager::LogError to keep the reference's behaviour.
+ *  - One host thread per context; all work is ordered on the context's own
+ *    CUDA stream.  No global mutable state is shared between contexts.
+ */
+#ifndef ZLLBM_B200_H_
+#define ZLLBM_B200_H_
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ZL_ABI_VERSION 1
+#define ZL_MAX_LEVELS 8
+
+/* error codes */
+#define ZL_OK 0
+#define ZL_EINVAL (-1)     /* bad argument */
+#define ZL_ETOPOLOGY (-2)  /* node codes inconsistent with the level / domain */
+#define ZL_EDEVICE (-3)    /* CUDA error */
+#define ZL_ETIMEOUT (-4)   /* a bounded device wait gave up */
+#define ZL_ENAN (-5)       /* non-finite populations detected */
+#define ZL_ESTATE (-6)     /* call out of order (e.g. stepping a level with no nodes) */
+
+/* lattice (SolverCreatorLbmD2Q9 / SolverCreatorLbmD3Q19, lbm_d2q9_mandatory.cpp:19-23,
+   lbm_d3q19_mandatory.cpp:20-24) */
+#define ZL_D2Q9 2
+#define ZL_D3Q19 3
+
+/* collision operators (ELbmCollisionOperatorType, collision_model/lbm_collision_models.h:21-25) */
+#define ZL_SRT 0
+#define ZL_MRT 1
+
+/* domain boundary conditions (ELbmBoundaryConditionScheme,
+   boundary_conditions/lbm_boundary_conditions.h:22-27) */
+#define ZL_BC_NONE 0
+#define ZL_BC_BOUNCE_BACK 1
+#define ZL_BC_PERIODIC 2
+#define ZL_BC_NONEQ_EXTRAPOLATION 3
+
+/* face slots (EDomainBoundaryDirection, amr_project/grid/grid_enumerates.h) */
+#define ZL_FACE_XMIN 0
+#define ZL_FACE_XMAX 1
+#define ZL_FACE_YMIN 2
+#define ZL_FACE_YMAX 3
+#define ZL_FACE_ZMIN 4
+#define ZL_FACE_ZMAX 5
+
+/* population storage in device memory */
+#define ZL_STORAGE_F64 0  /* raw f in FP64, reference arithmetic order: bit-exact parity mode */
+#define ZL_STORAGE_F32 1  /* f - w in FP32, FP32 collision */
+#define ZL_STORAGE_F16 2  /* (f - w) * scale in FP16, FP32 collision */
+#define ZL_STORAGE_BF16 3 /* (f - w) * scale in BF16, FP32 collision */
+
+/* Solver and domain settings: the values a reference application sets through
+   SolverLbmInterface::SetCollisionOperator / SetDomainBoundaryCondition + SetValues /
+   SetDefaultViscosity / SetDefaultDensity (lbm_project/lbm_interface.h:298-319,452-465)
+   and GridManagerInterface::SetDomainSize / SetMaxLevel (amr_project/grid/grid_manager.h:117-129). */
+typedef struct zl_config {
+    int lattice;               /* ZL_D2Q9 or ZL_D3Q19 */
+    int collision;             /* ZL_SRT or ZL_MRT */
+    int storage;               /* ZL_STORAGE_* */
+    int max_level;             /* finest refinement level, < ZL_MAX_LEVELS */
+    double viscosity;          /* lattice viscosity at the background level (tau_l = 3 nu 2^l + 0.5) */
+    double rho0;               /* default density */
+    int bc_kind[6];            /* ZL_BC_* per face slot */
+    double bc_velocity[6][3];  /* wall / boundary velocity per face slot */
+    int32_t domain_min[3];     /* background index range of the domain (the reference starts at 1) */
+    int32_t domain_max[3];
+    double init_velocity[3];   /* default velocity: nodes start at feq(rho0, init_velocity)
+                                  (SetDefaultVelocity, lbm_interface.h:300) */
+    double storage_scale;      /* scale of FP16/BF16 deviations (0 selects the default 2^13) */
+    int device;                /* CUDA device ordinal */
+} zl_config;
+
+typedef struct zl_ctx zl_ctx;
+
+/* Create a context on config->device.  Replaces SolverCreatorLbm*::CreateSolver plus
+   SolverLbmInterface::SolverInitial (lbm_solver_interface.cpp:19-44). */
+int zl_create(const zl_config* config, zl_ctx** out);
+
+/* Release every device allocation of the context. */
+int zl_destroy(zl_ctx* ctx);
+
+/* Hand over the node set of one refinement level: the Morton codes of
+   GridInfoInterface::map_grid_node_ (amr_project/grid/grid_info_interface.h:258), in any
+   order.  Codes are decoded and the level's dense device box, presence mask and per-node
+   boundary / missing-neighbour flags are built on the device.  Populations start at
+   feq(rho0, 0), as GridInfoLbmInteface::InitialGridInfo does (lbm_grid_interface.cpp:176-191). */
+int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n);
+
+/* Write / read the post-stream populations f_ (GridNodeLbm::f_, lbm_interface.h:37) of the
+   nodes with the given codes; f holds n * q doubles, node-major.  On periodic axes the
+   reference stores the maximum plane as a duplicate of the minimum plane
+   (grid/grid_manager3d.cpp:106-112); both codes address the same device node. */
+int zl_set_populations(zl_ctx* ctx, int level, const uint64_t* codes, const double* f, int64_t n);
+int zl_get_populations(zl_ctx* ctx, int level, const uint64_t* codes, double* f, int64_t n);
+
+/* Density and velocity recomputed from f_ like the reference's output variables
+   (lbm_grid_interface.cpp:614-657): rho[n], u[n * dims]. */
+int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, double* u, int64_t n);
+
+/* One time step of one level: collide, stream, domain boundary conditions.
+   Replaces GridInfoLbmInteface::AdvancingAtCurrentTime (lbm_grid_interface.cpp:104-153)
+   for a level without coarse/fine neighbours. */
+int zl_step_level(zl_ctx* ctx, int level);
+
+/* n background steps of every level, in the reference's sub-cycled order
+   (AmrManager::TimeMarching, amr_manager.cpp:279-300). */
+int zl_advance(zl_ctx* ctx, int steps);
+
+/* Sum over a level's nodes of rho and rho*u, accumulated in FP64 on the device:
+   out[0] = mass, out[1..dims] = momentum.  Non-finite sums return ZL_ENAN. */
+int zl_conservation(zl_ctx* ctx, int level, double* out);
+
+/* Wait for all work of the context. */
+int zl_synchronize(zl_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that time or order work around it. */
+int zl_get_stream(const zl_ctx* ctx, void** stream);
+
+/* Make the context issue its work on a caller-owned cudaStream_t (NULL restores its own stream).
+   The caller keeps the stream alive while the context uses it. */
+int zl_set_stream(zl_ctx* ctx, void* stream);
+
+/* Copy the last error message (NUL-terminated, truncated to n bytes). */
+int zl_last_error(const zl_ctx* ctx, char* buf, size_t n);
+
+/* Number of nodes, box extents (x, y, z) and bytes of population storage of a level. */
+int zl_level_info(const zl_ctx* ctx, int level, int64_t* nodes, int32_t* extent, int64_t* pop_bytes);
+
+/* ---- topology helpers (device Morton arithmetic, bit-exact with the reference) ---- */
+
+/* For each code, the six (2D: four) axis neighbours computed on the device with the
+   reference's FindXNeg/FindXPos/... (amr_project/grid/morton_aux.hpp:65-297), including
+   its rule that a Neg step at a zero axis field returns the input code.  out holds
+   n * 2 * dims codes ordered xneg, xpos, yneg, ypos[, zneg, zpos]. */
+int zl_morton_neighbors(int dims, const uint64_t* codes, int64_t n, uint64_t* out);
+
+/* For each node i of a code set and each direction q, the position in `codes` of the
+   upstream node x - c_q the reference's stream pulls from
+   (d3q19_model/lbm_d3q19_solver.cpp:20-136, d2q9_model/lbm_d2q9_solver.cpp:21-82), or -1
+   when it is not in the set (the reference then keeps the stale value).  Resolved on the
+   device by Morton neighbour arithmetic and binary search; out holds n * q int64. */
+int zl_upstream_index(int lattice, const uint64_t* codes, int64_t n, int64_t* out);
+
+/* The MRT collision matrix M^-1 S M for relaxation time tau, built in the reference's loop
+   order (collision_model/lbm_collision_model_mrt.cpp:63-82); out holds q * q doubles. */
+int zl_mrt_matrix(int lattice, double tau, double* out);
+
+/* ABI version of the loaded library. */
+int zl_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ZLLBM_B200_H_ */

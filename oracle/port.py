@@ -218,7 +218,8 @@ def tgv_init(cfg: LevelConfig, u0: float, port: Port | None = None) -> np.ndarra
     """Taylor-Green initial populations on the stored nodes (x = 2*pi*i/cells), feq from the oracle."""
     port = port or Port()
     cells = [v - 1 for v in cfg.n[: cfg.dims]]
-    axes = [2.0 * np.pi * np.arange(v) / c for v, c in zip(cfg.n[: cfg.dims], cells)]
+    # coordinates modulo the period: the duplicated max plane starts identical to the min plane
+    axes = [2.0 * np.pi * (np.arange(v) % c) / c for v, c in zip(cfg.n[: cfg.dims], cells)]
     if cfg.dims == 3:
         z, y, x = np.meshgrid(axes[2], axes[1], axes[0], indexing="ij")
         ux = u0 * np.sin(x) * np.cos(y) * np.cos(z)
@@ -250,3 +251,63 @@ def run_reference(cfg: LevelConfig, steps: int, workdir: str, init: str = "eq", 
                                              f"out0={out0}", f"out={out1}"] + (extra or [])
     subprocess.run(args, check=True, cwd=workdir, stdout=subprocess.DEVNULL)
     return load_dump(out0)[2], load_dump(out1)[2]
+
+
+# ---- Morton neighbour arithmetic (restates amr_project/grid/morton_aux.hpp:65-297) ----
+def _axis_mask(dims: int, axis: int) -> int:
+    nb = 64 // dims
+    m = 0
+    for i in range(nb):
+        m |= 1 << (dims * i + axis)
+    return m
+
+
+def morton_neg(code: int, dims: int, axis: int) -> int:
+    """FindXNeg/FindYNeg/FindZNeg: returns the input when the axis field is zero."""
+    mk = _axis_mask(dims, axis)
+    others = 0
+    for a in range(dims):
+        if a != axis:
+            others |= _axis_mask(dims, a)
+    v = code & mk
+    if v == 0:
+        return code
+    return ((v - 1) & mk) | (code & others)
+
+
+def morton_pos(code: int, dims: int, axis: int) -> int:
+    """FindXPos/FindYPos/FindZPos: carry through the other axes' bits, wrap at 64 bits."""
+    mk = _axis_mask(dims, axis)
+    others = 0
+    for a in range(dims):
+        if a != axis:
+            others |= _axis_mask(dims, a)
+    t = ((code | (~mk & (2**64 - 1))) + 1) & (2**64 - 1)
+    return (t & mk) | (code & others)
+
+
+LATTICE_C = {
+    2: [(0, 0), (1, 0), (0, 1), (-1, 0), (0, -1), (1, 1), (-1, 1), (-1, -1), (1, -1)],
+    3: [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (1, 1, 0), (-1, 1, 0),
+        (1, -1, 0), (-1, -1, 0), (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1), (0, 1, 1), (0, -1, 1), (0, 1, -1),
+        (0, -1, -1)],
+}
+
+
+def upstream_lookup(codes, dims: int) -> np.ndarray:
+    """Position of node x - c_q in `codes` (or -1), by Morton steps and a dict lookup, the way the
+    reference's stream finds its source nodes in the level's hash map."""
+    codes = [int(c) for c in np.asarray(codes, dtype=np.uint64)]
+    where = {c: i for i, c in enumerate(codes)}
+    cs = LATTICE_C[dims]
+    out = np.full((len(codes), len(cs)), -1, dtype=np.int64)
+    for i, code in enumerate(codes):
+        for q, c in enumerate(cs):
+            u = code
+            for a in range(dims):
+                if c[a] > 0:
+                    u = morton_neg(u, dims, a)
+                elif c[a] < 0:
+                    u = morton_pos(u, dims, a)
+            out[i, q] = where.get(u, -1)
+    return out

@@ -9,7 +9,7 @@
 //   bc=<face>:<bb|per|neq>[:ux,uy[,uz]]  (repeatable; faces xmin xmax ymin ymax zmin zmax)
 //   init=eq|tgv  u0=<TGV amplitude>  rho0=<default density>  vel=ux,uy[,uz] (initial uniform)
 //   out0=<file>  out=<file>  (binary dumps before and after stepping; optional)
-//   timing=1 (print wall-clock seconds of the TimeMarching loop)
+//   timing=1 (print wall-clock seconds of the TimeMarching loop)  warmup=W (untimed steps first)
 //
 // Dump format (little endian): int32 dims, int32 q, int64 n, then n records of
 // uint64 morton code, int32 flag, int32 pad, double f[q]; records sorted by code.
@@ -88,6 +88,38 @@ void dump(const std::string& path, int dims, int q, amrproject::GridInfoInterfac
 }
 }  // namespace
 
+// mode=morton dims=D in=<file of uint64 codes> out=<file>: for every code write the reference's
+// FindXNeg, FindXPos, FindYNeg, FindYPos[, FindZNeg, FindZPos] (grid/morton_aux.hpp:65-297).
+int morton_mode(int dims, const std::string& in, const std::string& out) {
+    FILE* fi = std::fopen(in.c_str(), "rb");
+    if (!fi) return 3;
+    std::vector<uint64_t> codes;
+    uint64_t v;
+    while (std::fread(&v, sizeof(v), 1, fi) == 1) codes.push_back(v);
+    std::fclose(fi);
+    std::vector<uint64_t> res;
+    amrproject::SFBitsetAux2D a2;
+    amrproject::SFBitsetAux3D a3;
+    a2.SFBitsetInitial();
+    a3.SFBitsetInitial();
+    for (uint64_t c : codes) {
+        DefSFBitset b(c);
+        if (dims == 2) {
+            for (DefSFBitset r : {a2.FindXNeg(b), a2.FindXPos(b), a2.FindYNeg(b), a2.FindYPos(b)})
+                res.push_back(r.to_ullong());
+        } else {
+            for (DefSFBitset r : {a3.FindXNeg(b), a3.FindXPos(b), a3.FindYNeg(b), a3.FindYPos(b),
+                                  a3.FindZNeg(b), a3.FindZPos(b)})
+                res.push_back(r.to_ullong());
+        }
+    }
+    FILE* fo = std::fopen(out.c_str(), "wb");
+    if (!fo) return 3;
+    std::fwrite(res.data(), sizeof(uint64_t), res.size(), fo);
+    std::fclose(fo);
+    return 0;
+}
+
 int main(int argc, char* argv[]) {
     std::map<std::string, std::string> kv;
     std::vector<FaceBc> bcs;
@@ -108,6 +140,7 @@ int main(int argc, char* argv[]) {
         }
     }
     const int dims = kv.count("dims") ? std::atoi(kv["dims"].c_str()) : 2;
+    if (kv.count("mode") && kv["mode"] == "morton") return morton_mode(dims, kv["in"], kv["out"]);
     const std::vector<double> n = parse_list(kv.count("n") ? kv["n"] : "16,16,16");
     const int steps = kv.count("steps") ? std::atoi(kv["steps"].c_str()) : 1;
     const std::string coll = kv.count("coll") ? kv["coll"] : "srt";
@@ -158,7 +191,9 @@ int main(int argc, char* argv[]) {
     auto& grid0 = *amr->ptr_grid_manager_->vec_ptr_grid_info_.at(0);
     const int q = solver.k0NumQ_;
     if (init == "tgv") {
-        // Taylor-Green vortex written into the public node members after SetupMesh.
+        // Taylor-Green vortex written into the public node members after SetupMesh.  The
+        // coordinate is taken modulo the period so the duplicated maximum plane of a periodic
+        // axis starts bit-identical to the minimum plane.
         auto& nodes = *dynamic_cast<lbmproject::GridInfoLbmInteface&>(grid0).GetPtrToLbmGrid();
         auto* aux3 = dynamic_cast<amrproject::SFBitsetAux3D*>(amr->ptr_grid_manager_.get());
         auto* aux2 = dynamic_cast<amrproject::SFBitsetAux2D*>(amr->ptr_grid_manager_.get());
@@ -168,14 +203,14 @@ int main(int argc, char* argv[]) {
             if (dims == 3) {
                 std::array<DefAmrLUint, 3> idx;
                 aux3->SFBitsetComputeIndices(it.first, &idx);
-                x = two_pi * (idx[0] - 1) / n[0];
-                y = two_pi * (idx[1] - 1) / n[1];
-                z = two_pi * (idx[2] - 1) / n[2];
+                x = two_pi * ((idx[0] - 1) % static_cast<DefAmrLUint>(n[0])) / n[0];
+                y = two_pi * ((idx[1] - 1) % static_cast<DefAmrLUint>(n[1])) / n[1];
+                z = two_pi * ((idx[2] - 1) % static_cast<DefAmrLUint>(n[2])) / n[2];
             } else {
                 std::array<DefAmrLUint, 2> idx;
                 aux2->SFBitsetComputeIndices(it.first, &idx);
-                x = two_pi * (idx[0] - 1) / n[0];
-                y = two_pi * (idx[1] - 1) / n[1];
+                x = two_pi * ((idx[0] - 1) % static_cast<DefAmrLUint>(n[0])) / n[0];
+                y = two_pi * ((idx[1] - 1) % static_cast<DefAmrLUint>(n[1])) / n[1];
             }
             std::vector<double> u(dims);
             u[0] = u0 * std::sin(x) * std::cos(y) * std::cos(z);
@@ -192,8 +227,10 @@ int main(int argc, char* argv[]) {
         }
     }
     if (kv.count("out0")) dump(kv["out0"], dims, q, grid0);
+    const int warmup = kv.count("warmup") ? std::atoi(kv["warmup"].c_str()) : 0;
+    for (int it = 0; it < warmup; ++it) amr->TimeMarching(it);
     auto t0 = std::chrono::steady_clock::now();
-    for (int it = 0; it < steps; ++it) amr->TimeMarching(it);
+    for (int it = warmup; it < warmup + steps; ++it) amr->TimeMarching(it);
     auto t1 = std::chrono::steady_clock::now();
     if (kv.count("out")) dump(kv["out"], dims, q, grid0);
     if (kv.count("timing")) {

@@ -1,0 +1,103 @@
+"""Generate the committed golden fixtures from the reference ZLLBM solver itself.
+
+Run in a container that has the reference sources (the oracle harness
+``oracle/_ref/zl_ref_run`` is built from them by ``make -C oracle ref``):
+
+    python tests/golden/make_golden.py
+
+Each ``lbm_<name>.npz`` holds the configuration, the Morton codes of every stored
+node (reference order: sorted codes) and the populations before and after
+``steps`` time steps of the reference's own TimeMarching.  ``morton_<d>d.npz``
+holds codes and the reference's FindXNeg/FindXPos/... results for them.
+"""
+from __future__ import annotations
+
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle.port import (BC_BOUNCE_BACK, BC_NONEQ, BC_PERIODIC, MRT, REF_RUN, SRT, LevelConfig,  # noqa: E402
+                         run_reference)
+
+Z3 = (0.0, 0.0, 0.0)
+
+CASES = {
+    # lid-driven cavity (configuration of the small plain-method case at reduced size)
+    "cavity2d_srt": (LevelConfig(dims=2, n=(16, 16), collision=SRT, nu=0.016,
+                                 bc_kind=(BC_BOUNCE_BACK,) * 4 + (0, 0),
+                                 bc_vel=(Z3, Z3, Z3, (0.1, 0.0, 0.0), Z3, Z3)), 200, "eq"),
+    "cavity2d_mrt": (LevelConfig(dims=2, n=(16, 16), collision=MRT, nu=0.016,
+                                 bc_kind=(BC_BOUNCE_BACK,) * 4 + (0, 0),
+                                 bc_vel=(Z3, Z3, Z3, (0.1, 0.0, 0.0), Z3, Z3)), 200, "eq"),
+    # periodic Taylor-Green vortex, 3D (MRT and SRT) and 2D
+    "tgv3d_mrt": (LevelConfig(dims=3, n=(11, 11, 11), collision=MRT, nu=0.05 / 3.0,
+                              bc_kind=(BC_PERIODIC,) * 6), 30, "tgv"),
+    "tgv3d_srt": (LevelConfig(dims=3, n=(11, 11, 11), collision=SRT, nu=0.05 / 3.0,
+                              bc_kind=(BC_PERIODIC,) * 6), 30, "tgv"),
+    "tgv2d_mrt": (LevelConfig(dims=2, n=(17, 17), collision=MRT, nu=0.02,
+                              bc_kind=(BC_PERIODIC,) * 4 + (0, 0)), 50, "tgv"),
+    # channel: non-equilibrium extrapolation inflow/outflow, bounce-back walls
+    "channel2d_neq": (LevelConfig(dims=2, n=(20, 12), collision=SRT, nu=0.05,
+                                  bc_kind=(BC_NONEQ, BC_NONEQ, BC_BOUNCE_BACK, BC_BOUNCE_BACK, 0, 0),
+                                  bc_vel=((0.05, 0, 0), (0.05, 0, 0), Z3, Z3, Z3, Z3)), 60, "eq"),
+    # mixed faces in 3D: NEQ in x, moving-wall bounce-back in y, periodic z
+    "box3d_mixed": (LevelConfig(dims=3, n=(10, 8, 9), collision=MRT, nu=0.05,
+                                bc_kind=(BC_NONEQ, BC_NONEQ, BC_BOUNCE_BACK, BC_BOUNCE_BACK, BC_PERIODIC, BC_PERIODIC),
+                                bc_vel=((0.05, 0, 0), (0.05, 0, 0), Z3, (0.03, 0, 0.01), Z3, Z3)), 30, "eq"),
+}
+
+
+def morton_cases(dims: int, rng: np.random.Generator) -> np.ndarray:
+    nb = 64 // dims
+    edge = []
+    for a in range(dims):
+        for v in (0, 1, 2, (1 << nb) - 1, (1 << nb) - 2, 1 << (nb - 1)):
+            idx = [5] * dims
+            idx[a] = v
+            code = 0
+            for i in range(nb):
+                for b in range(dims):
+                    code |= ((idx[b] >> i) & 1) << (dims * i + b)
+            edge.append(code)
+    edge += [0, (1 << 64) - 1, 1 << 63, (1 << 63) - 1]
+    rand = rng.integers(0, 2**63, size=200, dtype=np.int64).astype(np.uint64) * np.uint64(2) + \
+        rng.integers(0, 2, size=200, dtype=np.int64).astype(np.uint64)
+    return np.concatenate([np.array(edge, dtype=np.uint64), rand])
+
+
+def main():
+    if not os.path.exists(REF_RUN):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        for name, (cfg, steps, init) in CASES.items():
+            before, after = run_reference(cfg, steps, os.path.join(tmp, name), init=init, u0=0.05)
+            assert np.array_equal(before["code"], after["code"])
+            meta = dict(dims=cfg.dims, n=list(cfg.n), collision=cfg.collision, nu=cfg.nu, rho0=cfg.rho0,
+                        bc_kind=list(cfg.bc_kind), bc_vel=[list(v) for v in cfg.bc_vel], steps=steps, init=init,
+                        u0=0.05)
+            np.savez_compressed(os.path.join(HERE, f"lbm_{name}.npz"), meta=json.dumps(meta),
+                                codes=before["code"], f_before=before["f"], f_after=after["f"])
+            print(name, before.size, "nodes")
+        rng = np.random.default_rng(20261203)
+        for dims in (2, 3):
+            codes = morton_cases(dims, rng)
+            fin = os.path.join(tmp, f"codes{dims}.bin")
+            fout = os.path.join(tmp, f"nbr{dims}.bin")
+            codes.tofile(fin)
+            subprocess.run([REF_RUN, "mode=morton", f"dims={dims}", f"in={fin}", f"out={fout}"], check=True,
+                           cwd=tmp, stdout=subprocess.DEVNULL)
+            nbr = np.fromfile(fout, dtype=np.uint64).reshape(codes.size, 2 * dims)
+            np.savez_compressed(os.path.join(HERE, f"morton_{dims}d.npz"), codes=codes, neighbors=nbr)
+            print("morton", dims, codes.size)
+
+
+if __name__ == "__main__":
+    main()

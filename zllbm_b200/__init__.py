@@ -1,0 +1,294 @@
+"""zllbm_b200 — B200-native lattice-Boltzmann time step over ZLLBM's Morton-coded grid.
+
+The product is the CUDA library ``libzllbm_b200.so`` behind the C ABI declared in
+``include/zllbm_b200.h``.  This module is a thin ctypes binding over that ABI for
+Python callers (tests, benchmarks); it contains no numerics of its own and there
+is no CPU fallback: if the library is missing or no GPU is present, calls fail.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "libzllbm_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "zllbm_b200.h")
+
+D2Q9, D3Q19 = 2, 3
+SRT, MRT = 0, 1
+BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION = 0, 1, 2, 3
+STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
+STORAGE_NAMES = {"f64": STORAGE_F64, "f32": STORAGE_F32, "f16": STORAGE_F16, "bf16": STORAGE_BF16}
+ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE"}
+
+
+class ZlError(RuntimeError):
+    """A non-zero return from the C ABI (the reference logs these through LogManager::LogError)."""
+
+    def __init__(self, code: int, message: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code
+
+
+class ZlConfig(ctypes.Structure):
+    _fields_ = [
+        ("lattice", ctypes.c_int),
+        ("collision", ctypes.c_int),
+        ("storage", ctypes.c_int),
+        ("max_level", ctypes.c_int),
+        ("viscosity", ctypes.c_double),
+        ("rho0", ctypes.c_double),
+        ("bc_kind", ctypes.c_int * 6),
+        ("bc_velocity", (ctypes.c_double * 3) * 6),
+        ("domain_min", ctypes.c_int32 * 3),
+        ("domain_max", ctypes.c_int32 * 3),
+        ("init_velocity", ctypes.c_double * 3),
+        ("storage_scale", ctypes.c_double),
+        ("device", ctypes.c_int),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"zllbm_b200 CUDA library not built: {path} (run python -m zllbm_b200.build)")
+    lib = ctypes.CDLL(path)
+    P = ctypes.c_void_p
+    i64 = ctypes.c_int64
+    u64p = ctypes.POINTER(ctypes.c_uint64)
+    dp = ctypes.POINTER(ctypes.c_double)
+    sig = {
+        "zl_abi_version": ([], ctypes.c_int),
+        "zl_create": ([ctypes.POINTER(ZlConfig), ctypes.POINTER(P)], ctypes.c_int),
+        "zl_destroy": ([P], ctypes.c_int),
+        "zl_set_level_nodes": ([P, ctypes.c_int, u64p, i64], ctypes.c_int),
+        "zl_set_populations": ([P, ctypes.c_int, u64p, dp, i64], ctypes.c_int),
+        "zl_get_populations": ([P, ctypes.c_int, u64p, dp, i64], ctypes.c_int),
+        "zl_get_macros": ([P, ctypes.c_int, u64p, dp, dp, i64], ctypes.c_int),
+        "zl_step_level": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_advance": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_conservation": ([P, ctypes.c_int, dp], ctypes.c_int),
+        "zl_synchronize": ([P], ctypes.c_int),
+        "zl_get_stream": ([P, ctypes.POINTER(P)], ctypes.c_int),
+        "zl_set_stream": ([P, P], ctypes.c_int),
+        "zl_last_error": ([P, ctypes.c_char_p, ctypes.c_size_t], ctypes.c_int),
+        "zl_level_info": ([P, ctypes.c_int, ctypes.POINTER(i64), ctypes.POINTER(ctypes.c_int32),
+                           ctypes.POINTER(i64)], ctypes.c_int),
+        "zl_morton_neighbors": ([ctypes.c_int, u64p, i64, u64p], ctypes.c_int),
+        "zl_upstream_index": ([ctypes.c_int, u64p, i64, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "zl_mrt_matrix": ([ctypes.c_int, ctypes.c_double, dp], ctypes.c_int),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def header_symbols(path: str = HEADER) -> list[str]:
+    """Function names declared in include/zllbm_b200.h."""
+    import re
+
+    text = open(path).read()
+    return sorted(set(re.findall(r"^\s*int\s+(zl_\w+)\s*\(", text, flags=re.M)))
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.uint64))
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+
+
+def _p(a: np.ndarray, ct):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+@dataclass
+class SolverConfig:
+    """Mirror of the settings a reference application makes on SolverLbmInterface / GridManager."""
+
+    lattice: int = D3Q19
+    collision: int = SRT
+    storage: int = STORAGE_F64
+    max_level: int = 0
+    viscosity: float = 0.1
+    rho0: float = 1.0
+    bc_kind: tuple = (0, 0, 0, 0, 0, 0)
+    bc_velocity: tuple = ((0.0, 0.0, 0.0),) * 6
+    domain_min: tuple = (1, 1, 1)
+    domain_max: tuple = (2, 2, 2)
+    init_velocity: tuple = (0.0, 0.0, 0.0)
+    storage_scale: float = 0.0
+    device: int = 0
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def dims(self) -> int:
+        return 2 if self.lattice == D2Q9 else 3
+
+    @property
+    def q(self) -> int:
+        return 9 if self.lattice == D2Q9 else 19
+
+    def to_c(self) -> ZlConfig:
+        c = ZlConfig()
+        c.lattice, c.collision, c.storage, c.max_level = self.lattice, self.collision, self.storage, self.max_level
+        c.viscosity, c.rho0 = self.viscosity, self.rho0
+        for f in range(6):
+            c.bc_kind[f] = int(self.bc_kind[f])
+            for a in range(3):
+                c.bc_velocity[f][a] = float(self.bc_velocity[f][a]) if a < len(self.bc_velocity[f]) else 0.0
+        for a in range(3):
+            c.domain_min[a] = int(self.domain_min[a]) if a < len(self.domain_min) else 0
+            c.domain_max[a] = int(self.domain_max[a]) if a < len(self.domain_max) else 0
+            c.init_velocity[a] = float(self.init_velocity[a]) if a < len(self.init_velocity) else 0.0
+        c.storage_scale = self.storage_scale
+        c.device = self.device
+        return c
+
+
+class Context:
+    """One device context (zl_create / zl_destroy)."""
+
+    def __init__(self, config: SolverConfig):
+        self.lib = load_library()
+        self.config = config
+        h = ctypes.c_void_p()
+        self._cfg = config.to_c()
+        rc = self.lib.zl_create(ctypes.byref(self._cfg), ctypes.byref(h))
+        if rc != 0:
+            raise ZlError(rc, "zl_create failed")
+        self.handle = h
+
+    def _check(self, rc: int):
+        if rc != 0:
+            buf = ctypes.create_string_buffer(512)
+            self.lib.zl_last_error(self.handle, buf, 512)
+            raise ZlError(rc, buf.value.decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.zl_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def set_level_nodes(self, level: int, codes):
+        c = _u64(codes)
+        self._check(self.lib.zl_set_level_nodes(self.handle, level, _p(c, ctypes.c_uint64), c.size))
+
+    def set_populations(self, level: int, codes, f):
+        c, ff = _u64(codes), _f64(f)
+        assert ff.size == c.size * self.config.q
+        self._check(self.lib.zl_set_populations(self.handle, level, _p(c, ctypes.c_uint64),
+                                                _p(ff, ctypes.c_double), c.size))
+
+    def get_populations(self, level: int, codes) -> np.ndarray:
+        c = _u64(codes)
+        out = np.empty((c.size, self.config.q))
+        self._check(self.lib.zl_get_populations(self.handle, level, _p(c, ctypes.c_uint64),
+                                                _p(out, ctypes.c_double), c.size))
+        return out
+
+    def get_macros(self, level: int, codes):
+        c = _u64(codes)
+        rho = np.empty(c.size)
+        u = np.empty((c.size, self.config.dims))
+        self._check(self.lib.zl_get_macros(self.handle, level, _p(c, ctypes.c_uint64), _p(rho, ctypes.c_double),
+                                           _p(u, ctypes.c_double), c.size))
+        return rho, u
+
+    def step_level(self, level: int = 0):
+        self._check(self.lib.zl_step_level(self.handle, level))
+
+    def advance(self, steps: int):
+        self._check(self.lib.zl_advance(self.handle, steps))
+
+    def conservation(self, level: int = 0) -> np.ndarray:
+        out = np.zeros(4)
+        self._check(self.lib.zl_conservation(self.handle, level, _p(out, ctypes.c_double)))
+        return out[: self.config.dims + 1]
+
+    def synchronize(self):
+        self._check(self.lib.zl_synchronize(self.handle))
+
+    def stream(self) -> int:
+        """The cudaStream_t the context issues work on (as an integer handle)."""
+        h = ctypes.c_void_p()
+        self._check(self.lib.zl_get_stream(self.handle, ctypes.byref(h)))
+        return h.value or 0
+
+    def set_stream(self, stream: int | None):
+        self._check(self.lib.zl_set_stream(self.handle, ctypes.c_void_p(stream) if stream else None))
+
+    def level_info(self, level: int = 0):
+        n = ctypes.c_int64()
+        ext = (ctypes.c_int32 * 3)()
+        pb = ctypes.c_int64()
+        self._check(self.lib.zl_level_info(self.handle, level, ctypes.byref(n), ext, ctypes.byref(pb)))
+        return n.value, tuple(ext), pb.value
+
+
+def morton_neighbors(dims: int, codes) -> np.ndarray:
+    lib = load_library()
+    c = _u64(codes)
+    out = np.empty((c.size, 2 * dims), dtype=np.uint64)
+    rc = lib.zl_morton_neighbors(dims, _p(c, ctypes.c_uint64), c.size, _p(out, ctypes.c_uint64))
+    if rc:
+        raise ZlError(rc, "zl_morton_neighbors")
+    return out
+
+
+def upstream_index(lattice: int, codes) -> np.ndarray:
+    lib = load_library()
+    c = _u64(codes)
+    q = 9 if lattice == D2Q9 else 19
+    out = np.empty((c.size, q), dtype=np.int64)
+    rc = lib.zl_upstream_index(lattice, _p(c, ctypes.c_uint64), c.size, _p(out, ctypes.c_int64))
+    if rc:
+        raise ZlError(rc, "zl_upstream_index")
+    return out
+
+
+def mrt_matrix(lattice: int, tau: float) -> np.ndarray:
+    lib = load_library()
+    q = 9 if lattice == D2Q9 else 19
+    out = np.empty(q * q)
+    rc = lib.zl_mrt_matrix(lattice, tau, _p(out, ctypes.c_double))
+    if rc:
+        raise ZlError(rc, "zl_mrt_matrix")
+    return out.reshape(q, q)
+
+
+def box_codes(dims: int, lo, hi) -> np.ndarray:
+    """Morton codes of every node with lo <= index <= hi per axis, x fastest (host helper)."""
+    axes = [np.arange(lo[a], hi[a] + 1, dtype=np.uint64) for a in range(dims)]
+    grids = np.meshgrid(*reversed(axes), indexing="ij")
+    idx = np.stack([g.ravel() for g in reversed(grids)], axis=1)
+    out = np.zeros(idx.shape[0], dtype=np.uint64)
+    for i in range(64 // dims):
+        for a in range(dims):
+            out |= ((idx[:, a] >> np.uint64(i)) & np.uint64(1)) << np.uint64(dims * i + a)
+    return out

@@ -1,0 +1,384 @@
+// Fused collide + stream for one refinement level, single buffer (AA pattern),
+// structure-of-arrays populations in a dense, padded box per level.
+//
+// Replaces the reference's per-level RunSolverOnGivenGrid (collide every node,
+// then pull-stream every node through hash-map lookups,
+// lbm_project/lbm_solver_interface.cpp:246-262, d3q19_model/lbm_d3q19_solver.cpp:20-136)
+// plus the node-local part of ComputeDomainBoundaryCondition (bounce back,
+// lbm_project/boundary_conditions/lbm_bounce_back.cpp:28-91; periodic faces
+// become index wrap-around).
+//
+// State between steps is the reference's post-stream population f_, held in
+// one of two layouts that alternate every step:
+//   after an even step   f(x, q) lives in slot(x - c_q, opp(q))   (q != 0)
+//   after an odd step    f(x, q) lives in slot(x, q)
+// Slots of cells that hold no node (the one-cell ghost frame of non-periodic
+// axes, or cells a refinement level does not cover) carry the reference's
+// "stale" values: where the upstream node x - c_q does not exist the
+// reference leaves f_(x, q) unchanged (lbm_d3q19_solver.cpp:31-33); here the
+// node writes its own pre-collision value into the slot that holds f(x, q).
+#pragma once
+#include <cuda_fp16.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <cstdint>
+#include "lattice.cuh"
+
+namespace zl {
+
+enum BcKind : int { kBcNone = 0, kBcBounceBack = 1, kBcPeriodic = 2, kBcNeq = 3 };
+enum Collision : int { kSrt = 0, kMrt = 1 };
+
+// Per-cell information for levels whose node set does not fill its box.
+constexpr uint32_t kInfoPresent = 1u << 31;
+constexpr int kInfoFaceShift = 24;  // 6 bits: on face xmin..zmax (reference boundary node sets)
+
+struct LevelGeom {
+    int n[3];          // nodes per axis (periodic axes hold each plane once)
+    int g[3];          // ghost frame width per axis (0 on periodic axes, 1 otherwise)
+    int a[3];          // allocated extents, n + 2 g
+    int periodic[3];   // wrap-around per axis
+    long long stride;  // elements between population planes (>= a0 a1 a2)
+    int face_on_box;   // bit f: box edge f lies on domain face f (non-periodic faces only)
+    const uint32_t* info;  // per-cell info (masked levels), nullptr for full boxes
+};
+
+struct StepParams {
+    double tau;             // relaxation time at this level
+    double rho0;            // default density
+    int face_kind[6];       // BcKind per face
+    double bb_term[6][19];  // 6 rho0 w_o (c_o . U_face) for outgoing direction o
+    const double* mrt64;    // dense M^-1 S M, reference construction order (FP64 mode)
+    float mrt_coef[19];     // S_k / |M_k|^2 per moment (fast path)
+    float inv_scale;        // reduced storage: deviation = stored * inv_scale
+    float scale;
+};
+
+// ---------------------------------------------------------------- storage
+template <class S> struct Storage;
+template <> struct Storage<double> {
+    using T = double;
+    static constexpr bool kDeviation = false;
+    ZL_HD static T load(const double* p, const StepParams&) { return *p; }
+    ZL_HD static void store(double* p, T v, const StepParams&) { *p = v; }
+};
+template <> struct Storage<float> {
+    using T = float;
+    static constexpr bool kDeviation = true;
+    __device__ __forceinline__ static T load(const float* p, const StepParams&) { return __ldg(p); }
+    __device__ __forceinline__ static void store(float* p, T v, const StepParams&) { *p = v; }
+};
+template <> struct Storage<__half> {
+    using T = float;
+    static constexpr bool kDeviation = true;
+    __device__ __forceinline__ static T load(const __half* p, const StepParams& sp) {
+        return __half2float(__ldg(p)) * sp.inv_scale;
+    }
+    __device__ __forceinline__ static void store(__half* p, T v, const StepParams& sp) {
+        *p = __float2half_rn(v * sp.scale);
+    }
+};
+template <> struct Storage<__nv_bfloat16> {
+    using T = float;
+    static constexpr bool kDeviation = true;
+    __device__ __forceinline__ static T load(const __nv_bfloat16* p, const StepParams& sp) {
+        return __bfloat162float(__ldg(p)) * sp.inv_scale;
+    }
+    __device__ __forceinline__ static void store(__nv_bfloat16* p, T v, const StepParams& sp) {
+        *p = __float2bfloat16_rn(v * sp.scale);
+    }
+};
+
+// ---------------------------------------------------------------- collision
+// Exact FP64 path: reference arithmetic order (lbm_solver_interface.cpp:374-435, :477-532,
+// collision_model/lbm_collision_model_srt.cpp:20-25, lbm_collision_model_mrt.cpp:114-125).
+// Compiled with -fmad=false so that no product is fused into an FMA.  Terms the
+// reference multiplies by a zero lattice component add +-0 and are skipped: that
+// leaves every sum bit-identical.
+template <class L>
+__device__ __forceinline__ void macro_exact(const double* f, double& rho, double& ux, double& uy, double& uz) {
+    using Tb = Tables<L>;
+    rho = f[0];
+    ux = 0.;
+    uy = 0.;
+    uz = 0.;
+#pragma unroll
+    for (int q = 1; q < L::kQ; ++q) {
+        rho = rho + f[q];
+        if (Tb::cx(q) == 1) ux = ux + f[q];
+        if (Tb::cx(q) == -1) ux = ux - f[q];
+        if (Tb::cy(q) == 1) uy = uy + f[q];
+        if (Tb::cy(q) == -1) uy = uy - f[q];
+        if (L::kDims == 3) {
+            if (Tb::cz(q) == 1) uz = uz + f[q];
+            if (Tb::cz(q) == -1) uz = uz - f[q];
+        }
+    }
+    ux = ux / rho;
+    uy = uy / rho;
+    if (L::kDims == 3) uz = uz / rho;
+}
+
+template <class L>
+__device__ __forceinline__ void feq_exact(double rho, double ux, double uy, double uz, double* feq) {
+    using Tb = Tables<L>;
+    const double uv_sq = L::kDims == 3 ? (ux * ux + uy * uy) + uz * uz : ux * ux + uy * uy;
+#pragma unroll
+    for (int q = 0; q < L::kQ; ++q) {
+        // c.u over the non-zero components in x, y, z order
+        double cu = 0.;
+        bool first = true;
+        if (Tb::cx(q) != 0) {
+            cu = Tb::cx(q) == 1 ? ux : -ux;
+            first = false;
+        }
+        if (Tb::cy(q) != 0) {
+            const double t = Tb::cy(q) == 1 ? uy : -uy;
+            cu = first ? t : cu + t;
+            first = false;
+        }
+        if (L::kDims == 3 && Tb::cz(q) != 0) {
+            const double t = Tb::cz(q) == 1 ? uz : -uz;
+            cu = first ? t : cu + t;
+            first = false;
+        }
+        const double wr = Tb::w(q) * rho;
+        feq[q] = wr * (((1. + 3. * cu) + (4.5 * cu) * cu) - 1.5 * uv_sq);
+    }
+}
+
+template <class L>
+__device__ __forceinline__ void collide_exact(const double* f, double* out, const StepParams& p, int coll) {
+    constexpr int Q = L::kQ;
+    double rho, ux, uy, uz;
+    macro_exact<L>(f, rho, ux, uy, uz);
+    double feq[Q];
+    feq_exact<L>(rho, ux, uy, uz, feq);
+    if (coll == kSrt) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] = f[q] - (f[q] - feq[q]) / p.tau;
+    } else {
+        double d[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) d[q] = f[q] - feq[q];
+        const double* A = p.mrt64;
+#pragma unroll 1
+        for (int q = 0; q < Q; ++q) {
+            double acc = 0.;
+#pragma unroll
+            for (int s = 0; s < Q; ++s) acc = acc + __ldg(A + q * Q + s) * d[s];
+            out[q] = f[q] - acc;
+        }
+    }
+}
+
+// Fast path on deviations d_q = f_q - w_q, FP32 arithmetic.
+template <class L>
+__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll) {
+    using Tb = Tables<L>;
+    constexpr int Q = L::kQ;
+    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        drho += d[q];
+        if (Tb::cx(q)) jx += Tb::cx(q) == 1 ? d[q] : -d[q];
+        if (Tb::cy(q)) jy += Tb::cy(q) == 1 ? d[q] : -d[q];
+        if (L::kDims == 3 && Tb::cz(q)) jz += Tb::cz(q) == 1 ? d[q] : -d[q];
+    }
+    const float rho = 1.f + drho;
+    const float inv_rho = 1.f / rho;
+    const float ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+    const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+    float neq[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        const float cu = Tb::cx(q) * ux + Tb::cy(q) * uy + Tb::cz(q) * uz;
+        const float w = (float)Tb::w(q);
+        const float deq = w * (drho + rho * (3.f * cu + 4.5f * cu * cu - usq15));
+        neq[q] = d[q] - deq;
+    }
+    if (coll == kSrt) {
+        const float omega = (float)(1.0 / p.tau);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] = d[q] - omega * neq[q];
+    } else {
+        // m_k = M_k . neq for non-conserved moments, relaxed and mapped back with M^T / |M_k|^2
+        float mk[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            float acc = 0.f;
+            if (Tb::s(k) != 0.) {
+#pragma unroll
+                for (int j = 0; j < Q; ++j) {
+                    const int m = Tb::M(k, j);
+                    if (m == 1) acc += neq[j];
+                    else if (m == -1) acc -= neq[j];
+                    else if (m != 0) acc += (float)m * neq[j];
+                }
+            }
+            mk[k] = acc * p.mrt_coef[k];
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            float acc = 0.f;
+#pragma unroll
+            for (int k = 0; k < Q; ++k) {
+                if (Tb::s(k) == 0.) continue;
+                const int m = Tb::M(k, q);
+                if (m == 1) acc += mk[k];
+                else if (m == -1) acc -= mk[k];
+                else if (m != 0) acc += (float)m * mk[k];
+            }
+            out[q] = d[q] - acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- geometry helpers
+struct Coord {
+    int x[3];  // node coordinates, each in [0, n)
+};
+
+__device__ __forceinline__ int wrap_or_ghost(int v, int n, int g, int periodic) {
+    // node coordinate v in [-1, n] -> box coordinate
+    if (periodic) {
+        v = v < 0 ? v + n : (v >= n ? v - n : v);
+        return v;
+    }
+    return v + g;
+}
+
+template <class L>
+__device__ __forceinline__ bool upstream_missing(const LevelGeom& geo, const Coord& c, int q) {
+    using Tb = Tables<L>;
+    const int s[3] = {c.x[0] - Tb::cx(q), c.x[1] - Tb::cy(q), c.x[2] - Tb::cz(q)};
+#pragma unroll
+    for (int a = 0; a < L::kDims; ++a)
+        if (!geo.periodic[a] && (s[a] < 0 || s[a] >= geo.n[a])) return true;
+    return false;
+}
+
+__device__ __forceinline__ int on_faces(const LevelGeom& geo, const Coord& c, int dims) {
+    int bits = 0;
+    for (int a = 0; a < dims; ++a) {
+        if (c.x[a] == 0) bits |= 1 << (2 * a);
+        if (c.x[a] == geo.n[a] - 1) bits |= 1 << (2 * a + 1);
+    }
+    return bits & geo.face_on_box;
+}
+
+// Value of the incoming population f(x, q) when its upstream node is missing: the
+// bounce-back of the last bounce-back face (in the reference's order xmin, ymin, zmin,
+// xmax, ymax, zmax) the node lies on and q enters through, else the stale pre-collision value.
+template <class L, class T>
+__device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const T* post, const StepParams& p) {
+    T v = pre[q];
+#pragma unroll
+    for (int k = 0; k < 2 * L::kDims; ++k) {
+        const int face = k < L::kDims ? 2 * k : 2 * (k - L::kDims) + 1;
+        if ((faces >> face) & 1) {
+            if (p.face_kind[face] == kBcBounceBack && enters_through<L>(q, face)) {
+                const int o = Tables<L>::opp(q);
+                v = post[o] - (T)p.bb_term[face][o];
+            }
+        }
+    }
+    return v;
+}
+
+// ---------------------------------------------------------------- the step kernel
+// One thread per node of the level box.  Odd selects the layout read (see file comment).
+// Bnd: the level has at least one non-periodic axis.  Masked: the box holds absent cells.
+template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked>
+__global__ void __launch_bounds__(256) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    using Tb = Tables<L>;
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    Coord c;
+    c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
+    c.x[1] = blockIdx.y;
+    c.x[2] = blockIdx.z;
+    if (c.x[0] >= geo.n[0]) return;
+
+    // box coordinates of x-1, x, x+1 along each axis
+    int bx[3], by[3], bz[3];
+#pragma unroll
+    for (int d = -1; d <= 1; ++d) {
+        bx[d + 1] = wrap_or_ghost(c.x[0] + d, geo.n[0], geo.g[0], geo.periodic[0]);
+        by[d + 1] = wrap_or_ghost(c.x[1] + d, geo.n[1], geo.g[1], geo.periodic[1]);
+        bz[d + 1] = L::kDims == 3 ? wrap_or_ghost(c.x[2] + d, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+    }
+    const long long a0 = geo.a[0], a01 = (long long)geo.a[0] * geo.a[1];
+    auto cell = [&](int dx, int dy, int dz) -> long long {
+        return bx[dx + 1] + a0 * by[dy + 1] + a01 * bz[dz + 1];
+    };
+    const long long self = cell(0, 0, 0);
+
+    uint32_t info = 0;
+    if (Masked) {
+        info = __ldg(geo.info + self);
+        if (!(info & kInfoPresent)) return;
+    }
+    const long long st = geo.stride;
+
+    T pre[Q], post[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (Odd && q != 0) {
+            pre[q] = St::load(f + Tb::opp(q) * st + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), p);
+        } else {
+            pre[q] = St::load(f + q * st + self, p);
+        }
+    }
+
+    if constexpr (St::kDeviation) {
+        collide_dev<L>(pre, post, p, Coll);
+    } else {
+        collide_exact<L>(pre, post, p, Coll);
+    }
+
+    int faces = 0;
+    if (Bnd) faces = Masked ? (int)((info >> kInfoFaceShift) & 63u) : on_faces(geo, c, L::kDims);
+
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        if (Odd && q != 0) {
+            St::store(f + q * st + cell(Tb::cx(q), Tb::cy(q), Tb::cz(q)), post[q], p);
+        } else {
+            St::store(f + Tb::opp(q) * st + self, post[q], p);
+        }
+    }
+    if (Bnd || Masked) {
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            const bool miss = Masked ? ((info >> q) & 1u) : upstream_missing<L>(geo, c, q);
+            if (!miss) continue;
+            const T v = missing_value<L, T>(q, faces, pre, post, p);
+            if (Odd) {
+                St::store(f + q * st + self, v, p);
+            } else {
+                St::store(f + Tb::opp(q) * st + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v, p);
+            }
+        }
+    }
+}
+
+// Slot holding the post-stream population f(x, q) in the given layout phase.
+template <class L>
+__device__ __forceinline__ long long post_stream_slot(const LevelGeom& geo, const Coord& c, int q, bool even_layout) {
+    using Tb = Tables<L>;
+    int dx = 0, dy = 0, dz = 0, plane = q;
+    if (even_layout && q != 0) {
+        dx = -Tb::cx(q);
+        dy = -Tb::cy(q);
+        dz = -Tb::cz(q);
+        plane = Tb::opp(q);
+    }
+    const long long bx = wrap_or_ghost(c.x[0] + dx, geo.n[0], geo.g[0], geo.periodic[0]);
+    const long long by = wrap_or_ghost(c.x[1] + dy, geo.n[1], geo.g[1], geo.periodic[1]);
+    const long long bz = L::kDims == 3 ? wrap_or_ghost(c.x[2] + dz, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+    return plane * geo.stride + bx + (long long)geo.a[0] * (by + (long long)geo.a[1] * bz);
+}
+
+}  // namespace zl

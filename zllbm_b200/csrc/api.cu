@@ -1,0 +1,573 @@
+// C ABI of zllbm_b200 (include/zllbm_b200.h): contexts, levels, host exchange, stepping.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/zllbm_b200.h"
+#include "topology.cuh"
+
+using namespace zl;
+
+namespace {
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    ~DeviceBuffer() { release(); }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+};
+
+struct Level {
+    bool active = false;
+    LevelGeom geo{};
+    LevelMap map{};
+    StepParams params{};
+    DeviceBuffer f;          // populations
+    DeviceBuffer info;       // per-cell info (masked levels only)
+    DeviceBuffer mrt64;      // dense M^-1 S M (FP64 storage)
+    DeviceBuffer feq_face;   // feq(rho0, U_face) per face, 6 * q doubles
+    DeviceBuffer partial;    // conservation partial sums
+    int partial_blocks = 0;
+    bool bnd = false;        // some axis is not periodic
+    int even_layout = 0;     // 1 after an even step (see aa_kernel.cuh)
+    long long nodes = 0;
+    long long steps = 0;
+};
+
+}  // namespace
+
+struct zl_ctx {
+    zl_config cfg{};
+    int dims = 3;
+    int q = 19;
+    cudaStream_t stream = nullptr;      // stream all work is issued on
+    cudaStream_t own_stream = nullptr;  // the context's own stream
+    const LaunchSet* ops = nullptr;
+    Level levels[ZL_MAX_LEVELS];
+    std::string last_error;
+    DeviceBuffer scratch_flag;  // int error flag for kernels that validate codes
+};
+
+namespace {
+
+int fail(zl_ctx* ctx, int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->last_error = buf;
+    return code;
+}
+
+#define ZL_CUDA(ctx, expr)                                                                          \
+    do {                                                                                            \
+        cudaError_t _e = (expr);                                                                    \
+        if (_e != cudaSuccess)                                                                      \
+            return fail(ctx, ZL_EDEVICE, "%s failed: %s (%s:%d)", #expr, cudaGetErrorString(_e),    \
+                        __FILE__, __LINE__);                                                        \
+    } while (0)
+
+int alloc(zl_ctx* ctx, DeviceBuffer& b, size_t bytes) {
+    b.release();
+    if (bytes == 0) return ZL_OK;
+    cudaError_t e = cudaMalloc(&b.ptr, bytes);
+    if (e != cudaSuccess) {
+        b.ptr = nullptr;
+        return fail(ctx, ZL_EDEVICE, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+    }
+    b.bytes = bytes;
+    return ZL_OK;
+}
+
+double lattice_w(int dims, int q) { return dims == 2 ? Tables<D2Q9>::w(q) : Tables<D3Q19>::w(q); }
+int lattice_c(int dims, int q, int a) {
+    if (dims == 2) return a == 0 ? Tables<D2Q9>::cx(q) : (a == 1 ? Tables<D2Q9>::cy(q) : 0);
+    return a == 0 ? Tables<D3Q19>::cx(q) : (a == 1 ? Tables<D3Q19>::cy(q) : Tables<D3Q19>::cz(q));
+}
+int lattice_m(int dims, int k, int j) { return dims == 2 ? Tables<D2Q9>::M(k, j) : Tables<D3Q19>::M(k, j); }
+double lattice_s(int dims, int k) { return dims == 2 ? Tables<D2Q9>::s(k) : Tables<D3Q19>::s(k); }
+int lattice_norm2(int dims, int k) { return dims == 2 ? row_norm2<D2Q9>(k) : row_norm2<D3Q19>(k); }
+
+// feq in the reference's arithmetic order (lbm_solver_interface.cpp:374-417), host side
+void host_feq(int dims, double rho, const double* u, double* out) {
+    const int q = dims == 2 ? 9 : 19;
+    const double uv_sq = dims == 2 ? u[0] * u[0] + u[1] * u[1] : u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
+    for (int k = 0; k < q; ++k) {
+        const double cx = lattice_c(dims, k, 0), cy = lattice_c(dims, k, 1), cz = lattice_c(dims, k, 2);
+        const double c_uv = dims == 2 ? u[0] * cx + u[1] * cy : u[0] * cx + u[1] * cy + u[2] * cz;
+        out[k] = lattice_w(dims, k) * rho * (1. + 3. * c_uv + 4.5 * c_uv * c_uv - 1.5 * uv_sq);
+    }
+}
+
+// M^-1 S M (or M^-1 (I - S/2) M) in the reference's loop order
+// (collision_model/lbm_collision_model_mrt.cpp:63-107).  M^-1 = M^T diag(1/|M_k|^2).
+void host_mrt_matrix(int dims, double relax, bool d_matrix, double* out) {
+    const int q = dims == 2 ? 9 : 19;
+    std::vector<double> s(q), sm(q * q);
+    for (int k = 0; k < q; ++k) {
+        const double sk = lattice_s(dims, k);
+        s[k] = sk < 0. ? relax : sk;
+        if (d_matrix) s[k] = 1. - 0.5 * s[k];
+    }
+    for (int j = 0; j < q; ++j)
+        for (int i = 0; i < q; ++i) {
+            double acc = 0.;
+            for (int k = 0; k < q; ++k) acc = acc + (i == k ? s[i] : 0.) * (double)lattice_m(dims, k, j);
+            sm[i * q + j] = acc;
+        }
+    for (int j = 0; j < q; ++j)
+        for (int i = 0; i < q; ++i) {
+            double acc = 0.;
+            for (int k = 0; k < q; ++k) {
+                const double im = (double)lattice_m(dims, k, i) / (double)lattice_norm2(dims, k);
+                acc = acc + im * sm[k * q + j];
+            }
+            out[i * q + j] = acc;
+        }
+}
+
+int check_level(zl_ctx* ctx, int level, bool need_active) {
+    if (!ctx) return ZL_EINVAL;
+    if (level < 0 || level > ctx->cfg.max_level || level >= ZL_MAX_LEVELS)
+        return fail(ctx, ZL_EINVAL, "level %d outside [0, %d]", level, ctx->cfg.max_level);
+    if (need_active && !ctx->levels[level].active)
+        return fail(ctx, ZL_ESTATE, "level %d has no nodes (call zl_set_level_nodes first)", level);
+    return ZL_OK;
+}
+
+// Copy host codes to a temporary device array.
+int upload_codes(zl_ctx* ctx, const uint64_t* codes, int64_t n, DeviceBuffer& d) {
+    int rc = alloc(ctx, d, (size_t)n * sizeof(uint64_t));
+    if (rc) return rc;
+    if (n > 0) ZL_CUDA(ctx, cudaMemcpyAsync(d.ptr, codes, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
+    return ZL_OK;
+}
+
+int read_flag(zl_ctx* ctx, int* value) {
+    ZL_CUDA(ctx, cudaMemcpyAsync(value, ctx->scratch_flag.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return ZL_OK;
+}
+
+int reset_flag(zl_ctx* ctx) {
+    ZL_CUDA(ctx, cudaMemsetAsync(ctx->scratch_flag.ptr, 0, sizeof(int), ctx->stream));
+    return ZL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zl_abi_version(void) { return ZL_ABI_VERSION; }
+
+int zl_create(const zl_config* config, zl_ctx** out) {
+    if (!config || !out) return ZL_EINVAL;
+    *out = nullptr;
+    if (config->lattice != ZL_D2Q9 && config->lattice != ZL_D3Q19) return ZL_EINVAL;
+    if (config->collision != ZL_SRT && config->collision != ZL_MRT) return ZL_EINVAL;
+    if (config->storage < ZL_STORAGE_F64 || config->storage > ZL_STORAGE_BF16) return ZL_EINVAL;
+    if (config->max_level < 0 || config->max_level >= ZL_MAX_LEVELS) return ZL_EINVAL;
+    if (!(config->viscosity > 0.)) return ZL_EINVAL;
+    for (int f = 0; f < 6; ++f)
+        if (config->bc_kind[f] < ZL_BC_NONE || config->bc_kind[f] > ZL_BC_NONEQ_EXTRAPOLATION) return ZL_EINVAL;
+    const int dims = config->lattice == ZL_D2Q9 ? 2 : 3;
+    for (int a = 0; a < dims; ++a) {
+        if (config->domain_max[a] <= config->domain_min[a]) return ZL_EINVAL;
+        const bool pmin = config->bc_kind[2 * a] == ZL_BC_PERIODIC, pmax = config->bc_kind[2 * a + 1] == ZL_BC_PERIODIC;
+        if (pmin != pmax) return ZL_EINVAL;  // periodic faces come in pairs
+    }
+    if (cudaSetDevice(config->device) != cudaSuccess) return ZL_EDEVICE;
+    zl_ctx* ctx = new zl_ctx();
+    ctx->cfg = *config;
+    ctx->dims = dims;
+    ctx->q = dims == 2 ? 9 : 19;
+    switch (config->storage) {
+        case ZL_STORAGE_F64: ctx->ops = &launch_set_f64(); break;
+        case ZL_STORAGE_F32: ctx->ops = &launch_set_f32(); break;
+        case ZL_STORAGE_F16: ctx->ops = &launch_set_f16(); break;
+        default: ctx->ops = &launch_set_bf16(); break;
+    }
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return ZL_EDEVICE;
+    }
+    ctx->stream = ctx->own_stream;
+    if (alloc(ctx, ctx->scratch_flag, sizeof(int)) != ZL_OK) {
+        cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+        return ZL_EDEVICE;
+    }
+    *out = ctx;
+    return ZL_OK;
+}
+
+int zl_destroy(zl_ctx* ctx) {
+    if (!ctx) return ZL_EINVAL;
+    cudaSetDevice(ctx->cfg.device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& l : ctx->levels) {
+        l.f.release();
+        l.info.release();
+        l.mrt64.release();
+        l.feq_face.release();
+        l.partial.release();
+    }
+    ctx->scratch_flag.release();
+    cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return ZL_OK;
+}
+
+int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n) {
+    int rc = check_level(ctx, level, false);
+    if (rc) return rc;
+    if (!codes || n <= 0) return fail(ctx, ZL_EINVAL, "empty node set for level %d", level);
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    const int dims = ctx->dims, q = ctx->q;
+    Level& L = ctx->levels[level];
+    L.active = false;
+
+    DeviceBuffer dcodes, dminmax;
+    if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
+    if ((rc = alloc(ctx, dminmax, 6 * sizeof(int)))) return rc;
+    int init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, 0, 0, 0};
+    ZL_CUDA(ctx, cudaMemcpyAsync(dminmax.ptr, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+    ZL_CUDA(ctx, launch_decode_minmax((const uint64_t*)dcodes.ptr, n, dims, (int*)dminmax.ptr, ctx->stream));
+    int mm[6];
+    ZL_CUDA(ctx, cudaMemcpyAsync(mm, dminmax.ptr, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+
+    // level box: periodic axes that the level spans completely wrap around, others get a ghost frame
+    LevelGeom geo{};
+    LevelMap map{};
+    map.dims = dims;
+    geo.face_on_box = 0;
+    for (int a = 0; a < 3; ++a) {
+        if (a >= dims) {
+            geo.n[a] = 1;
+            geo.g[a] = 0;
+            geo.a[a] = 1;
+            geo.periodic[a] = 0;
+            map.lo[a] = 0;
+            map.n[a] = 1;
+            map.periodic[a] = 0;
+            continue;
+        }
+        const long long dlo = (long long)ctx->cfg.domain_min[a] << level;
+        const long long dhi = (long long)ctx->cfg.domain_max[a] << level;
+        if (mm[a] < dlo || mm[3 + a] > dhi)
+            return fail(ctx, ZL_ETOPOLOGY, "level %d node indices [%d, %d] on axis %d leave the domain [%lld, %lld]",
+                        level, mm[a], mm[3 + a], a, dlo, dhi);
+        const bool per = ctx->cfg.bc_kind[2 * a] == ZL_BC_PERIODIC;
+        if (per && mm[a] == dlo && mm[3 + a] == dhi) {
+            geo.n[a] = (int)(dhi - dlo);
+            geo.g[a] = 0;
+            geo.periodic[a] = 1;
+            map.lo[a] = (int)dlo;
+        } else {
+            geo.n[a] = mm[3 + a] - mm[a] + 1;
+            geo.g[a] = 1;
+            geo.periodic[a] = 0;
+            map.lo[a] = mm[a];
+            if (!per) {
+                if (mm[a] == dlo) geo.face_on_box |= 1 << (2 * a);
+                if (mm[3 + a] == dhi) geo.face_on_box |= 1 << (2 * a + 1);
+            }
+        }
+        geo.a[a] = geo.n[a] + 2 * geo.g[a];
+        map.n[a] = geo.n[a];
+        map.periodic[a] = geo.periodic[a];
+    }
+    const long long cells = (long long)geo.a[0] * geo.a[1] * geo.a[2];
+    geo.stride = (cells + 63) / 64 * 64;
+    geo.info = nullptr;
+
+    // presence mask; a full box drops it and uses the coordinate-only kernels
+    if ((rc = alloc(ctx, L.info, (size_t)cells * sizeof(uint32_t)))) return rc;
+    ZL_CUDA(ctx, cudaMemsetAsync(L.info.ptr, 0, (size_t)cells * sizeof(uint32_t), ctx->stream));
+    if ((rc = reset_flag(ctx))) return rc;
+    ZL_CUDA(ctx, launch_mark_present((const uint64_t*)dcodes.ptr, n, map, geo, (uint32_t*)L.info.ptr,
+                                     (int*)ctx->scratch_flag.ptr, ctx->stream));
+    DeviceBuffer dcount;
+    if ((rc = alloc(ctx, dcount, sizeof(unsigned long long)))) return rc;
+    ZL_CUDA(ctx, cudaMemsetAsync(dcount.ptr, 0, sizeof(unsigned long long), ctx->stream));
+    ZL_CUDA(ctx, launch_count_present((const uint32_t*)L.info.ptr, cells, (unsigned long long*)dcount.ptr,
+                                      ctx->stream));
+    unsigned long long present = 0;
+    ZL_CUDA(ctx, cudaMemcpyAsync(&present, dcount.ptr, sizeof(present), cudaMemcpyDeviceToHost, ctx->stream));
+    int bad = 0;
+    if ((rc = read_flag(ctx, &bad))) return rc;
+    if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
+    const long long box_nodes = (long long)geo.n[0] * geo.n[1] * geo.n[2];
+    if ((long long)present == box_nodes) {
+        L.info.release();
+    } else {
+        geo.info = (const uint32_t*)L.info.ptr;
+        launch_node_info(dims, geo, (uint32_t*)L.info.ptr, ctx->stream);
+        ZL_CUDA(ctx, cudaGetLastError());
+    }
+    L.nodes = (long long)present;
+    L.bnd = false;
+    for (int a = 0; a < dims; ++a)
+        if (!geo.periodic[a]) L.bnd = true;
+
+    // parameters (relaxation time per level: lbm_collision_models.cpp:105-118)
+    StepParams& p = L.params;
+    std::memset(&p, 0, sizeof(p));
+    const double dt = 1. / (double)(1u << level);
+    p.tau = ctx->cfg.viscosity * 3. / dt + 0.5;
+    p.rho0 = ctx->cfg.rho0;
+    for (int f = 0; f < 6; ++f) p.face_kind[f] = ctx->cfg.bc_kind[f];
+    for (int f = 0; f < 2 * dims; ++f) {
+        const double* U = ctx->cfg.bc_velocity[f];
+        for (int o = 0; o < q; ++o) {
+            const double cx = lattice_c(dims, o, 0), cy = lattice_c(dims, o, 1), cz = lattice_c(dims, o, 2);
+            const double cu = dims == 2 ? cx * U[0] + cy * U[1] : cx * U[0] + cy * U[1] + cz * U[2];
+            p.bb_term[f][o] = 6 * ctx->cfg.rho0 * lattice_w(dims, o) * cu;
+        }
+    }
+    for (int k = 0; k < q; ++k) {
+        const double sk = lattice_s(dims, k);
+        p.mrt_coef[k] = (float)((sk < 0. ? 1. / p.tau : sk) / (double)lattice_norm2(dims, k));
+    }
+    const double scale = ctx->cfg.storage_scale > 0. ? ctx->cfg.storage_scale : 8192.;
+    p.scale = ctx->cfg.storage == ZL_STORAGE_F16 || ctx->cfg.storage == ZL_STORAGE_BF16 ? (float)scale : 1.f;
+    p.inv_scale = 1.f / p.scale;
+    if (ctx->cfg.collision == ZL_MRT && ctx->cfg.storage == ZL_STORAGE_F64) {
+        std::vector<double> m(q * q);
+        host_mrt_matrix(dims, 1. / p.tau, false, m.data());
+        if ((rc = alloc(ctx, L.mrt64, m.size() * sizeof(double)))) return rc;
+        ZL_CUDA(ctx, cudaMemcpy(L.mrt64.ptr, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
+        p.mrt64 = (const double*)L.mrt64.ptr;
+    }
+    std::vector<double> feq_face(6 * q, 0.);
+    for (int f = 0; f < 2 * dims; ++f) host_feq(dims, ctx->cfg.rho0, ctx->cfg.bc_velocity[f], &feq_face[f * q]);
+    if ((rc = alloc(ctx, L.feq_face, feq_face.size() * sizeof(double)))) return rc;
+    ZL_CUDA(ctx, cudaMemcpy(L.feq_face.ptr, feq_face.data(), feq_face.size() * sizeof(double), cudaMemcpyHostToDevice));
+
+    // populations: every slot starts at feq(rho0, default velocity)
+    if ((rc = alloc(ctx, L.f, (size_t)q * geo.stride * ctx->ops->elem_bytes))) return rc;
+    std::vector<double> f0(q);
+    host_feq(dims, ctx->cfg.rho0, ctx->cfg.init_velocity, f0.data());
+    if (ctx->cfg.storage != ZL_STORAGE_F64)
+        for (int k = 0; k < q; ++k) f0[k] -= lattice_w(dims, k);
+    DeviceBuffer dval;
+    if ((rc = alloc(ctx, dval, q * sizeof(double)))) return rc;
+    ZL_CUDA(ctx, cudaMemcpy(dval.ptr, f0.data(), q * sizeof(double), cudaMemcpyHostToDevice));
+    ZL_CUDA(ctx, launch_fill(ctx->cfg.storage, L.f.ptr, geo.stride, q, p, (const double*)dval.ptr, ctx->stream));
+
+    L.partial_blocks = 148 * 4;
+    if ((rc = alloc(ctx, L.partial, (size_t)L.partial_blocks * 4 * sizeof(double) + 4 * sizeof(double)))) return rc;
+
+    L.geo = geo;
+    L.map = map;
+    L.even_layout = 0;
+    L.steps = 0;
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    L.active = true;
+    return ZL_OK;
+}
+
+static int exchange(zl_ctx* ctx, int level, const uint64_t* codes, double* f_host, double* rho, double* u, int64_t n,
+                    bool write) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (n < 0 || (n > 0 && !codes)) return fail(ctx, ZL_EINVAL, "bad node list");
+    if (n == 0) return ZL_OK;
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    Level& L = ctx->levels[level];
+    const int q = ctx->q, dims = ctx->dims;
+    DeviceBuffer dcodes, dbuf, dmac;
+    if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
+    if ((rc = reset_flag(ctx))) return rc;
+    if (write) {
+        if ((rc = alloc(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
+        ZL_CUDA(ctx, cudaMemcpyAsync(dbuf.ptr, f_host, (size_t)n * q * 8, cudaMemcpyHostToDevice, ctx->stream));
+        ZL_CUDA(ctx, ctx->ops->scatter(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
+                                       (const uint64_t*)dcodes.ptr, (const double*)dbuf.ptr, n,
+                                       (int*)ctx->scratch_flag.ptr, ctx->stream));
+    } else {
+        if (f_host && (rc = alloc(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
+        if (rho && (rc = alloc(ctx, dmac, (size_t)n * (dims + 1) * sizeof(double)))) return rc;
+        double* drho = rho ? (double*)dmac.ptr : nullptr;
+        double* du = rho ? drho + n : nullptr;
+        ZL_CUDA(ctx, ctx->ops->gather(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
+                                      (const uint64_t*)dcodes.ptr, (double*)dbuf.ptr, drho, du, n,
+                                      (int*)ctx->scratch_flag.ptr, ctx->stream));
+        if (f_host)
+            ZL_CUDA(ctx, cudaMemcpyAsync(f_host, dbuf.ptr, (size_t)n * q * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        if (rho) {
+            ZL_CUDA(ctx, cudaMemcpyAsync(rho, drho, (size_t)n * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            if (u) ZL_CUDA(ctx, cudaMemcpyAsync(u, du, (size_t)n * dims * 8, cudaMemcpyDeviceToHost, ctx->stream));
+        }
+    }
+    int bad = 0;
+    if ((rc = read_flag(ctx, &bad))) return rc;
+    if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code is not part of the level", level);
+    return ZL_OK;
+}
+
+int zl_set_populations(zl_ctx* ctx, int level, const uint64_t* codes, const double* f, int64_t n) {
+    if (n > 0 && !f) return ZL_EINVAL;
+    return exchange(ctx, level, codes, const_cast<double*>(f), nullptr, nullptr, n, true);
+}
+
+int zl_get_populations(zl_ctx* ctx, int level, const uint64_t* codes, double* f, int64_t n) {
+    if (n > 0 && !f) return ZL_EINVAL;
+    return exchange(ctx, level, codes, f, nullptr, nullptr, n, false);
+}
+
+int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, double* u, int64_t n) {
+    if (n > 0 && !rho) return ZL_EINVAL;
+    return exchange(ctx, level, codes, nullptr, rho, u, n, false);
+}
+
+int zl_step_level(zl_ctx* ctx, int level) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    const bool odd = L.even_layout == 1;
+    ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr, L.geo,
+                                L.params, ctx->stream));
+    L.even_layout ^= 1;
+    // non-equilibrium extrapolation faces, in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
+    for (int k = 0; k < 2 * ctx->dims; ++k) {
+        const int face = k < ctx->dims ? 2 * k : 2 * (k - ctx->dims) + 1;
+        if (ctx->cfg.bc_kind[face] != ZL_BC_NONEQ_EXTRAPOLATION) continue;
+        if (!((L.geo.face_on_box >> face) & 1)) continue;
+        ZL_CUDA(ctx, ctx->ops->neq(ctx->dims, L.f.ptr, L.geo, L.params, face, L.even_layout,
+                                   (const double*)L.feq_face.ptr + face * ctx->q, ctx->stream));
+    }
+    ++L.steps;
+    return ZL_OK;
+}
+
+int zl_advance(zl_ctx* ctx, int steps) {
+    if (!ctx || steps < 0) return ZL_EINVAL;
+    if (ctx->cfg.max_level != 0)
+        return fail(ctx, ZL_ESTATE, "multi-level stepping needs the coarse/fine transfer set-up");
+    for (int s = 0; s < steps; ++s) {
+        int rc = zl_step_level(ctx, 0);
+        if (rc) return rc;
+    }
+    return ZL_OK;
+}
+
+int zl_conservation(zl_ctx* ctx, int level, double* out) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (!out) return ZL_EINVAL;
+    Level& L = ctx->levels[level];
+    double* partial = (double*)L.partial.ptr;
+    double* result = partial + (size_t)L.partial_blocks * 4;
+    ZL_CUDA(ctx, ctx->ops->conservation(ctx->dims, L.f.ptr, L.geo, L.params, L.even_layout, partial,
+                                        L.partial_blocks, result, ctx->stream));
+    double host[4];
+    ZL_CUDA(ctx, cudaMemcpyAsync(host, result, sizeof(host), cudaMemcpyDeviceToHost, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    for (int k = 0; k <= ctx->dims; ++k) out[k] = host[k];
+    for (int k = 0; k <= ctx->dims; ++k)
+        if (!std::isfinite(host[k])) return fail(ctx, ZL_ENAN, "non-finite conservation sum on level %d", level);
+    return ZL_OK;
+}
+
+int zl_synchronize(zl_ctx* ctx) {
+    if (!ctx) return ZL_EINVAL;
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return ZL_OK;
+}
+
+int zl_get_stream(const zl_ctx* ctx, void** stream) {
+    if (!ctx || !stream) return ZL_EINVAL;
+    *stream = (void*)ctx->stream;
+    return ZL_OK;
+}
+
+int zl_set_stream(zl_ctx* ctx, void* stream) {
+    if (!ctx) return ZL_EINVAL;
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return ZL_OK;
+}
+
+int zl_last_error(const zl_ctx* ctx, char* buf, size_t n) {
+    if (!ctx || !buf || n == 0) return ZL_EINVAL;
+    std::snprintf(buf, n, "%s", ctx->last_error.c_str());
+    return ZL_OK;
+}
+
+int zl_level_info(const zl_ctx* ctx, int level, int64_t* nodes, int32_t* extent, int64_t* pop_bytes) {
+    if (!ctx || level < 0 || level >= ZL_MAX_LEVELS) return ZL_EINVAL;
+    const Level& L = ctx->levels[level];
+    if (nodes) *nodes = L.active ? L.nodes : 0;
+    if (extent)
+        for (int a = 0; a < 3; ++a) extent[a] = L.active ? L.geo.n[a] : 0;
+    if (pop_bytes) *pop_bytes = L.active ? (int64_t)L.f.bytes : 0;
+    return ZL_OK;
+}
+
+int zl_morton_neighbors(int dims, const uint64_t* codes, int64_t n, uint64_t* out) {
+    if ((dims != 2 && dims != 3) || n < 0 || (n > 0 && (!codes || !out))) return ZL_EINVAL;
+    if (n == 0) return ZL_OK;
+    uint64_t *dc = nullptr, *dout = nullptr;
+    if (cudaMalloc(&dc, n * 8) != cudaSuccess) return ZL_EDEVICE;
+    if (cudaMalloc(&dout, n * 2 * dims * 8) != cudaSuccess) {
+        cudaFree(dc);
+        return ZL_EDEVICE;
+    }
+    int rc = ZL_OK;
+    if (cudaMemcpy(dc, codes, n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+        launch_morton_neighbors(dc, n, dims, dout, 0) != cudaSuccess ||
+        cudaMemcpy(out, dout, n * 2 * dims * 8, cudaMemcpyDeviceToHost) != cudaSuccess)
+        rc = ZL_EDEVICE;
+    cudaFree(dc);
+    cudaFree(dout);
+    return rc;
+}
+
+int zl_upstream_index(int lattice, const uint64_t* codes, int64_t n, int64_t* out) {
+    if ((lattice != ZL_D2Q9 && lattice != ZL_D3Q19) || n < 0 || (n > 0 && (!codes || !out))) return ZL_EINVAL;
+    if (n == 0) return ZL_OK;
+    const int dims = lattice == ZL_D2Q9 ? 2 : 3, q = dims == 2 ? 9 : 19;
+    // sort codes on the host side of the call (set-up path), resolve on the device
+    std::vector<std::pair<uint64_t, long long>> order(n);
+    for (int64_t i = 0; i < n; ++i) order[i] = {codes[i], (long long)i};
+    std::sort(order.begin(), order.end());
+    std::vector<uint64_t> sorted(n);
+    std::vector<long long> pos(n);
+    for (int64_t i = 0; i < n; ++i) {
+        sorted[i] = order[i].first;
+        pos[i] = order[i].second;
+    }
+    uint64_t* ds = nullptr;
+    long long *dp = nullptr, *dout = nullptr;
+    int rc = ZL_OK;
+    if (cudaMalloc(&ds, n * 8) != cudaSuccess || cudaMalloc(&dp, n * 8) != cudaSuccess ||
+        cudaMalloc(&dout, (size_t)n * q * 8) != cudaSuccess) {
+        rc = ZL_EDEVICE;
+    } else if (cudaMemcpy(ds, sorted.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+               cudaMemcpy(dp, pos.data(), n * 8, cudaMemcpyHostToDevice) != cudaSuccess ||
+               launch_upstream_index(dims, ds, dp, n, dout, 0) != cudaSuccess ||
+               cudaMemcpy(out, dout, (size_t)n * q * 8, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        rc = ZL_EDEVICE;
+    }
+    if (ds) cudaFree(ds);
+    if (dp) cudaFree(dp);
+    if (dout) cudaFree(dout);
+    return rc;
+}
+
+int zl_mrt_matrix(int lattice, double tau, double* out) {
+    if ((lattice != ZL_D2Q9 && lattice != ZL_D3Q19) || !out || !(tau > 0.)) return ZL_EINVAL;
+    host_mrt_matrix(lattice == ZL_D2Q9 ? 2 : 3, 1. / tau, false, out);
+    return ZL_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,128 @@
+// Host-side launchers for one population storage type.  Each storage type is
+// compiled in its own translation unit (the FP64 one with -fmad=false, so its
+// arithmetic follows the reference's rounding step for step).
+#pragma once
+#include <cuda_runtime.h>
+#include "level_ops.cuh"
+
+namespace zl {
+
+struct LaunchSet {
+    int elem_bytes;
+    cudaError_t (*step)(int dims, int coll, bool odd, bool bnd, bool masked, void* f, const LevelGeom& geo,
+                        const StepParams& p, cudaStream_t s);
+    cudaError_t (*neq)(int dims, void* f, const LevelGeom& geo, const StepParams& p, int face, int even_layout,
+                       const double* feq_b, cudaStream_t s);
+    cudaError_t (*scatter)(int dims, void* f, const LevelGeom& geo, const StepParams& p, const LevelMap& m,
+                           int even_layout, const uint64_t* codes, const double* fin, long long n, int* bad,
+                           cudaStream_t s);
+    cudaError_t (*gather)(int dims, const void* f, const LevelGeom& geo, const StepParams& p, const LevelMap& m,
+                          int even_layout, const uint64_t* codes, double* fout, double* rho, double* u, long long n,
+                          int* bad, cudaStream_t s);
+    cudaError_t (*conservation)(int dims, const void* f, const LevelGeom& geo, const StepParams& p,
+                                int even_layout, double* partial, int nblocks, double* out, cudaStream_t s);
+};
+
+const LaunchSet& launch_set_f64();
+const LaunchSet& launch_set_f32();
+const LaunchSet& launch_set_f16();
+const LaunchSet& launch_set_bf16();
+
+// Block size and grid of the fused step: one thread per node, x fastest.
+inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) {
+    int bx = 256;
+    while (bx > 32 && bx / 2 >= geo.n[0]) bx /= 2;
+    block = dim3(bx, 1, 1);
+    grid = dim3((geo.n[0] + bx - 1) / bx, geo.n[1], dims == 3 ? geo.n[2] : 1);
+}
+
+#define ZL_DEFINE_LAUNCH_SET(NAME, S)                                                                            \
+    namespace NAME##_impl {                                                                                      \
+    template <class L, int C, bool O, bool B, bool M>                                                            \
+    cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {                      \
+        dim3 g, b;                                                                                               \
+        step_shape(geo, L::kDims, g, b);                                                                         \
+        aa_step_kernel<L, S, C, O, B, M><<<g, b, 0, s>>>(f, geo, p);                                             \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    template <class L, int C>                                                                                    \
+    cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,        \
+                        cudaStream_t s) {                                                                        \
+        if (masked) {                                                                                            \
+            return odd ? step_one<L, C, true, true, true>(f, geo, p, s)                                          \
+                       : step_one<L, C, false, true, true>(f, geo, p, s);                                        \
+        }                                                                                                        \
+        if (bnd) {                                                                                               \
+            return odd ? step_one<L, C, true, true, false>(f, geo, p, s)                                         \
+                       : step_one<L, C, false, true, false>(f, geo, p, s);                                       \
+        }                                                                                                        \
+        return odd ? step_one<L, C, true, false, false>(f, geo, p, s)                                            \
+                   : step_one<L, C, false, false, false>(f, geo, p, s);                                          \
+    }                                                                                                            \
+    cudaError_t step_any(int dims, int coll, bool odd, bool bnd, bool masked, void* fv, const LevelGeom& geo,    \
+                         const StepParams& p, cudaStream_t s) {                                                  \
+        S* f = static_cast<S*>(fv);                                                                              \
+        if (dims == 2)                                                                                           \
+            return coll == kMrt ? step_lc<D2Q9, kMrt>(odd, bnd, masked, f, geo, p, s)                            \
+                                : step_lc<D2Q9, kSrt>(odd, bnd, masked, f, geo, p, s);                           \
+        return coll == kMrt ? step_lc<D3Q19, kMrt>(odd, bnd, masked, f, geo, p, s)                               \
+                            : step_lc<D3Q19, kSrt>(odd, bnd, masked, f, geo, p, s);                              \
+    }                                                                                                            \
+    cudaError_t neq_any(int dims, void* fv, const LevelGeom& geo, const StepParams& p, int face, int even,       \
+                        const double* feq_b, cudaStream_t s) {                                                   \
+        S* f = static_cast<S*>(fv);                                                                              \
+        const int axis = face >> 1;                                                                              \
+        const int o0 = axis == 0 ? 1 : 0, o1 = axis == 2 ? 1 : 2;                                                \
+        const int n0 = geo.n[o0], n1 = dims == 3 ? geo.n[o1] : 1;                                                \
+        dim3 b(128), g((n0 + 127) / 128, n1);                                                                    \
+        if (dims == 2)                                                                                           \
+            neq_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even, feq_b);                              \
+        else                                                                                                     \
+            neq_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even, feq_b);                             \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    cudaError_t scatter_any(int dims, void* fv, const LevelGeom& geo, const StepParams& p, const LevelMap& m,    \
+                            int even, const uint64_t* codes, const double* fin, long long n, int* bad,           \
+                            cudaStream_t s) {                                                                    \
+        if (n <= 0) return cudaSuccess;                                                                          \
+        S* f = static_cast<S*>(fv);                                                                              \
+        const unsigned blocks = (unsigned)((n + 255) / 256);                                                     \
+        if (dims == 2)                                                                                           \
+            scatter_kernel<D2Q9, S><<<blocks, 256, 0, s>>>(f, geo, p, m, even, codes, fin, n, bad);              \
+        else                                                                                                     \
+            scatter_kernel<D3Q19, S><<<blocks, 256, 0, s>>>(f, geo, p, m, even, codes, fin, n, bad);             \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    cudaError_t gather_any(int dims, const void* fv, const LevelGeom& geo, const StepParams& p,                  \
+                           const LevelMap& m, int even, const uint64_t* codes, double* fout, double* rho,        \
+                           double* u, long long n, int* bad, cudaStream_t s) {                                   \
+        if (n <= 0) return cudaSuccess;                                                                          \
+        const S* f = static_cast<const S*>(fv);                                                                  \
+        const unsigned blocks = (unsigned)((n + 255) / 256);                                                     \
+        if (dims == 2)                                                                                           \
+            gather_kernel<D2Q9, S><<<blocks, 256, 0, s>>>(f, geo, p, m, even, codes, fout, rho, u, n, bad);        \
+        else                                                                                                     \
+            gather_kernel<D3Q19, S><<<blocks, 256, 0, s>>>(f, geo, p, m, even, codes, fout, rho, u, n, bad);       \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    cudaError_t conservation_any(int dims, const void* fv, const LevelGeom& geo, const StepParams& p, int even,  \
+                                 double* partial, int nblocks, double* out, cudaStream_t s) {                    \
+        const S* f = static_cast<const S*>(fv);                                                                  \
+        if (dims == 2)                                                                                           \
+            conservation_partial_kernel<D2Q9, S><<<nblocks, 256, 0, s>>>(f, geo, p, even, partial);              \
+        else                                                                                                     \
+            conservation_partial_kernel<D3Q19, S><<<nblocks, 256, 0, s>>>(f, geo, p, even, partial);             \
+        cudaError_t e = cudaGetLastError();                                                                      \
+        if (e != cudaSuccess) return e;                                                                          \
+        conservation_final_kernel<<<1, 32, 0, s>>>(partial, nblocks, out);                                       \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    }                                                                                                            \
+    const LaunchSet& NAME() {                                                                                    \
+        static const LaunchSet set = {(int)sizeof(S), NAME##_impl::step_any, NAME##_impl::neq_any,                \
+                                      NAME##_impl::scatter_any, NAME##_impl::gather_any,                         \
+                                      NAME##_impl::conservation_any};                                            \
+        return set;                                                                                              \
+    }
+
+}  // namespace zl

@@ -1,0 +1,251 @@
+// Per-level kernels other than the fused step: non-equilibrium extrapolation
+// faces, host <-> device population exchange in the reference's node order,
+// macroscopic fields and FP64 conservation sums.
+#pragma once
+#include "aa_kernel.cuh"
+
+namespace zl {
+
+// Mapping from a reference Morton code to this level's node coordinates.
+struct LevelMap {
+    int dims;
+    int lo[3];        // reference index of node coordinate 0 (at this level)
+    int n[3];
+    int periodic[3];  // a periodic axis stores the max plane folded onto coordinate 0
+};
+
+// Bit-exact restatement of SFBitsetComputeIndices (amr_project/grid/morton_aux.cpp:107-119, :336-351).
+ZL_HD void morton_decode(uint64_t code, int dims, uint32_t* idx) {
+    idx[0] = idx[1] = idx[2] = 0;
+    const int nbits = 64 / dims;
+    for (int i = 0; i < nbits; ++i)
+        for (int a = 0; a < dims; ++a) idx[a] |= (uint32_t)((code >> (dims * i + a)) & 1ull) << i;
+}
+
+ZL_HD uint64_t morton_encode(const uint32_t* idx, int dims) {
+    uint64_t code = 0;
+    const int nbits = 64 / dims;
+    for (int i = 0; i < nbits; ++i)
+        for (int a = 0; a < dims; ++a) code |= (uint64_t)((idx[a] >> i) & 1u) << (dims * i + a);
+    return code;
+}
+
+__device__ __forceinline__ bool code_to_node(uint64_t code, const LevelMap& m, Coord& c) {
+    uint32_t idx[3];
+    morton_decode(code, m.dims, idx);
+    c.x[2] = 0;
+    for (int a = 0; a < m.dims; ++a) {
+        int v = (int)idx[a] - m.lo[a];
+        if (m.periodic[a] && v == m.n[a]) v = 0;
+        if (v < 0 || v >= m.n[a]) return false;
+        c.x[a] = v;
+    }
+    return true;
+}
+
+// ---------------------------------------------------------------- deviation-form helpers
+template <class L>
+__device__ __forceinline__ void macro_dev(const float* d, float& rho, float& ux, float& uy, float& uz) {
+    using Tb = Tables<L>;
+    float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
+#pragma unroll
+    for (int q = 0; q < L::kQ; ++q) {
+        drho += d[q];
+        if (Tb::cx(q)) jx += Tb::cx(q) == 1 ? d[q] : -d[q];
+        if (Tb::cy(q)) jy += Tb::cy(q) == 1 ? d[q] : -d[q];
+        if (L::kDims == 3 && Tb::cz(q)) jz += Tb::cz(q) == 1 ? d[q] : -d[q];
+    }
+    rho = 1.f + drho;
+    ux = jx / rho;
+    uy = jy / rho;
+    uz = jz / rho;
+}
+
+template <class L>
+__device__ __forceinline__ void feq_dev(float rho, float ux, float uy, float uz, float* deq) {
+    using Tb = Tables<L>;
+    const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
+#pragma unroll
+    for (int q = 0; q < L::kQ; ++q) {
+        const float cu = Tb::cx(q) * ux + Tb::cy(q) * uy + Tb::cz(q) * uz;
+        deq[q] = (float)Tb::w(q) * ((rho - 1.f) + rho * (3.f * cu + 4.5f * cu * cu - usq15));
+    }
+}
+
+// ---------------------------------------------------------------- NEQ extrapolation
+// lbm_project/boundary_conditions/lbm_noneq_extrapolation.cpp:89-144: every population of a
+// face node becomes feq(rho0, U_face) + f(inner) - feq(rho(inner), u(inner)), using the inner
+// node's post-stream populations.  One launch per face, in the reference's face order.
+template <class L, class S>
+__global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout,
+                                const double* __restrict__ feq_b) {
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    const int axis = face >> 1;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;  // coordinate along first other axis
+    const int t1 = blockIdx.y;                             // along second other axis (3D)
+    const int o0 = axis == 0 ? 1 : 0;
+    const int o1 = axis == 2 ? 1 : 2;
+    if (t0 >= geo.n[o0]) return;
+    if (L::kDims == 3 && t1 >= geo.n[o1]) return;
+    Coord c;
+    c.x[2] = 0;
+    c.x[axis] = (face & 1) ? geo.n[axis] - 1 : 0;
+    c.x[o0] = t0;
+    if (L::kDims == 3) c.x[o1] = t1;
+    const long long self = (long long)(c.x[0] + geo.g[0]) +
+                           (long long)geo.a[0] * ((c.x[1] + geo.g[1]) + (long long)geo.a[1] * (c.x[2] + geo.g[2]));
+    if (geo.info && !(__ldg(geo.info + self) & kInfoPresent)) return;
+    Coord ci = c;
+    ci.x[axis] += (face & 1) ? -1 : 1;
+    if (geo.info) {
+        const long long inner = (long long)(ci.x[0] + geo.g[0]) +
+                                (long long)geo.a[0] * ((ci.x[1] + geo.g[1]) + (long long)geo.a[1] * (ci.x[2] + geo.g[2]));
+        if (!(__ldg(geo.info + inner) & kInfoPresent)) return;
+    }
+    T fi[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) fi[q] = St::load(f + post_stream_slot<L>(geo, ci, q, even_layout), p);
+    if constexpr (St::kDeviation) {
+        float rho, ux, uy, uz, deq[Q];
+        macro_dev<L>(fi, rho, ux, uy, uz);
+        feq_dev<L>(rho, ux, uy, uz, deq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float db = (float)(feq_b[q] - Tables<L>::w(q));
+            St::store(f + post_stream_slot<L>(geo, c, q, even_layout), db + fi[q] - deq[q], p);
+        }
+    } else {
+        double rho, ux, uy, uz, feq[Q];
+        macro_exact<L>(fi, rho, ux, uy, uz);
+        feq_exact<L>(rho, ux, uy, uz, feq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+            St::store(f + post_stream_slot<L>(geo, c, q, even_layout), (feq_b[q] + fi[q]) - feq[q], p);
+    }
+}
+
+// ---------------------------------------------------------------- host exchange
+template <class L, class S>
+__global__ void scatter_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, LevelMap m, int even_layout,
+                               const uint64_t* __restrict__ codes, const double* __restrict__ fin, long long n,
+                               int* __restrict__ bad) {
+    using St = Storage<S>;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Coord c;
+    if (!code_to_node(codes[i], m, c)) {
+        atomicExch(bad, 1);
+        return;
+    }
+    for (int q = 0; q < L::kQ; ++q) {
+        double v = fin[i * L::kQ + q];
+        if constexpr (St::kDeviation) v -= Tables<L>::w(q);
+        St::store(f + post_stream_slot<L>(geo, c, q, even_layout), (typename St::T)v, p);
+    }
+}
+
+template <class L, class S>
+__global__ void gather_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, LevelMap m, int even_layout,
+                              const uint64_t* __restrict__ codes, double* __restrict__ fout, double* __restrict__ rho_out,
+                              double* __restrict__ u_out, long long n, int* __restrict__ bad) {
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    constexpr int D = L::kDims;
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Coord c;
+    if (!code_to_node(codes[i], m, c)) {
+        atomicExch(bad, 1);
+        return;
+    }
+    T v[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) v[q] = St::load(f + post_stream_slot<L>(geo, c, q, even_layout), p);
+    if (fout) {
+        for (int q = 0; q < Q; ++q) {
+            double x = (double)v[q];
+            if constexpr (St::kDeviation) x += Tables<L>::w(q);
+            fout[i * Q + q] = x;
+        }
+    }
+    if (rho_out) {
+        // velocity recomputed from post-boundary f, as the reference's output does
+        // (lbm_grid_interface.cpp:614-657)
+        if constexpr (St::kDeviation) {
+            float rho, ux, uy, uz;
+            macro_dev<L>(v, rho, ux, uy, uz);
+            rho_out[i] = rho;
+            u_out[i * D] = ux;
+            u_out[i * D + 1] = uy;
+            if (D == 3) u_out[i * D + 2] = uz;
+        } else {
+            double rho, ux, uy, uz;
+            macro_exact<L>(v, rho, ux, uy, uz);
+            rho_out[i] = rho;
+            u_out[i * D] = ux;
+            u_out[i * D + 1] = uy;
+            if (D == 3) u_out[i * D + 2] = uz;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- FP64 conservation sums
+// Mass and momentum of every node of the level, accumulated in FP64: one partial per
+// block into `partial`, then a single-block pass adds the partials in a fixed order
+// (deterministic result for a given launch shape).
+template <class L, class S>
+__global__ void __launch_bounds__(256) conservation_partial_kernel(const S* __restrict__ f, LevelGeom geo,
+                                                                   StepParams p, int even_layout,
+                                                                   double* __restrict__ partial) {
+    using St = Storage<S>;
+    constexpr int Q = L::kQ;
+    __shared__ double red[4][256 / 32];
+    double acc[4] = {0., 0., 0., 0.};
+    const long long total = (long long)geo.n[0] * geo.n[1] * (L::kDims == 3 ? geo.n[2] : 1);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        Coord c;
+        c.x[0] = (int)(i % geo.n[0]);
+        c.x[1] = (int)((i / geo.n[0]) % geo.n[1]);
+        c.x[2] = L::kDims == 3 ? (int)(i / ((long long)geo.n[0] * geo.n[1])) : 0;
+        if (geo.info) {
+            const long long self = (long long)(c.x[0] + geo.g[0]) +
+                                   (long long)geo.a[0] * ((c.x[1] + geo.g[1]) + (long long)geo.a[1] * (c.x[2] + geo.g[2]));
+            if (!(__ldg(geo.info + self) & kInfoPresent)) continue;
+        }
+        double rho = 0., jx = 0., jy = 0., jz = 0.;
+        for (int q = 0; q < Q; ++q) {
+            double v = (double)St::load(f + post_stream_slot<L>(geo, c, q, even_layout), p);
+            if constexpr (St::kDeviation) v += Tables<L>::w(q);
+            rho += v;
+            jx += Tables<L>::cx(q) * v;
+            jy += Tables<L>::cy(q) * v;
+            jz += Tables<L>::cz(q) * v;
+        }
+        acc[0] += rho;
+        acc[1] += jx;
+        acc[2] += jy;
+        acc[3] += jz;
+    }
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        double v = acc[k];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        double v = 0.;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += red[threadIdx.x][w];
+        partial[blockIdx.x * 4 + threadIdx.x] = v;
+    }
+}
+
+__global__ void conservation_final_kernel(const double* __restrict__ partial, int nblocks, double* __restrict__ out);
+
+}  // namespace zl
