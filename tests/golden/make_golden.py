@@ -52,6 +52,14 @@ CASES = {
     "box3d_mixed": (LevelConfig(dims=3, n=(10, 8, 9), collision=MRT, nu=0.05,
                                 bc_kind=(BC_NONEQ, BC_NONEQ, BC_BOUNCE_BACK, BC_BOUNCE_BACK, BC_PERIODIC, BC_PERIODIC),
                                 bc_vel=((0.05, 0, 0), (0.05, 0, 0), Z3, (0.03, 0, 0.01), Z3, Z3)), 30, "eq"),
+    # bounce back with moving walls next to a periodic axis (device wraps the periodic axis)
+    "box3d_bbper": (LevelConfig(dims=3, n=(9, 10, 8), collision=SRT, nu=0.04,
+                                bc_kind=(BC_BOUNCE_BACK, BC_BOUNCE_BACK, BC_BOUNCE_BACK, BC_BOUNCE_BACK,
+                                         BC_PERIODIC, BC_PERIODIC),
+                                bc_vel=((0, 0.02, 0), Z3, Z3, (0.05, 0, 0.02), Z3, Z3)), 40, "eq"),
+    "channel2d_per": (LevelConfig(dims=2, n=(14, 11), collision=MRT, nu=0.03,
+                                  bc_kind=(BC_PERIODIC, BC_PERIODIC, BC_BOUNCE_BACK, BC_BOUNCE_BACK, 0, 0),
+                                  bc_vel=(Z3, Z3, Z3, (0.08, 0, 0), Z3, Z3)), 80, "eq"),
 }
 
 

@@ -49,9 +49,11 @@ struct StepParams {
     int face_kind[6];       // BcKind per face
     double bb_term[6][19];  // 6 rho0 w_o (c_o . U_face) for outgoing direction o
     const double* mrt64;    // dense M^-1 S M, reference construction order (FP64 mode)
-    float mrt_coef[19];     // S_k / |M_k|^2 per moment (fast path)
+    float mrt_coef[19];     // (s_k - 1/tau) / |M_k|^2 per non-shear moment, 0 elsewhere (fast path)
+    float omega32;          // 1/tau in FP32 (fast path)
     float inv_scale;        // reduced storage: deviation = stored * inv_scale
     float scale;
+    int fuse_bb;            // bounce back applied inside the step kernel (no ordered face passes needed)
 };
 
 // ---------------------------------------------------------------- storage
@@ -173,8 +175,14 @@ __device__ __forceinline__ void collide_exact(const double* f, double* out, cons
 }
 
 // Fast path on deviations d_q = f_q - w_q, FP32 arithmetic.
+//
+// MRT as f* = f - S_nu neq - sum_k lambda_k m_k M_k^T over the moments whose rate differs
+// from the shear rate S_nu = 1/tau (the basis is orthogonal, so the shear moments fold into
+// the first term); lambda_k = (s_k - 1/tau) / |M_k|^2 and m_k = M_k . neq.  The conserved
+// moments of neq vanish and are skipped.
 template <class L>
-__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll) {
+__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float& omega_unused) {
+    (void)omega_unused;
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
@@ -189,25 +197,119 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
     const float inv_rho = 1.f / rho;
     const float ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
     const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-    float neq[Q];
+    // even part shared by opposite directions, odd part 3 rho (c.u) w
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
+        const int opp = Tb::opp(q);
+        if (opp < q) continue;
         const float cu = Tb::cx(q) * ux + Tb::cy(q) * uy + Tb::cz(q) * uz;
         const float w = (float)Tb::w(q);
-        const float deq = w * (drho + rho * (3.f * cu + 4.5f * cu * cu - usq15));
-        neq[q] = d[q] - deq;
+        const float even = w * (drho + rho * (4.5f * cu * cu - usq15));
+        if (q == 0) {
+            neq[0] = d[0] - even;
+        } else {
+            const float odd = w * rho * 3.f * cu;
+            neq[q] = d[q] - (even + odd);
+            neq[opp] = d[opp] - (even - odd);
+        }
     }
-    if (coll == kSrt) {
-        const float omega = (float)(1.0 / p.tau);
+}
+
+__device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, float* out, float omega,
+                                              const StepParams& p) {
+    // pair sums / differences over opposite directions
+    const float S1 = n[1] + n[2], D1 = n[1] - n[2];
+    const float S2 = n[3] + n[4], D2 = n[3] - n[4];
+    const float S3 = n[5] + n[6], D3 = n[5] - n[6];
+    const float S4 = n[7] + n[10], D4 = n[7] - n[10];
+    const float S5 = n[8] + n[9], D5 = n[8] - n[9];
+    const float S6 = n[11] + n[14], D6 = n[11] - n[14];
+    const float S7 = n[12] + n[13], D7 = n[12] - n[13];
+    const float S8 = n[15] + n[18], D8 = n[15] - n[18];
+    const float S9 = n[16] + n[17], D9 = n[16] - n[17];
+    const float Sa = S1 + S2 + S3;
+    const float Sxy = S4 + S5, Sxz = S6 + S7, Syz = S8 + S9;
+    const float Sd = Sxy + Sxz + Syz;
+    const float m1 = -30.f * n[0] - 11.f * Sa + 8.f * Sd;
+    const float m2 = 12.f * n[0] - 4.f * Sa + Sd;
+    const float m10 = -4.f * S1 + 2.f * (S2 + S3) + Sxy + Sxz - 2.f * Syz;
+    const float m12 = -2.f * S2 + 2.f * S3 + Sxy - Sxz;
+    const float X1 = D4 - D5, X2 = D6 - D7;
+    const float Y1 = D4 + D5, Y2 = D8 - D9;
+    const float Z1 = D6 + D7, Z2 = D8 + D9;
+    const float m4 = -4.f * D1 + X1 + X2, m16 = X1 - X2;
+    const float m6 = -4.f * D2 + Y1 + Y2, m17 = -Y1 + Y2;
+    const float m8 = -4.f * D3 + Z1 + Z2, m18 = Z1 - Z2;
+    // lambda_k = (s_k - omega) / |M_k|^2 (p.mrt_coef holds them per moment)
+    const float a1 = p.mrt_coef[1] * m1, a2 = p.mrt_coef[2] * m2;
+    const float a4 = p.mrt_coef[4] * m4, a6 = p.mrt_coef[6] * m6, a8 = p.mrt_coef[8] * m8;
+    const float a10 = p.mrt_coef[10] * m10, a12 = p.mrt_coef[12] * m12;
+    const float a16 = p.mrt_coef[16] * m16, a17 = p.mrt_coef[17] * m17, a18 = p.mrt_coef[18] * m18;
+    const float e_ax = -11.f * a1 - 4.f * a2;
+    const float e_dg = 8.f * a1 + a2;
+    float c[19];
+    c[0] = -30.f * a1 + 12.f * a2;
+    {
+        const float E = e_ax - 4.f * a10, O = -4.f * a4;
+        c[1] = E + O; c[2] = E - O;
+    }
+    {
+        const float E = e_ax + 2.f * a10 - 2.f * a12, O = -4.f * a6;
+        c[3] = E + O; c[4] = E - O;
+    }
+    {
+        const float E = e_ax + 2.f * a10 + 2.f * a12, O = -4.f * a8;
+        c[5] = E + O; c[6] = E - O;
+    }
+    const float e_xy = e_dg + a10 + a12, e_xz = e_dg + a10 - a12, e_yz = e_dg - 2.f * a10;
+    {
+        const float O = a4 + a6 + a16 - a17;   // q = 7 (+1,+1,0), opposite 10
+        c[7] = e_xy + O; c[10] = e_xy - O;
+    }
+    {
+        const float O = -a4 + a6 - a16 - a17;  // q = 8 (-1,+1,0), opposite 9
+        c[8] = e_xy + O; c[9] = e_xy - O;
+    }
+    {
+        const float O = a4 + a8 - a16 + a18;   // q = 11 (+1,0,+1), opposite 14
+        c[11] = e_xz + O; c[14] = e_xz - O;
+    }
+    {
+        const float O = -a4 + a8 + a16 + a18;  // q = 12 (-1,0,+1), opposite 13
+        c[12] = e_xz + O; c[13] = e_xz - O;
+    }
+    {
+        const float O = a6 + a8 + a17 - a18;   // q = 15 (0,+1,+1), opposite 18
+        c[15] = e_yz + O; c[18] = e_yz - O;
+    }
+    {
+        const float O = -a6 + a8 - a17 - a18;  // q = 16 (0,-1,+1), opposite 17
+        c[16] = e_yz + O; c[17] = e_yz - O;
+    }
 #pragma unroll
-        for (int q = 0; q < Q; ++q) out[q] = d[q] - omega * neq[q];
+    for (int q = 0; q < 19; ++q) out[q] = fmaf(-omega, n[q], d[q]) - c[q];
+}
+
+template <class L>
+__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll) {
+    using Tb = Tables<L>;
+    constexpr int Q = L::kQ;
+    float neq[Q];
+    float unused = 0.f;
+    feq_neq_dev<L>(d, neq, unused);
+    const float omega = p.omega32;
+    if (coll == kSrt) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] = fmaf(-omega, neq[q], d[q]);
+    } else if constexpr (L::kQ == 19) {
+        mrt_d3q19_dev(d, neq, out, omega, p);
     } else {
-        // m_k = M_k . neq for non-conserved moments, relaxed and mapped back with M^T / |M_k|^2
-        float mk[Q];
+        // generic orthogonal-basis MRT (D2Q9): m_k for non-shear moments, mapped back with M^T
+        float ak[Q];
 #pragma unroll
         for (int k = 0; k < Q; ++k) {
             float acc = 0.f;
-            if (Tb::s(k) != 0.) {
+            if (Tb::s(k) > 0.) {
 #pragma unroll
                 for (int j = 0; j < Q; ++j) {
                     const int m = Tb::M(k, j);
@@ -216,20 +318,20 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
                     else if (m != 0) acc += (float)m * neq[j];
                 }
             }
-            mk[k] = acc * p.mrt_coef[k];
+            ak[k] = acc * p.mrt_coef[k];
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             float acc = 0.f;
 #pragma unroll
             for (int k = 0; k < Q; ++k) {
-                if (Tb::s(k) == 0.) continue;
+                if (!(Tb::s(k) > 0.)) continue;
                 const int m = Tb::M(k, q);
-                if (m == 1) acc += mk[k];
-                else if (m == -1) acc -= mk[k];
-                else if (m != 0) acc += (float)m * mk[k];
+                if (m == 1) acc += ak[k];
+                else if (m == -1) acc -= ak[k];
+                else if (m != 0) acc += (float)m * ak[k];
             }
-            out[q] = d[q] - acc;
+            out[q] = fmaf(-omega, neq[q], d[q]) - acc;
         }
     }
 }
@@ -273,6 +375,7 @@ __device__ __forceinline__ int on_faces(const LevelGeom& geo, const Coord& c, in
 template <class L, class T>
 __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const T* post, const StepParams& p) {
     T v = pre[q];
+    if (!p.fuse_bb) return v;
 #pragma unroll
     for (int k = 0; k < 2 * L::kDims; ++k) {
         const int face = k < L::kDims ? 2 * k : 2 * (k - L::kDims) + 1;
@@ -301,19 +404,23 @@ __global__ void __launch_bounds__(256) aa_step_kernel(S* __restrict__ f, LevelGe
     c.x[2] = blockIdx.z;
     if (c.x[0] >= geo.n[0]) return;
 
-    // box coordinates of x-1, x, x+1 along each axis
-    int bx[3], by[3], bz[3];
+    // box coordinates of x-1, x, x+1 along each axis; cell indices fit in 32 bits (checked at set-up)
+    int bx[3], row[3][3];
+    {
+        int by[3], bz[3];
 #pragma unroll
-    for (int d = -1; d <= 1; ++d) {
-        bx[d + 1] = wrap_or_ghost(c.x[0] + d, geo.n[0], geo.g[0], geo.periodic[0]);
-        by[d + 1] = wrap_or_ghost(c.x[1] + d, geo.n[1], geo.g[1], geo.periodic[1]);
-        bz[d + 1] = L::kDims == 3 ? wrap_or_ghost(c.x[2] + d, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+        for (int d = -1; d <= 1; ++d) {
+            bx[d + 1] = wrap_or_ghost(c.x[0] + d, geo.n[0], geo.g[0], geo.periodic[0]);
+            by[d + 1] = wrap_or_ghost(c.x[1] + d, geo.n[1], geo.g[1], geo.periodic[1]);
+            bz[d + 1] = L::kDims == 3 ? wrap_or_ghost(c.x[2] + d, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+        }
+#pragma unroll
+        for (int dy = 0; dy < 3; ++dy)
+#pragma unroll
+            for (int dz = 0; dz < 3; ++dz) row[dy][dz] = geo.a[0] * (by[dy] + geo.a[1] * bz[dz]);
     }
-    const long long a0 = geo.a[0], a01 = (long long)geo.a[0] * geo.a[1];
-    auto cell = [&](int dx, int dy, int dz) -> long long {
-        return bx[dx + 1] + a0 * by[dy + 1] + a01 * bz[dz + 1];
-    };
-    const long long self = cell(0, 0, 0);
+    auto cell = [&](int dx, int dy, int dz) -> int { return bx[dx + 1] + row[dy + 1][dz + 1]; };
+    const int self = cell(0, 0, 0);
 
     uint32_t info = 0;
     if (Masked) {
@@ -374,6 +481,24 @@ __device__ __forceinline__ long long post_stream_slot(const LevelGeom& geo, cons
         dy = -Tb::cy(q);
         dz = -Tb::cz(q);
         plane = Tb::opp(q);
+    }
+    const long long bx = wrap_or_ghost(c.x[0] + dx, geo.n[0], geo.g[0], geo.periodic[0]);
+    const long long by = wrap_or_ghost(c.x[1] + dy, geo.n[1], geo.g[1], geo.periodic[1]);
+    const long long bz = L::kDims == 3 ? wrap_or_ghost(c.x[2] + dz, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+    return plane * geo.stride + bx + (long long)geo.a[0] * (by + (long long)geo.a[1] * bz);
+}
+
+// Slot holding the post-collision population f*(x, o) right after a step whose kernel
+// left the given layout: an even step stores it in slot(x, opp(o)), an odd step in slot(x + c_o, o).
+template <class L>
+__device__ __forceinline__ long long post_collision_slot(const LevelGeom& geo, const Coord& c, int o, bool even_layout) {
+    using Tb = Tables<L>;
+    int dx = 0, dy = 0, dz = 0, plane = Tb::opp(o);
+    if (!even_layout && o != 0) {
+        dx = Tb::cx(o);
+        dy = Tb::cy(o);
+        dz = Tb::cz(o);
+        plane = o;
     }
     const long long bx = wrap_or_ghost(c.x[0] + dx, geo.n[0], geo.g[0], geo.periodic[0]);
     const long long by = wrap_or_ghost(c.x[1] + dy, geo.n[1], geo.g[1], geo.periodic[1]);

@@ -5,7 +5,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
-#include "../../include/zllbm_b200.h"
+#include "zllbm_b200.h"
 #include "topology.cuh"
 
 using namespace zl;
@@ -35,6 +35,7 @@ struct Level {
     DeviceBuffer partial;    // conservation partial sums
     int partial_blocks = 0;
     bool bnd = false;        // some axis is not periodic
+    bool ordered = false;    // faces applied as ordered passes after the step kernel
     int even_layout = 0;     // 1 after an even step (see aa_kernel.cuh)
     long long nodes = 0;
     long long steps = 0;
@@ -244,48 +245,61 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     ZL_CUDA(ctx, cudaMemcpyAsync(mm, dminmax.ptr, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
 
-    // level box: periodic axes that the level spans completely wrap around, others get a ghost frame
+    // Level box.  A periodic axis the level spans completely wraps around (each plane stored
+    // once) unless the level also has a non-equilibrium face: the reference then reads its
+    // duplicated maximum plane in a face-by-face order that only an explicit copy reproduces,
+    // so the duplicate plane is kept and the periodic faces become ordered copy passes.
     LevelGeom geo{};
     LevelMap map{};
-    map.dims = dims;
-    geo.face_on_box = 0;
-    for (int a = 0; a < 3; ++a) {
-        if (a >= dims) {
-            geo.n[a] = 1;
-            geo.g[a] = 0;
-            geo.a[a] = 1;
-            geo.periodic[a] = 0;
-            map.lo[a] = 0;
-            map.n[a] = 1;
-            map.periodic[a] = 0;
-            continue;
-        }
+    for (int a = 0; a < dims; ++a) {
         const long long dlo = (long long)ctx->cfg.domain_min[a] << level;
         const long long dhi = (long long)ctx->cfg.domain_max[a] << level;
         if (mm[a] < dlo || mm[3 + a] > dhi)
             return fail(ctx, ZL_ETOPOLOGY, "level %d node indices [%d, %d] on axis %d leave the domain [%lld, %lld]",
                         level, mm[a], mm[3 + a], a, dlo, dhi);
-        const bool per = ctx->cfg.bc_kind[2 * a] == ZL_BC_PERIODIC;
-        if (per && mm[a] == dlo && mm[3 + a] == dhi) {
-            geo.n[a] = (int)(dhi - dlo);
-            geo.g[a] = 0;
-            geo.periodic[a] = 1;
-            map.lo[a] = (int)dlo;
-        } else {
-            geo.n[a] = mm[3 + a] - mm[a] + 1;
-            geo.g[a] = 1;
-            geo.periodic[a] = 0;
-            map.lo[a] = mm[a];
-            if (!per) {
+    }
+    auto make_geo = [&](bool allow_wrap) {
+        geo = LevelGeom{};
+        map = LevelMap{};
+        map.dims = dims;
+        for (int a = 0; a < 3; ++a) {
+            if (a >= dims) {
+                geo.n[a] = 1;
+                geo.a[a] = 1;
+                map.n[a] = 1;
+                continue;
+            }
+            const long long dlo = (long long)ctx->cfg.domain_min[a] << level;
+            const long long dhi = (long long)ctx->cfg.domain_max[a] << level;
+            const bool per = ctx->cfg.bc_kind[2 * a] == ZL_BC_PERIODIC;
+            if (per && allow_wrap && mm[a] == dlo && mm[3 + a] == dhi) {
+                geo.n[a] = (int)(dhi - dlo);
+                geo.g[a] = 0;
+                geo.periodic[a] = 1;
+                map.lo[a] = (int)dlo;
+            } else {
+                geo.n[a] = mm[3 + a] - mm[a] + 1;
+                geo.g[a] = 1;
+                geo.periodic[a] = 0;
+                map.lo[a] = mm[a];
                 if (mm[a] == dlo) geo.face_on_box |= 1 << (2 * a);
                 if (mm[3 + a] == dhi) geo.face_on_box |= 1 << (2 * a + 1);
             }
+            geo.a[a] = geo.n[a] + 2 * geo.g[a];
+            map.n[a] = geo.n[a];
+            map.periodic[a] = geo.periodic[a];
         }
-        geo.a[a] = geo.n[a] + 2 * geo.g[a];
-        map.n[a] = geo.n[a];
-        map.periodic[a] = geo.periodic[a];
-    }
+    };
+    make_geo(true);
+    bool has_neq = false, wraps = false;
+    for (int f = 0; f < 2 * dims; ++f)
+        if (ctx->cfg.bc_kind[f] == ZL_BC_NONEQ_EXTRAPOLATION && ((geo.face_on_box >> f) & 1)) has_neq = true;
+    for (int a = 0; a < dims; ++a) wraps = wraps || geo.periodic[a];
+    if (has_neq && wraps) make_geo(false);
+    L.ordered = has_neq;
     const long long cells = (long long)geo.a[0] * geo.a[1] * geo.a[2];
+    if (cells >= (1ll << 31))
+        return fail(ctx, ZL_EINVAL, "level %d box of %lld cells exceeds 2^31 (split the level)", level, cells);
     geo.stride = (cells + 63) / 64 * 64;
     geo.info = nullptr;
 
@@ -324,6 +338,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     const double dt = 1. / (double)(1u << level);
     p.tau = ctx->cfg.viscosity * 3. / dt + 0.5;
     p.rho0 = ctx->cfg.rho0;
+    p.fuse_bb = L.ordered ? 0 : 1;
     for (int f = 0; f < 6; ++f) p.face_kind[f] = ctx->cfg.bc_kind[f];
     for (int f = 0; f < 2 * dims; ++f) {
         const double* U = ctx->cfg.bc_velocity[f];
@@ -333,9 +348,12 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
             p.bb_term[f][o] = 6 * ctx->cfg.rho0 * lattice_w(dims, o) * cu;
         }
     }
+    p.omega32 = (float)(1. / p.tau);
     for (int k = 0; k < q; ++k) {
+        // fast-path MRT: shear moments relax with 1/tau through the SRT term; the others add
+        // (s_k - 1/tau) / |M_k|^2 (conserved moments of neq vanish and stay out)
         const double sk = lattice_s(dims, k);
-        p.mrt_coef[k] = (float)((sk < 0. ? 1. / p.tau : sk) / (double)lattice_norm2(dims, k));
+        p.mrt_coef[k] = sk > 0. ? (float)((sk - 1. / p.tau) / (double)lattice_norm2(dims, k)) : 0.f;
     }
     const double scale = ctx->cfg.storage_scale > 0. ? ctx->cfg.storage_scale : 8192.;
     p.scale = ctx->cfg.storage == ZL_STORAGE_F16 || ctx->cfg.storage == ZL_STORAGE_BF16 ? (float)scale : 1.f;
@@ -437,13 +455,24 @@ int zl_step_level(zl_ctx* ctx, int level) {
     ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr, L.geo,
                                 L.params, ctx->stream));
     L.even_layout ^= 1;
-    // non-equilibrium extrapolation faces, in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
+    // domain faces in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
+    // (lbm_grid_interface.cpp:225-314); bounce back is fused into the step kernel unless
+    // the level needs every face as an ordered pass
     for (int k = 0; k < 2 * ctx->dims; ++k) {
         const int face = k < ctx->dims ? 2 * k : 2 * (k - ctx->dims) + 1;
-        if (ctx->cfg.bc_kind[face] != ZL_BC_NONEQ_EXTRAPOLATION) continue;
         if (!((L.geo.face_on_box >> face) & 1)) continue;
-        ZL_CUDA(ctx, ctx->ops->neq(ctx->dims, L.f.ptr, L.geo, L.params, face, L.even_layout,
-                                   (const double*)L.feq_face.ptr + face * ctx->q, ctx->stream));
+        const int kind = ctx->cfg.bc_kind[face];
+        if (kind == ZL_BC_NONEQ_EXTRAPOLATION) {
+            ZL_CUDA(ctx, ctx->ops->neq(ctx->dims, L.f.ptr, L.geo, L.params, face, L.even_layout,
+                                       (const double*)L.feq_face.ptr + face * ctx->q, ctx->stream));
+        } else if (L.ordered && kind == ZL_BC_PERIODIC) {
+            // copies need the opposite face on the same level (lbm_periodic.cpp:124-131 skips otherwise)
+            const int both = 3 << (2 * (face >> 1));
+            if ((L.geo.face_on_box & both) != both) continue;
+            ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
+        } else if (L.ordered && kind == ZL_BC_BOUNCE_BACK) {
+            ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
+        }
     }
     ++L.steps;
     return ZL_OK;

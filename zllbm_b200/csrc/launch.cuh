@@ -13,6 +13,9 @@ struct LaunchSet {
                         const StepParams& p, cudaStream_t s);
     cudaError_t (*neq)(int dims, void* f, const LevelGeom& geo, const StepParams& p, int face, int even_layout,
                        const double* feq_b, cudaStream_t s);
+    // kind: ZL_BC_BOUNCE_BACK or ZL_BC_PERIODIC face pass
+    cudaError_t (*face)(int dims, int kind, void* f, const LevelGeom& geo, const StepParams& p, int face,
+                        int even_layout, cudaStream_t s);
     cudaError_t (*scatter)(int dims, void* f, const LevelGeom& geo, const StepParams& p, const LevelMap& m,
                            int even_layout, const uint64_t* codes, const double* fin, long long n, int* bad,
                            cudaStream_t s);
@@ -81,6 +84,22 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
             neq_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even, feq_b);                             \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
+    cudaError_t face_any(int dims, int kind, void* fv, const LevelGeom& geo, const StepParams& p, int face,     \
+                         int even, cudaStream_t s) {                                                             \
+        S* f = static_cast<S*>(fv);                                                                              \
+        const int axis = face >> 1;                                                                              \
+        const int o0 = axis == 0 ? 1 : 0, o1 = axis == 2 ? 1 : 2;                                                \
+        const int n0 = geo.n[o0], n1 = dims == 3 ? geo.n[o1] : 1;                                                \
+        dim3 b(128), g((n0 + 127) / 128, n1);                                                                    \
+        if (dims == 2) {                                                                                         \
+            if (kind == kBcBounceBack) bb_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);           \
+            else periodic_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);                           \
+        } else {                                                                                                 \
+            if (kind == kBcBounceBack) bb_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);          \
+            else periodic_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);                          \
+        }                                                                                                        \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
     cudaError_t scatter_any(int dims, void* fv, const LevelGeom& geo, const StepParams& p, const LevelMap& m,    \
                             int even, const uint64_t* codes, const double* fin, long long n, int* bad,           \
                             cudaStream_t s) {                                                                    \
@@ -120,6 +139,7 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
     }                                                                                                            \
     const LaunchSet& NAME() {                                                                                    \
         static const LaunchSet set = {(int)sizeof(S), NAME##_impl::step_any, NAME##_impl::neq_any,                \
+                                      NAME##_impl::face_any,                                                     \
                                       NAME##_impl::scatter_any, NAME##_impl::gather_any,                         \
                                       NAME##_impl::conservation_any};                                            \
         return set;                                                                                              \

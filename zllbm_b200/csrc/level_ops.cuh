@@ -126,6 +126,73 @@ __global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, 
     }
 }
 
+// ---------------------------------------------------------------- ordered face passes
+// Face nodes of `face` (the box edge lying on that domain face), one thread each.
+struct FaceNode {
+    Coord c;
+    long long self;
+    bool ok;
+};
+
+template <class L>
+__device__ __forceinline__ FaceNode face_node(const LevelGeom& geo, int face) {
+    FaceNode r;
+    const int axis = face >> 1;
+    const int o0 = axis == 0 ? 1 : 0;
+    const int o1 = axis == 2 ? 1 : 2;
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t1 = blockIdx.y;
+    r.ok = t0 < geo.n[o0] && (L::kDims == 2 || t1 < geo.n[o1]);
+    r.c.x[2] = 0;
+    r.c.x[axis] = (face & 1) ? geo.n[axis] - 1 : 0;
+    r.c.x[o0] = t0;
+    if (L::kDims == 3) r.c.x[o1] = t1;
+    r.self = (long long)(r.c.x[0] + geo.g[0]) +
+             (long long)geo.a[0] * ((r.c.x[1] + geo.g[1]) + (long long)geo.a[1] * (r.c.x[2] + geo.g[2]));
+    if (r.ok && geo.info && !(__ldg(geo.info + r.self) & kInfoPresent)) r.ok = false;
+    return r;
+}
+
+// Bounce back as its own pass (lbm_bounce_back.cpp:66-91): f(x, q_in) = f*(x, opp(q_in)) - 6 rho0 w (c.U).
+// Used when the level's faces must be applied one after another in the reference's order.
+template <class L, class S>
+__global__ void bb_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    using St = Storage<S>;
+    const FaceNode fn = face_node<L>(geo, face);
+    if (!fn.ok) return;
+#pragma unroll
+    for (int q = 1; q < L::kQ; ++q) {
+        if (!enters_through<L>(q, face)) continue;
+        const int o = Tables<L>::opp(q);
+        const auto v = St::load(f + post_collision_slot<L>(geo, fn.c, o, even_layout), p);
+        St::store(f + post_stream_slot<L>(geo, fn.c, q, even_layout), v - (decltype(v))p.bb_term[face][o], p);
+    }
+}
+
+// Periodic face on a level that keeps the reference's duplicated maximum plane
+// (lbm_periodic.cpp:77-133): the populations entering through the face are copied from the
+// node with the same other coordinates on the opposite face.
+template <class L, class S>
+__global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    using St = Storage<S>;
+    const FaceNode fn = face_node<L>(geo, face);
+    if (!fn.ok) return;
+    const int axis = face >> 1;
+    Coord other = fn.c;
+    other.x[axis] = (face & 1) ? 0 : geo.n[axis] - 1;
+    if (geo.info) {
+        const long long oc = (long long)(other.x[0] + geo.g[0]) +
+                             (long long)geo.a[0] * ((other.x[1] + geo.g[1]) + (long long)geo.a[1] * (other.x[2] + geo.g[2]));
+        if (!(__ldg(geo.info + oc) & kInfoPresent)) return;
+    }
+#pragma unroll
+    for (int q = 1; q < L::kQ; ++q) {
+        if (!enters_through<L>(q, face)) continue;
+        St::store(f + post_stream_slot<L>(geo, fn.c, q, even_layout),
+                  St::load(f + post_stream_slot<L>(geo, other, q, even_layout), p), p);
+    }
+}
+
 // ---------------------------------------------------------------- host exchange
 template <class L, class S>
 __global__ void scatter_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, LevelMap m, int even_layout,
