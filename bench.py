@@ -30,6 +30,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "D3Q19 MLUPS & HBM-roofline %; learned vs Smagorinsky LES error at same GPU"
 CELLS = 256          # unique nodes per axis (periodic; the reference stores 257 planes)
+COLLISION = "mrt"
 U0 = 0.05
 TAU = 0.55
 NU = (TAU - 0.5) / 3.0
@@ -66,7 +67,8 @@ def tgv_nodes(cells: int):
 def solver_config(storage: int, device: int):
     import zllbm_b200 as zl
     n = CELLS + 1
-    return zl.SolverConfig(lattice=zl.D3Q19, collision=zl.MRT, storage=storage, viscosity=NU, rho0=1.0,
+    return zl.SolverConfig(lattice=zl.D3Q19, collision=zl.MRT if COLLISION == "mrt" else zl.SRT,
+                           storage=storage, viscosity=NU, rho0=1.0,
                            bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(1, 1, 1), domain_max=(n, n, n), device=device)
 
 
@@ -348,17 +350,17 @@ def run_ours(args):
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
-            "config": {"workload": f"D3Q19 MRT Taylor-Green vortex, periodic {CELLS}^3 "
+            "config": {"workload": f"D3Q19 {COLLISION.upper()} Taylor-Green vortex, periodic {CELLS}^3 "
                                    f"(reference stores {CELLS + 1}^3), u0={U0}, tau={TAU}, "
                                    f"{args.storage} population storage, FP32 collision"
                                    if args.storage != "f64" else "FP64 collision",
-                       "nodes_per_gpu": nodes, "storage": args.storage, "collision": "MRT",
+                       "nodes_per_gpu": nodes, "storage": args.storage, "collision": COLLISION.upper(),
                        "l2": f"inputs larger than L2 ({alg_bytes / 2 / 1e9:.2f} GB of populations)",
                        "parallelism": f"{world} independent replica(s)" if world > 1 else "single GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": "aa_step_kernel<D3Q19, MRT>"},
+                         "kernel": f"aa_step_kernel<D3Q19, {COLLISION.upper()}>"},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -379,6 +381,8 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_BYTES))
+    ap.add_argument("--cells", type=int, default=CELLS, help="lattice edge (256 is the benchmark workload)")
+    ap.add_argument("--collision", default="mrt", choices=["mrt", "srt"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
@@ -386,6 +390,9 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    global CELLS, COLLISION
+    CELLS = args.cells
+    COLLISION = args.collision
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)

@@ -381,7 +381,7 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
         const int face = k < L::kDims ? 2 * k : 2 * (k - L::kDims) + 1;
         if ((faces >> face) & 1) {
             if (p.face_kind[face] == kBcBounceBack && enters_through<L>(q, face)) {
-                const int o = Tables<L>::opp(q);
+                const int o = bb_source<L>(q, face);
                 v = post[o] - (T)p.bb_term[face][o];
             }
         }
@@ -393,7 +393,7 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
 // One thread per node of the level box.  Odd selects the layout read (see file comment).
 // Bnd: the level has at least one non-periodic axis.  Masked: the box holds absent cells.
 template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked>
-__global__ void __launch_bounds__(256) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+__global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
     using Tb = Tables<L>;
     using St = Storage<S>;
     using T = typename St::T;

@@ -132,4 +132,24 @@ ZL_HD constexpr bool enters_through(int q, int face) {
     return (face & 1) ? (c < 0) : (c > 0);
 }
 
+// Source direction of the bounce-back for a population q entering through `face`: the
+// reference pairs the n-th entry of its per-axis "positive" and "negative" index lists
+// (d2q9_model/lbm_d2q9.h:62-67, d3q19_model/lbm_d3q19.h:86-95, used by
+// boundary_conditions/lbm_bounce_back.cpp:28-91).  For D3Q19 every pair is an opposite pair.
+// For D2Q9 the x lists are {1, 8, 5} / {3, 7, 6}: the diagonals of an x wall are reflected
+// specularly (8 <- 7, 5 <- 6) while y walls reflect them back (5 <- 7, 6 <- 8).
+template <class L>
+ZL_HD constexpr int bb_source(int q, int face) {
+    if constexpr (L::kQ == 9) {
+        if ((face >> 1) == 0) {
+            constexpr int xmin[9] = {0, 3, 0, 0, 0, 6, 0, 0, 7};  // 1<-3, 5<-6, 8<-7
+            constexpr int xmax[9] = {0, 0, 0, 1, 0, 0, 5, 8, 0};  // 3<-1, 6<-5, 7<-8
+            return (face & 1) ? xmax[q] : xmin[q];
+        }
+        return Tables<L>::opp(q);
+    } else {
+        return Tables<L>::opp(q);
+    }
+}
+
 }  // namespace zl

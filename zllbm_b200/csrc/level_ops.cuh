@@ -153,7 +153,8 @@ __device__ __forceinline__ FaceNode face_node(const LevelGeom& geo, int face) {
     return r;
 }
 
-// Bounce back as its own pass (lbm_bounce_back.cpp:66-91): f(x, q_in) = f*(x, opp(q_in)) - 6 rho0 w (c.U).
+// Bounce back as its own pass (lbm_bounce_back.cpp:28-91): f(x, q_in) = f*(x, o) - 6 rho0 w_o (c_o.U),
+// o = bb_source(q_in, face).
 // Used when the level's faces must be applied one after another in the reference's order.
 template <class L, class S>
 __global__ void bb_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
@@ -163,7 +164,7 @@ __global__ void bb_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, i
 #pragma unroll
     for (int q = 1; q < L::kQ; ++q) {
         if (!enters_through<L>(q, face)) continue;
-        const int o = Tables<L>::opp(q);
+        const int o = bb_source<L>(q, face);
         const auto v = St::load(f + post_collision_slot<L>(geo, fn.c, o, even_layout), p);
         St::store(f + post_stream_slot<L>(geo, fn.c, q, even_layout), v - (decltype(v))p.bb_term[face][o], p);
     }
