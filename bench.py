@@ -381,7 +381,7 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--storage", default="f32", choices=sorted(STORAGE_BYTES))
-    ap.add_argument("--cells", type=int, default=CELLS, help="lattice edge (256 is the benchmark workload)")
+    ap.add_argument("--cells", type=int, default=256, help="lattice edge (256 is the benchmark workload)")
     ap.add_argument("--collision", default="mrt", choices=["mrt", "srt"])
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variants", type=int, default=1)
@@ -390,9 +390,8 @@ def main():
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    global CELLS, COLLISION
-    CELLS = args.cells
-    COLLISION = args.collision
+    globals()["CELLS"] = args.cells
+    globals()["COLLISION"] = args.collision
     if args.impl == "reference":
         return run_reference_arm(args)
     return run_ours(args)
