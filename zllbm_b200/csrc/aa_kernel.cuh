@@ -53,6 +53,7 @@ struct StepParams {
     float omega32;          // 1/tau in FP32 (fast path)
     float inv_scale;        // reduced storage: deviation = stored * inv_scale
     float scale;
+    double scale_d;         // the same scale in FP64 (1 for FP64 / FP32 storage)
     int fuse_bb;            // bounce back applied inside the step kernel (no ordered face passes needed)
 };
 
@@ -61,33 +62,47 @@ template <class S> struct Storage;
 template <> struct Storage<double> {
     using T = double;
     static constexpr bool kDeviation = false;
+    static constexpr bool kScaled = false;
+    ZL_HD static T load_raw(const double* p) { return *p; }
+    ZL_HD static void store_raw(double* p, T v) { *p = v; }
     ZL_HD static T load(const double* p, const StepParams&) { return *p; }
     ZL_HD static void store(double* p, T v, const StepParams&) { *p = v; }
 };
 template <> struct Storage<float> {
     using T = float;
     static constexpr bool kDeviation = true;
+    static constexpr bool kScaled = false;
+    __device__ __forceinline__ static T load_raw(const float* p) { return __ldg(p); }
+    __device__ __forceinline__ static void store_raw(float* p, T v) { *p = v; }
     __device__ __forceinline__ static T load(const float* p, const StepParams&) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, T v, const StepParams&) { *p = v; }
 };
+// Reduced storage keeps (f - w) * scale.  The fused step kernel works directly in these
+// scaled units (the collision is linear in the deviations apart from the equilibrium, which
+// un-scales density and momentum once), so only the exchange and boundary kernels apply the
+// scale per population.
 template <> struct Storage<__half> {
     using T = float;
     static constexpr bool kDeviation = true;
+    static constexpr bool kScaled = true;
+    __device__ __forceinline__ static T load_raw(const __half* p) { return __half2float(__ldg(p)); }
+    __device__ __forceinline__ static void store_raw(__half* p, T v) { *p = __float2half_rn(v); }
     __device__ __forceinline__ static T load(const __half* p, const StepParams& sp) {
-        return __half2float(__ldg(p)) * sp.inv_scale;
+        return load_raw(p) * sp.inv_scale;
     }
-    __device__ __forceinline__ static void store(__half* p, T v, const StepParams& sp) {
-        *p = __float2half_rn(v * sp.scale);
-    }
+    __device__ __forceinline__ static void store(__half* p, T v, const StepParams& sp) { store_raw(p, v * sp.scale); }
 };
 template <> struct Storage<__nv_bfloat16> {
     using T = float;
     static constexpr bool kDeviation = true;
+    static constexpr bool kScaled = true;
+    __device__ __forceinline__ static T load_raw(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
+    __device__ __forceinline__ static void store_raw(__nv_bfloat16* p, T v) { *p = __float2bfloat16_rn(v); }
     __device__ __forceinline__ static T load(const __nv_bfloat16* p, const StepParams& sp) {
-        return __bfloat162float(__ldg(p)) * sp.inv_scale;
+        return load_raw(p) * sp.inv_scale;
     }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, T v, const StepParams& sp) {
-        *p = __float2bfloat16_rn(v * sp.scale);
+        store_raw(p, v * sp.scale);
     }
 };
 
@@ -180,9 +195,21 @@ __device__ __forceinline__ void collide_exact(const double* f, double* out, cons
 // from the shear rate S_nu = 1/tau (the basis is orthogonal, so the shear moments fold into
 // the first term); lambda_k = (s_k - 1/tau) / |M_k|^2 and m_k = M_k . neq.  The conserved
 // moments of neq vanish and are skipped.
+// c_q . u with the zero components left out (a product with 0.f is not folded away under IEEE rules)
 template <class L>
-__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float& omega_unused) {
-    (void)omega_unused;
+__device__ __forceinline__ float signed_dot(int q, float ux, float uy, float uz) {
+    using Tb = Tables<L>;
+    float cu = 0.f;
+    bool first = true;
+    if (Tb::cx(q)) { cu = Tb::cx(q) > 0 ? ux : -ux; first = false; }
+    if (Tb::cy(q)) { cu = first ? (Tb::cy(q) > 0 ? uy : -uy) : (Tb::cy(q) > 0 ? cu + uy : cu - uy); first = false; }
+    if (L::kDims == 3 && Tb::cz(q)) { cu = first ? (Tb::cz(q) > 0 ? uz : -uz) : (Tb::cz(q) > 0 ? cu + uz : cu - uz); }
+    return cu;
+}
+
+template <class L>
+__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float scale, float inv_scale) {
+    // d are deviations times `scale`; neq is returned in the same units
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
@@ -193,22 +220,23 @@ __device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float& o
         if (Tb::cy(q)) jy += Tb::cy(q) == 1 ? d[q] : -d[q];
         if (L::kDims == 3 && Tb::cz(q)) jz += Tb::cz(q) == 1 ? d[q] : -d[q];
     }
-    const float rho = 1.f + drho;
-    const float inv_rho = 1.f / rho;
-    const float ux = jx * inv_rho, uy = jy * inv_rho, uz = jz * inv_rho;
+    const float rho = fmaf(drho, inv_scale, 1.f);
+    const float k = inv_scale / rho;
+    const float ux = jx * k, uy = jy * k, uz = jz * k;
     const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
-    // even part shared by opposite directions, odd part 3 rho (c.u) w
+    const float srho = scale * rho;
+    // even part shared by opposite directions, odd part 3 w rho (c.u)
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         const int opp = Tb::opp(q);
         if (opp < q) continue;
-        const float cu = Tb::cx(q) * ux + Tb::cy(q) * uy + Tb::cz(q) * uz;
+        const float cu = signed_dot<L>(q, ux, uy, uz);
         const float w = (float)Tb::w(q);
-        const float even = w * (drho + rho * (4.5f * cu * cu - usq15));
+        const float even = w * fmaf(srho, fmaf(4.5f * cu, cu, -usq15), drho);
         if (q == 0) {
             neq[0] = d[0] - even;
         } else {
-            const float odd = w * rho * 3.f * cu;
+            const float odd = (3.f * w) * srho * cu;
             neq[q] = d[q] - (even + odd);
             neq[opp] = d[opp] - (even - odd);
         }
@@ -295,8 +323,7 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float neq[Q];
-    float unused = 0.f;
-    feq_neq_dev<L>(d, neq, unused);
+    feq_neq_dev<L>(d, neq, p.scale, p.inv_scale);
     const float omega = p.omega32;
     if (coll == kSrt) {
 #pragma unroll
@@ -382,7 +409,7 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
         if ((faces >> face) & 1) {
             if (p.face_kind[face] == kBcBounceBack && enters_through<L>(q, face)) {
                 const int o = bb_source<L>(q, face);
-                v = post[o] - (T)p.bb_term[face][o];
+                v = post[o] - (T)(p.bb_term[face][o] * p.scale_d);
             }
         }
     }
@@ -421,21 +448,23 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
     }
     auto cell = [&](int dx, int dy, int dz) -> int { return bx[dx + 1] + row[dy + 1][dz + 1]; };
     const int self = cell(0, 0, 0);
+    // population planes: uniform 64-bit bases, per-thread 32-bit cell offsets
+    const long long st = geo.stride;
+    auto plane = [&](int q) -> S* { return f + q * st; };
 
     uint32_t info = 0;
     if (Masked) {
         info = __ldg(geo.info + self);
         if (!(info & kInfoPresent)) return;
     }
-    const long long st = geo.stride;
 
     T pre[Q], post[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         if (Odd && q != 0) {
-            pre[q] = St::load(f + Tb::opp(q) * st + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), p);
+            pre[q] = St::load_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)));
         } else {
-            pre[q] = St::load(f + q * st + self, p);
+            pre[q] = St::load_raw(plane(q) + self);
         }
     }
 
@@ -451,9 +480,9 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         if (Odd && q != 0) {
-            St::store(f + q * st + cell(Tb::cx(q), Tb::cy(q), Tb::cz(q)), post[q], p);
+            St::store_raw(plane(q) + cell(Tb::cx(q), Tb::cy(q), Tb::cz(q)), post[q]);
         } else {
-            St::store(f + Tb::opp(q) * st + self, post[q], p);
+            St::store_raw(plane(Tb::opp(q)) + self, post[q]);
         }
     }
     if (Bnd || Masked) {
@@ -463,9 +492,9 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
             if (!miss) continue;
             const T v = missing_value<L, T>(q, faces, pre, post, p);
             if (Odd) {
-                St::store(f + q * st + self, v, p);
+                St::store_raw(plane(q) + self, v);
             } else {
-                St::store(f + Tb::opp(q) * st + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v, p);
+                St::store_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v);
             }
         }
     }

@@ -67,7 +67,7 @@ __device__ __forceinline__ void feq_dev(float rho, float ux, float uy, float uz,
     const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
 #pragma unroll
     for (int q = 0; q < L::kQ; ++q) {
-        const float cu = Tb::cx(q) * ux + Tb::cy(q) * uy + Tb::cz(q) * uz;
+        const float cu = signed_dot<L>(q, ux, uy, uz);
         deq[q] = (float)Tb::w(q) * ((rho - 1.f) + rho * (3.f * cu + 4.5f * cu * cu - usq15));
     }
 }
