@@ -298,7 +298,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     if (has_neq && wraps) make_geo(false);
     L.ordered = has_neq;
     const long long cells = (long long)geo.a[0] * geo.a[1] * geo.a[2];
-    if (cells >= (1ll << 31))
+    if (cells >= (1ll << 31) - 64)
         return fail(ctx, ZL_EINVAL, "level %d box of %lld cells exceeds 2^31 (split the level)", level, cells);
     geo.stride = (cells + 63) / 64 * 64;
     geo.info = nullptr;
@@ -358,6 +358,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     const double scale = ctx->cfg.storage_scale > 0. ? ctx->cfg.storage_scale : 8192.;
     p.scale = ctx->cfg.storage == ZL_STORAGE_F16 || ctx->cfg.storage == ZL_STORAGE_BF16 ? (float)scale : 1.f;
     p.inv_scale = 1.f / p.scale;
+    p.scale_d = (double)p.scale;
     if (ctx->cfg.collision == ZL_MRT && ctx->cfg.storage == ZL_STORAGE_F64) {
         std::vector<double> m(q * q);
         host_mrt_matrix(dims, 1. / p.tau, false, m.data());
