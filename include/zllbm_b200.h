@@ -44,6 +44,7 @@ extern "C" {
 #define ZL_ETIMEOUT (-4)   /* a bounded device wait gave up */
 #define ZL_ENAN (-5)       /* non-finite populations detected */
 #define ZL_ESTATE (-6)     /* call out of order (e.g. stepping a level with no nodes) */
+#define ZL_ETOOLARGE (-7)  /* input larger than a fixed-capacity entry point accepts */
 
 /* lattice (SolverCreatorLbmD2Q9 / SolverCreatorLbmD3Q19, lbm_d2q9_mandatory.cpp:19-23,
    lbm_d3q19_mandatory.cpp:20-24) */
@@ -173,6 +174,24 @@ int zl_mrt_matrix(int lattice, double tau, double* out);
 
 /* ABI version of the loaded library. */
 int zl_abi_version(void);
+
+/* ---- allocation-free entry point (no counterpart in the reference) ---- */
+
+/* Mass and momentum of n nodes, summed in FP64 like zl_conservation, for callers that cannot
+   call cudaMalloc (work issued from a loop where cudaMalloc / cudaFree would synchronize the
+   device, or device memory owned entirely by another allocator).  It allocates nothing:
+     - f_device: caller-owned device array of n * q doubles, node-major (GridNodeLbm::f_ order);
+     - out_device: caller-owned device array of 4 doubles {mass, jx, jy, jz} (jz = 0 in 2D);
+     - stream: cudaStream_t to issue on (NULL: the legacy default stream).
+   Block partial sums go to a fixed static device array of 128 KiB that every GPU loading the
+   library keeps until process exit; its capacity caps n at 16,777,216 nodes per call (larger
+   n returns ZL_ETOOLARGE).  The first call on a device looks up that array's device address
+   with that device current, so make the first call before any stream capture.  The array is
+   shared by all calls and keeps the last call's partials; every call rewrites the partials it
+   reads, but calls that overlap on the GPU (different streams, or host threads without
+   ordering) race on it.  The call is asynchronous on `stream`; read out_device after
+   synchronizing. */
+int zl_moments_noalloc(int lattice, const double* f_device, int64_t n, double* out_device, void* stream);
 
 #ifdef __cplusplus
 }

@@ -22,7 +22,8 @@ SRT, MRT = 0, 1
 BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION = 0, 1, 2, 3
 STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORAGE_F64, "f32": STORAGE_F32, "f16": STORAGE_F16, "bf16": STORAGE_BF16}
-ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE"}
+ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE",
+          -7: "ETOOLARGE"}
 
 
 class ZlError(RuntimeError):
@@ -86,6 +87,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_morton_neighbors": ([ctypes.c_int, u64p, i64, u64p], ctypes.c_int),
         "zl_upstream_index": ([ctypes.c_int, u64p, i64, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "zl_mrt_matrix": ([ctypes.c_int, ctypes.c_double, dp], ctypes.c_int),
+        "zl_moments_noalloc": ([ctypes.c_int, P, i64, P, P], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

@@ -30,6 +30,7 @@ SOURCES = {
     "kernels_f64.cu": ["-fmad=false"],
     "kernels_f32.cu": [],
     "kernels_f16.cu": [],
+    "static_scratch.cu": [],
 }
 
 
