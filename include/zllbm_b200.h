@@ -129,8 +129,29 @@ int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, do
    for a level without coarse/fine neighbours. */
 int zl_step_level(zl_ctx* ctx, int level);
 
+/* Coarse/fine interface of refinement level `level` (>= 1) with level - 1, from the reference's
+   interface layer maps (InterfaceLayerInfo, amr_project/grid/grid_info_interface.h:117-127):
+     c2f_fine        fine nodes of the fine-to-coarse layers 1..2 of `level` (vec_{inner,outer}_
+                     fine2coarse_), the targets of the explosion (TransferInfoFromCoarseGrid,
+                     lbm_grid_interface.cpp:408-515);
+     f2c_coarse      coarse nodes of coarse-to-fine layer 1 of `level - 1` (vec_{inner,outer}_
+                     coarse2fine_), the targets of the coalescence (TransferInfoToCoarseGrid, :524-564);
+     coarse_excluded coarse nodes flagged kNodeStatusCoarse2FineGhost_ (amr_project/grid/grid_manager.h:64-73),
+                     which the interpolation skips in favour of the coincident fine node.
+   Interpolation stencils (4-point Lagrange per axis, grid/grid_interpolation.cpp:433-525) are
+   resolved here; stencils that reach the domain boundary return ZL_ETOPOLOGY. */
+int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int64_t n_c2f,
+                           const uint64_t* f2c_coarse, int64_t n_f2c, const uint64_t* coarse_excluded,
+                           int64_t n_excluded);
+
+/* Exchange between `fine_level` and fine_level - 1 (SolverLbmInterface::InformationFromGridOfDifferentLevel,
+   lbm_solver_interface.cpp:224-238): explosion into the fine ghost layers, then coalescence. */
+int zl_transfer_levels(zl_ctx* ctx, int fine_level);
+
 /* n background steps of every level, in the reference's sub-cycled order
-   (AmrManager::TimeMarching, amr_manager.cpp:279-300). */
+   (AmrManager::TimeMarching, amr_manager.cpp:279-300; MultiTimeSteppingC2F,
+   grid/grid_manager.cpp:997-1023), with the coarse/fine exchange after every second
+   sub-step of a fine level. */
 int zl_advance(zl_ctx* ctx, int steps);
 
 /* Sum over a level's nodes of rho and rho*u, accumulated in FP64 on the device:

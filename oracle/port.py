@@ -311,3 +311,38 @@ def upstream_lookup(codes, dims: int) -> np.ndarray:
                     u = morton_pos(u, dims, a)
             out[i, q] = where.get(u, -1)
     return out
+
+
+def load_levels(path: str):
+    """Read a multi-level dump of ``ref_harness.cpp`` (``lout0=`` / ``lout=``).
+
+    Returns (dims, q, levels) where each level is a dict with ``nodes`` (structured array of
+    code, flag, rho, u[3], f[q], sorted by code) and ``layers`` {(kind, layer): codes}; kinds
+    0/1 are the inner/outer coarse-to-fine layers of the level, 2/3 its inner/outer
+    fine-to-coarse layers (grid/grid_info_interface.h:117-127)."""
+    with open(path, "rb") as fh:
+        raw = fh.read()
+    dims, q, nlev = (int(v) for v in np.frombuffer(raw[:12], np.int32))
+    off = 12
+    rec = np.dtype([("code", "<u8"), ("flag", "<i4"), ("pad", "<i4"), ("rho", "<f8"), ("u", "<f8", (3,)),
+                    ("f", "<f8", (q,))])
+    levels = []
+    for _ in range(nlev):
+        n = int(np.frombuffer(raw[off:off + 8], np.int64)[0])
+        off += 8
+        nodes = np.frombuffer(raw[off:off + n * rec.itemsize], rec, count=n)
+        off += n * rec.itemsize
+        layers = {}
+        while True:
+            kind, layer = (int(v) for v in np.frombuffer(raw[off:off + 8], np.int32))
+            off += 8
+            if kind < 0:
+                break
+            c = int(np.frombuffer(raw[off:off + 8], np.int64)[0])
+            off += 8
+            codes = np.frombuffer(raw[off:off + 8 * c], np.uint64, count=c)
+            off += 8 * c
+            key = (kind, layer)
+            layers[key] = np.union1d(layers[key], codes) if key in layers else codes.copy()
+        levels.append({"nodes": nodes, "layers": layers})
+    return dims, q, levels

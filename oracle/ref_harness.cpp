@@ -26,6 +26,8 @@
 #include "./amr_manager.h"
 #include "d2q9_model/lbm_d2q9.h"
 #include "d3q19_model/lbm_d3q19.h"
+#include "criterion/geometry_info_origin.h"
+#include "criterion/geometry_default_shape.h"
 
 using namespace rootproject;
 using amrproject::EDomainBoundaryDirection;
@@ -63,6 +65,55 @@ ELbmBoundaryConditionScheme kind_of(const std::string& k) {
     if (k == "neq") return ELbmBoundaryConditionScheme::kNonEqExtrapolation;
     std::fprintf(stderr, "unknown bc kind %s\n", k.c_str());
     std::exit(2);
+}
+
+// Multi-level dump: int32 dims, q, nlevels; per level: int64 n, then n records of
+// uint64 code, int32 flag, int32 pad, double rho, double u[3], double f[q] (sorted by code);
+// then 8 layer lists (inner c2f, outer c2f, inner f2c, outer f2c; each for layers 0..),
+// written as int32 kind, int32 layer, int64 count, uint64 codes[count]; terminated by kind -1.
+void dump_levels(const std::string& path, int dims, int q, amrproject::GridManagerInterface& gm) {
+    FILE* fp = std::fopen(path.c_str(), "wb");
+    if (!fp) { std::perror(path.c_str()); std::exit(3); }
+    int32_t hdr[3] = {dims, q, static_cast<int32_t>(gm.vec_ptr_grid_info_.size())};
+    std::fwrite(hdr, sizeof(hdr), 1, fp);
+    for (auto& g : gm.vec_ptr_grid_info_) {
+        auto& nodes = *dynamic_cast<lbmproject::GridInfoLbmInteface&>(*g).GetPtrToLbmGrid();
+        std::vector<std::pair<uint64_t, lbmproject::GridNodeLbm*>> order;
+        for (auto& it : nodes) order.emplace_back(it.first.to_ullong(), it.second.get());
+        std::sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        int64_t n = static_cast<int64_t>(order.size());
+        std::fwrite(&n, sizeof(n), 1, fp);
+        for (auto& [code, node] : order) {
+            int32_t fl[2] = {node->flag_status_, 0};
+            double mac[4] = {node->rho_, 0., 0., 0.};
+            for (size_t a = 0; a < node->velocity_.size() && a < 3; ++a) mac[1 + a] = node->velocity_[a];
+            std::fwrite(&code, sizeof(code), 1, fp);
+            std::fwrite(fl, sizeof(fl), 1, fp);
+            std::fwrite(mac, sizeof(mac), 1, fp);
+            std::fwrite(node->f_.data(), sizeof(double), q, fp);
+        }
+        auto write_layers = [&](int32_t kind, const std::vector<DefMap<DefInt>>& layers) {
+            for (size_t i = 0; i < layers.size(); ++i) {
+                std::vector<uint64_t> codes;
+                for (auto& it : layers[i]) codes.push_back(it.first.to_ullong());
+                std::sort(codes.begin(), codes.end());
+                int32_t kl[2] = {kind, static_cast<int32_t>(i)};
+                int64_t c = static_cast<int64_t>(codes.size());
+                std::fwrite(kl, sizeof(kl), 1, fp);
+                std::fwrite(&c, sizeof(c), 1, fp);
+                std::fwrite(codes.data(), sizeof(uint64_t), codes.size(), fp);
+            }
+        };
+        for (auto& [key, info] : g->map_ptr_interface_layer_info_) {
+            write_layers(0, info->vec_inner_coarse2fine_);
+            write_layers(1, info->vec_outer_coarse2fine_);
+            write_layers(2, info->vec_inner_fine2coarse_);
+            write_layers(3, info->vec_outer_fine2coarse_);
+        }
+        int32_t end[2] = {-1, 0};
+        std::fwrite(end, sizeof(end), 1, fp);
+    }
+    std::fclose(fp);
 }
 
 void dump(const std::string& path, int dims, int q, amrproject::GridInfoInterface& grid) {
@@ -154,8 +205,50 @@ int main(int argc, char* argv[]) {
     amrproject::AmrManager* amr = amrproject::AmrManager::GetInstance();
     amr->StartupAmrManager(argc, argv);
     amr->StartupInitialization(dims);
-    amr->ptr_grid_manager_->SetMaxLevel(0);
+    const int max_level = kv.count("levels") ? std::atoi(kv["levels"].c_str()) : 0;
+    amr->ptr_grid_manager_->SetMaxLevel(max_level);
     amr->program_name_ = "zl_ref_run";
+    // optional refinement around a default shape (no immersed-boundary forcing):
+    //   geo=circle:cx,cy,r  or  geo=cube:cx,cy,cz,edge ; ext=<outer layers per level> ; inner=<layers>
+    if (kv.count("geo") && max_level > 0) {
+        const std::string g = kv["geo"];
+        const std::string kind = g.substr(0, g.find(':'));
+        const std::vector<double> gp = parse_list(g.substr(g.find(':') + 1));
+        amrproject::GeometryInfoOriginCreator creator;
+        amr->ptr_criterion_manager_->vec_ptr_geometries_.push_back(creator.CreateGeometryInfo(dims));
+        auto geo = amr->ptr_criterion_manager_->vec_ptr_geometries_.back();
+        if (kind == "circle") {
+            auto shape = std::make_unique<amrproject::GeoShapeDefaultCircle2D>(geo);
+            shape->center_ = {gp[0], gp[1]};
+            shape->radius_ = gp[2];
+            geo->ptr_geo_shape_ = std::move(shape);
+        } else {
+            auto shape = std::make_unique<amrproject::GeoShapeDefaultCube3D>(geo);
+            shape->center_ = {gp[0], gp[1], gp[2]};
+            shape->length_ = gp[3];
+            geo->ptr_geo_shape_ = std::move(shape);
+        }
+        geo->SetGridExtendType(amrproject::EGridExtendType::kInAndOut);
+        geo->SetLevel(max_level);
+        std::vector<DefInt> ext;
+        for (double v : parse_list(kv.count("ext") ? kv["ext"] : "4")) ext.push_back(static_cast<DefInt>(v));
+        ext.resize(max_level + 1, ext.back());
+        std::vector<DefInt> inner;
+        for (double v : parse_list(kv.count("inner") ? kv["inner"] : "4")) inner.push_back(static_cast<DefInt>(v));
+        inner.resize(max_level + 1, inner.back());
+        geo->SetXExtendPositive(ext);
+        geo->SetXExtendNegative(ext);
+        geo->SetYExtendPositive(ext);
+        geo->SetYExtendNegative(ext);
+        if (dims == 3) {
+            geo->SetZExtendPositive(ext);
+            geo->SetZExtendNegative(ext);
+        }
+        geo->SetInnerExtend(inner);
+        amr->ptr_grid_manager_->vec_ptr_tracking_info_creator_.push_back(
+            std::make_unique<amrproject::TrackingGridInfoCreatorInterface>());
+        geo->SetPtrTrackingGridInfoCreator(amr->ptr_grid_manager_->vec_ptr_tracking_info_creator_.back().get());
+    }
     std::vector<double> domain(n.begin(), n.begin() + dims);
     amr->ptr_grid_manager_->SetDomainSize(domain);
     amr->ptr_grid_manager_->SetDomainGridSize({1.});
@@ -226,6 +319,7 @@ int main(int argc, char* argv[]) {
             it.second->velocity_ = u;
         }
     }
+    if (kv.count("lout0")) dump_levels(kv["lout0"], dims, q, *amr->ptr_grid_manager_);
     if (kv.count("out0")) dump(kv["out0"], dims, q, grid0);
     const int warmup = kv.count("warmup") ? std::atoi(kv["warmup"].c_str()) : 0;
     for (int it = 0; it < warmup; ++it) amr->TimeMarching(it);
@@ -233,6 +327,7 @@ int main(int argc, char* argv[]) {
     for (int it = warmup; it < warmup + steps; ++it) amr->TimeMarching(it);
     auto t1 = std::chrono::steady_clock::now();
     if (kv.count("out")) dump(kv["out"], dims, q, grid0);
+    if (kv.count("lout")) dump_levels(kv["lout"], dims, q, *amr->ptr_grid_manager_);
     if (kv.count("timing")) {
         const double sec = std::chrono::duration<double>(t1 - t0).count();
         std::printf("{\"nodes\": %zu, \"steps\": %d, \"seconds\": %.6f}\n", grid0.map_grid_node_.size(), steps, sec);

@@ -63,6 +63,44 @@ CASES = {
 }
 
 
+# multi-level grids refined around a default shape (the reference's GeometryInfoOrigin), NEQ inflow/outflow
+AMR_CASES = {
+    "amr2d_l1": dict(dims=2, n=(40, 32), levels=1, geo="circle:20,16,3", ext=3, inner=2, coll="srt", nu=0.02,
+                     bc=["xmin:neq:0.05,0", "xmax:neq:0.05,0", "ymin:bb", "ymax:bb"], steps=6),
+    "amr2d_l2": dict(dims=2, n=(48, 40), levels=2, geo="circle:24,20,2", ext=3, inner=2, coll="mrt", nu=0.01,
+                     bc=["xmin:neq:0.04,0", "xmax:neq:0.04,0", "ymin:bb", "ymax:bb:0.02,0"], steps=4),
+    "amr3d_l1": dict(dims=3, n=(20, 16, 16), levels=1, geo="cube:10,8,8,2", ext=2, inner=1, coll="mrt", nu=0.02,
+                     bc=["xmin:neq:0.05,0,0", "xmax:neq:0.05,0,0", "ymin:bb", "ymax:bb", "zmin:bb", "zmax:bb"], steps=3),
+}
+
+
+def run_amr(name, case, tmp):
+    from oracle.port import load_levels
+    wd = os.path.join(tmp, name)
+    os.makedirs(wd, exist_ok=True)
+    args = [REF_RUN, f"dims={case['dims']}", "n=" + ",".join(str(v) for v in case["n"]), f"levels={case['levels']}",
+            f"geo={case['geo']}", f"ext={case['ext']}", f"inner={case['inner']}", f"coll={case['coll']}",
+            f"nu={case['nu']!r}", f"steps={case['steps']}", "lout0=" + os.path.join(wd, "l0.bin"),
+            "lout=" + os.path.join(wd, "l1.bin")] + [f"bc={b}" for b in case["bc"]]
+    subprocess.run(args, check=True, cwd=wd, stdout=subprocess.DEVNULL)
+    dims, q, before = load_levels(os.path.join(wd, "l0.bin"))
+    _, _, after = load_levels(os.path.join(wd, "l1.bin"))
+    out = {"meta": json.dumps(case)}
+    for lv, (b, a) in enumerate(zip(before, after)):
+        assert np.array_equal(b["nodes"]["code"], a["nodes"]["code"])
+        out[f"codes{lv}"] = b["nodes"]["code"]
+        out[f"flags{lv}"] = b["nodes"]["flag"]
+        out[f"f_before{lv}"] = b["nodes"]["f"]
+        out[f"f_after{lv}"] = a["nodes"]["f"]
+        lay = b["layers"]
+        empty = np.zeros(0, dtype=np.uint64)
+        out[f"c2f_fine{lv}"] = np.union1d(np.union1d(lay.get((2, 1), empty), lay.get((3, 1), empty)),
+                                          np.union1d(lay.get((2, 2), empty), lay.get((3, 2), empty)))
+        out[f"f2c_coarse{lv}"] = np.union1d(lay.get((0, 1), empty), lay.get((1, 1), empty))
+    np.savez_compressed(os.path.join(HERE, f"amr_{name}.npz"), **out)
+    print(name, [len(l["nodes"]) for l in before], "nodes per level")
+
+
 def morton_cases(dims: int, rng: np.random.Generator) -> np.ndarray:
     nb = 64 // dims
     edge = []
@@ -94,6 +132,8 @@ def main():
             np.savez_compressed(os.path.join(HERE, f"lbm_{name}.npz"), meta=json.dumps(meta),
                                 codes=before["code"], f_before=before["f"], f_after=after["f"])
             print(name, before.size, "nodes")
+        for name, case in AMR_CASES.items():
+            run_amr(name, case, tmp)
         rng = np.random.default_rng(20261203)
         for dims in (2, 3):
             codes = morton_cases(dims, rng)

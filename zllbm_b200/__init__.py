@@ -77,6 +77,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_get_macros": ([P, ctypes.c_int, u64p, dp, dp, i64], ctypes.c_int),
         "zl_step_level": ([P, ctypes.c_int], ctypes.c_int),
         "zl_advance": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_level_interface": ([P, ctypes.c_int, u64p, i64, u64p, i64, u64p, i64], ctypes.c_int),
+        "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
         "zl_conservation": ([P, ctypes.c_int, dp], ctypes.c_int),
         "zl_synchronize": ([P], ctypes.c_int),
         "zl_get_stream": ([P, ctypes.POINTER(P)], ctypes.c_int),
@@ -221,6 +223,14 @@ class Context:
         self._check(self.lib.zl_get_macros(self.handle, level, _p(c, ctypes.c_uint64), _p(rho, ctypes.c_double),
                                            _p(u, ctypes.c_double), c.size))
         return rho, u
+
+    def set_level_interface(self, level: int, c2f_fine, f2c_coarse, coarse_excluded):
+        a, b, c = _u64(c2f_fine), _u64(f2c_coarse), _u64(coarse_excluded)
+        self._check(self.lib.zl_set_level_interface(self.handle, level, _p(a, ctypes.c_uint64), a.size,
+                                                    _p(b, ctypes.c_uint64), b.size, _p(c, ctypes.c_uint64), c.size))
+
+    def transfer_levels(self, fine_level: int):
+        self._check(self.lib.zl_transfer_levels(self.handle, fine_level))
 
     def step_level(self, level: int = 0):
         self._check(self.lib.zl_step_level(self.handle, level))

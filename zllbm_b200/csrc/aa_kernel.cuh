@@ -31,6 +31,7 @@ enum Collision : int { kSrt = 0, kMrt = 1 };
 
 // Per-cell information for levels whose node set does not fill its box.
 constexpr uint32_t kInfoPresent = 1u << 31;
+constexpr uint32_t kInfoSaveMacro = 1u << 30;  // keep rho, u of the last collision (coarse/fine transfer source)
 constexpr int kInfoFaceShift = 24;  // 6 bits: on face xmin..zmax (reference boundary node sets)
 
 struct LevelGeom {
@@ -55,6 +56,7 @@ struct StepParams {
     float scale;
     double scale_d;         // the same scale in FP64 (1 for FP64 / FP32 storage)
     int fuse_bb;            // bounce back applied inside the step kernel (no ordered face passes needed)
+    double* macro;          // rho, ux, uy, uz per cell for nodes flagged kInfoSaveMacro (else unused)
 };
 
 // ---------------------------------------------------------------- storage
@@ -165,10 +167,15 @@ __device__ __forceinline__ void feq_exact(double rho, double ux, double uy, doub
 }
 
 template <class L>
-__device__ __forceinline__ void collide_exact(const double* f, double* out, const StepParams& p, int coll) {
+__device__ __forceinline__ void collide_exact(const double* f, double* out, const StepParams& p, int coll,
+                                              double* mac) {
     constexpr int Q = L::kQ;
     double rho, ux, uy, uz;
     macro_exact<L>(f, rho, ux, uy, uz);
+    mac[0] = rho;
+    mac[1] = ux;
+    mac[2] = uy;
+    mac[3] = uz;
     double feq[Q];
     feq_exact<L>(rho, ux, uy, uz, feq);
     if (coll == kSrt) {
@@ -208,7 +215,7 @@ __device__ __forceinline__ float signed_dot(int q, float ux, float uy, float uz)
 }
 
 template <class L>
-__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float scale, float inv_scale) {
+__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float scale, float inv_scale, float* mac) {
     // d are deviations times `scale`; neq is returned in the same units
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
@@ -223,6 +230,10 @@ __device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float sc
     const float rho = fmaf(drho, inv_scale, 1.f);
     const float k = inv_scale / rho;
     const float ux = jx * k, uy = jy * k, uz = jz * k;
+    mac[0] = rho;
+    mac[1] = ux;
+    mac[2] = uy;
+    mac[3] = uz;
     const float usq15 = 1.5f * (ux * ux + uy * uy + uz * uz);
     const float srho = scale * rho;
     // even part shared by opposite directions, odd part 3 w rho (c.u)
@@ -319,11 +330,11 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
 }
 
 template <class L>
-__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll) {
+__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll, float* mac) {
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float neq[Q];
-    feq_neq_dev<L>(d, neq, p.scale, p.inv_scale);
+    feq_neq_dev<L>(d, neq, p.scale, p.inv_scale, mac);
     const float omega = p.omega32;
     if (coll == kSrt) {
 #pragma unroll
@@ -468,10 +479,18 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
         }
     }
 
+    T mac[4];
     if constexpr (St::kDeviation) {
-        collide_dev<L>(pre, post, p, Coll);
+        collide_dev<L>(pre, post, p, Coll, mac);
     } else {
-        collide_exact<L>(pre, post, p, Coll);
+        collide_exact<L>(pre, post, p, Coll, mac);
+    }
+    if (Masked && (info & kInfoSaveMacro)) {
+        double* m = p.macro + (long long)self * 4;
+        m[0] = (double)mac[0];
+        m[1] = (double)mac[1];
+        m[2] = (double)mac[2];
+        m[3] = (double)mac[3];
     }
 
     int faces = 0;

@@ -4,6 +4,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <algorithm>
 #include <vector>
 #include "zllbm_b200.h"
 #include "topology.cuh"
@@ -39,6 +40,15 @@ struct Level {
     int even_layout = 0;     // 1 after an even step (see aa_kernel.cuh)
     long long nodes = 0;
     long long steps = 0;
+    std::vector<uint64_t> codes;  // sorted node codes (kept for multi-level set-ups)
+    // coarse/fine transfer with the next coarser level (this level is the fine side)
+    DeviceBuffer macro;                                   // rho, u of transfer sources
+    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_fine, c2f_w;
+    int n_c2f = 0;
+    DeviceBuffer f2c_coarse, f2c_fine;
+    int n_f2c = 0;
+    bool has_transfer = false;
+    double tau_c2f = 0., tau_f2c = 0.;
 };
 
 }  // namespace
@@ -320,7 +330,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     if ((rc = read_flag(ctx, &bad))) return rc;
     if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
     const long long box_nodes = (long long)geo.n[0] * geo.n[1] * geo.n[2];
-    if ((long long)present == box_nodes) {
+    if ((long long)present == box_nodes && ctx->cfg.max_level == 0) {
         L.info.release();
     } else {
         geo.info = (const uint32_t*)L.info.ptr;
@@ -389,6 +399,13 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     L.map = map;
     L.even_layout = 0;
     L.steps = 0;
+    L.has_transfer = false;
+    L.codes.clear();
+    if (ctx->cfg.max_level > 0) {
+        L.codes.assign(codes, codes + n);
+        std::sort(L.codes.begin(), L.codes.end());
+        L.codes.erase(std::unique(L.codes.begin(), L.codes.end()), L.codes.end());
+    }
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     L.active = true;
     return ZL_OK;
@@ -479,14 +496,220 @@ int zl_step_level(zl_ctx* ctx, int level) {
     return ZL_OK;
 }
 
+int zl_transfer_levels(zl_ctx* ctx, int fine_level) {
+    int rc = check_level(ctx, fine_level, true);
+    if (rc) return rc;
+    if (fine_level < 1) return fail(ctx, ZL_EINVAL, "level %d has no coarser level", fine_level);
+    Level& F = ctx->levels[fine_level];
+    Level& C = ctx->levels[fine_level - 1];
+    if (!F.has_transfer) return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface first", fine_level);
+    C2FStencil st{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
+                  (const uint8_t*)F.c2f_fine.ptr, (const double*)F.c2f_w.ptr, F.n_c2f};
+    ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
+                               C.params, st, F.tau_c2f, ctx->stream));
+    ZL_CUDA(ctx, ctx->ops->f2c(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
+                               C.params, (const int*)F.f2c_coarse.ptr, (const int*)F.f2c_fine.ptr, F.n_f2c,
+                               (const double*)F.macro.ptr, F.tau_f2c, ctx->stream));
+    return ZL_OK;
+}
+
+// Sub-cycled order of one background step (MultiTimeSteppingC2F, amr_project/grid/grid_manager.cpp:997-1023):
+// level l is followed by two sweeps of level l + 1.
+static void time_stepping_order(int level, int max_level, std::vector<int>* order) {
+    order->push_back(level);
+    if (level < max_level) {
+        time_stepping_order(level + 1, max_level, order);
+        time_stepping_order(level + 1, max_level, order);
+    }
+}
+
 int zl_advance(zl_ctx* ctx, int steps) {
     if (!ctx || steps < 0) return ZL_EINVAL;
-    if (ctx->cfg.max_level != 0)
-        return fail(ctx, ZL_ESTATE, "multi-level stepping needs the coarse/fine transfer set-up");
+    std::vector<int> order;
+    time_stepping_order(0, ctx->cfg.max_level, &order);
+    for (int l = 1; l <= ctx->cfg.max_level; ++l)
+        if (!ctx->levels[l].has_transfer)
+            return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface before zl_advance", l);
     for (int s = 0; s < steps; ++s) {
-        int rc = zl_step_level(ctx, 0);
-        if (rc) return rc;
+        int count[ZL_MAX_LEVELS] = {0};
+        for (int l : order) {
+            ++count[l];
+            int rc = zl_step_level(ctx, l);
+            if (rc) return rc;
+            // InformationFromGridOfDifferentLevel (lbm_solver_interface.cpp:224-238)
+            if (l > 0 && count[l] % 2 == 0) {
+                rc = zl_transfer_levels(ctx, l);
+                if (rc) return rc;
+            }
+        }
     }
+    return ZL_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// cell index of a code on a level box, or -1 when the level has no such node
+long long cell_of_code(const Level& L, int dims, uint64_t code) {
+    if (!std::binary_search(L.codes.begin(), L.codes.end(), code)) return -1;
+    uint32_t idx[3];
+    zl::morton_decode(code, dims, idx);
+    long long b[3] = {0, 0, 0};
+    for (int a = 0; a < dims; ++a) {
+        long long v = (long long)idx[a] - L.map.lo[a];
+        if (L.map.periodic[a] && v == L.map.n[a]) v = 0;
+        if (v < 0 || v >= L.map.n[a]) return -1;
+        b[a] = v + L.geo.g[a];
+    }
+    return b[0] + (long long)L.geo.a[0] * (b[1] + (long long)L.geo.a[1] * b[2]);
+}
+
+// Lagrangian coefficients of half length 2 at the mid point (grid/grid_interpolation.cpp:87-112)
+void lagrange_mid(double* c) {
+    const int len = 2, num = 2 * len, offset = len - 1;
+    for (int iy = 0; iy < num; ++iy) {
+        c[iy] = 1.;
+        const double y = (double)iy;
+        for (int ix = 0; ix < num; ++ix) {
+            if (iy == ix) continue;
+            const double x = (double)ix;
+            c[iy] *= (0.5 + offset - x) / (y - x);
+        }
+    }
+}
+
+__global__ void or_bits_kernel(uint32_t* info, const int* cells, int n, uint32_t bits) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) info[cells[i]] |= bits;
+}
+
+template <class T>
+int upload_vec(zl_ctx* ctx, DeviceBuffer& b, const std::vector<T>& v) {
+    int rc = alloc(ctx, b, v.size() * sizeof(T));
+    if (rc) return rc;
+    if (!v.empty()) ZL_CUDA(ctx, cudaMemcpy(b.ptr, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return ZL_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int64_t n_c2f,
+                           const uint64_t* f2c_coarse, int64_t n_f2c, const uint64_t* coarse_excluded,
+                           int64_t n_excluded) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (level < 1) return fail(ctx, ZL_EINVAL, "interfaces belong to levels >= 1");
+    if ((rc = check_level(ctx, level - 1, true))) return rc;
+    if ((n_c2f > 0 && !c2f_fine) || (n_f2c > 0 && !f2c_coarse) || (n_excluded > 0 && !coarse_excluded) ||
+        n_c2f < 0 || n_f2c < 0 || n_excluded < 0)
+        return fail(ctx, ZL_EINVAL, "bad interface lists");
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    const int dims = ctx->dims;
+    Level& F = ctx->levels[level];
+    Level& C = ctx->levels[level - 1];
+    std::vector<uint64_t> excluded(coarse_excluded, coarse_excluded + n_excluded);
+    std::sort(excluded.begin(), excluded.end());
+    std::vector<uint64_t> targets(c2f_fine, c2f_fine + n_c2f);
+    std::sort(targets.begin(), targets.end());
+    double mid[4], one[4] = {0., 1., 0., 0.};
+    lagrange_mid(mid);
+    const long long clo[3] = {(long long)ctx->cfg.domain_min[0] << (level - 1),
+                              (long long)ctx->cfg.domain_min[1] << (level - 1),
+                              (long long)ctx->cfg.domain_min[2] << (level - 1)};
+    const long long chi[3] = {(long long)ctx->cfg.domain_max[0] << (level - 1),
+                              (long long)ctx->cfg.domain_max[1] << (level - 1),
+                              (long long)ctx->cfg.domain_max[2] << (level - 1)};
+    std::vector<int> tgt, off(1, 0), src;
+    std::vector<uint8_t> src_fine;
+    std::vector<double> wts;
+    for (int64_t i = 0; i < n_c2f; ++i) {
+        const long long tc = cell_of_code(F, dims, c2f_fine[i]);
+        if (tc < 0) return fail(ctx, ZL_ETOPOLOGY, "level %d: interpolation target is not a node of the level", level);
+        uint32_t fidx[3], cidx[3];
+        zl::morton_decode(c2f_fine[i], dims, fidx);
+        const uint64_t ccode = c2f_fine[i] >> dims;  // SFBitsetToNLowerLevel(1)
+        zl::morton_decode(ccode, dims, cidx);
+        const double* coef[3] = {one, one, one};
+        for (int a = 0; a < dims; ++a) {
+            coef[a] = (fidx[a] & 1u) ? mid : one;
+            if ((long long)cidx[a] - 1 < clo[a] || (long long)cidx[a] + 2 > chi[a] || (long long)cidx[a] == clo[a])
+                return fail(ctx, ZL_ETOPOLOGY,
+                            "level %d: interpolation stencil reaches the domain boundary (not supported)", level);
+        }
+        const int nz = dims == 3 ? 4 : 1;
+        for (int iz = 0; iz < nz; ++iz)
+            for (int iy = 0; iy < 4; ++iy)
+                for (int ix = 0; ix < 4; ++ix) {
+                    const double w = dims == 3 ? coef[0][ix] * coef[1][iy] * coef[2][iz] : coef[0][ix] * coef[1][iy];
+                    if (!(std::fabs(w) > 1e-6)) continue;
+                    uint32_t r[3] = {cidx[0] + ix - 1, cidx[1] + iy - 1, dims == 3 ? cidx[2] + iz - 1 : 0u};
+                    const uint64_t rc_code = zl::morton_encode(r, dims);
+                    const long long cc = std::binary_search(excluded.begin(), excluded.end(), rc_code)
+                                             ? -1 : cell_of_code(C, dims, rc_code);
+                    if (cc >= 0) {
+                        src.push_back((int)cc);
+                        src_fine.push_back(0);
+                    } else {
+                        const uint64_t fcode = rc_code << dims;  // SFBitsetToNHigherLevel(1)
+                        const long long fc = cell_of_code(F, dims, fcode);
+                        if (fc < 0)
+                            return fail(ctx, ZL_ETOPOLOGY, "level %d: interpolation source found on neither level",
+                                        level);
+                        if (std::binary_search(targets.begin(), targets.end(), fcode))
+                            return fail(ctx, ZL_ETOPOLOGY,
+                                        "level %d: an interpolation source is itself a target (order dependent)",
+                                        level);
+                        src.push_back((int)fc);
+                        src_fine.push_back(1);
+                    }
+                    wts.push_back(w);
+                }
+        tgt.push_back((int)tc);
+        off.push_back((int)src.size());
+    }
+    std::vector<int> f2c_c, f2c_f;
+    for (int64_t i = 0; i < n_f2c; ++i) {
+        const long long cc = cell_of_code(C, dims, f2c_coarse[i]);
+        const long long fc = cell_of_code(F, dims, f2c_coarse[i] << dims);
+        if (cc < 0 || fc < 0)
+            return fail(ctx, ZL_ETOPOLOGY, "level %d: coalescence node missing on the fine or coarse level", level);
+        f2c_c.push_back((int)cc);
+        f2c_f.push_back((int)fc);
+    }
+    if ((rc = upload_vec(ctx, F.c2f_target, tgt)) || (rc = upload_vec(ctx, F.c2f_offset, off)) ||
+        (rc = upload_vec(ctx, F.c2f_src, src)) || (rc = upload_vec(ctx, F.c2f_fine, src_fine)) ||
+        (rc = upload_vec(ctx, F.c2f_w, wts)) || (rc = upload_vec(ctx, F.f2c_coarse, f2c_c)) ||
+        (rc = upload_vec(ctx, F.f2c_fine, f2c_f)))
+        return rc;
+    F.n_c2f = (int)tgt.size();
+    F.n_f2c = (int)f2c_c.size();
+    // coalescence sources keep rho, u of their last collision
+    if (F.n_f2c > 0) {
+        const long long cells = (long long)F.geo.a[0] * F.geo.a[1] * F.geo.a[2];
+        if ((rc = alloc(ctx, F.macro, (size_t)cells * 4 * sizeof(double)))) return rc;
+        ZL_CUDA(ctx, cudaMemset(F.macro.ptr, 0, (size_t)cells * 4 * sizeof(double)));
+        F.params.macro = (double*)F.macro.ptr;
+        or_bits_kernel<<<(F.n_f2c + 127) / 128, 128, 0, ctx->stream>>>((uint32_t*)F.info.ptr,
+                                                                        (const int*)F.f2c_fine.ptr, F.n_f2c,
+                                                                        kInfoSaveMacro);
+        ZL_CUDA(ctx, cudaGetLastError());
+    }
+    // relaxation-time ratios (collision_model/lbm_collision_models.cpp:142-151)
+    const double vis = ctx->cfg.viscosity;
+    const double dt_c = 1. / (double)(1u << (level - 1)), dt_f = 1. / (double)(1u << level);
+    {
+        const double tf = vis * 3. / dt_c * 2. + 0.5, tc = vis * 3. / dt_c + 0.5;
+        F.tau_c2f = 0.5 * tf / tc;  // the coarse level's tau_stream_c2f
+    }
+    {
+        const double tf = vis * 3. / dt_f + 0.5, tc = vis * 3. / dt_f / 2 + 0.5;
+        F.tau_f2c = 2. * tc / tf;   // the fine level's tau_stream_f2c
+    }
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    F.has_transfer = true;
     return ZL_OK;
 }
 

@@ -24,6 +24,12 @@ struct LaunchSet {
                           int* bad, cudaStream_t s);
     cudaError_t (*conservation)(int dims, const void* f, const LevelGeom& geo, const StepParams& p,
                                 int even_layout, double* partial, int nblocks, double* out, cudaStream_t s);
+    cudaError_t (*c2f)(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc, const LevelGeom& cgeo,
+                       int c_even, const StepParams& fp, const StepParams& cp, const C2FStencil& st, double tau_ratio,
+                       cudaStream_t s);
+    cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
+                       int c_even, const StepParams& fp, const StepParams& cp, const int* coarse_cell,
+                       const int* fine_cell, int n, const double* fine_macro, double tau_ratio, cudaStream_t s);
 };
 
 const LaunchSet& launch_set_f64();
@@ -136,12 +142,40 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
         conservation_final_kernel<<<1, 32, 0, s>>>(partial, nblocks, out);                                       \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
+    cudaError_t c2f_any(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc,                   \
+                        const LevelGeom& cgeo, int c_even, const StepParams& fp, const StepParams& cp,           \
+                        const C2FStencil& st, double tau_ratio, cudaStream_t s) {                                \
+        if (st.n_targets <= 0) return cudaSuccess;                                                               \
+        const unsigned blocks = (unsigned)((st.n_targets + 127) / 128);                                          \
+        if (dims == 2)                                                                                           \
+            c2f_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp, cp, \
+                                                       st, tau_ratio);                                           \
+        else                                                                                                     \
+            c2f_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp,    \
+                                                        cp, st, tau_ratio);                                      \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    cudaError_t f2c_any(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc,                   \
+                        const LevelGeom& cgeo, int c_even, const StepParams& fp, const StepParams& cp,           \
+                        const int* coarse_cell, const int* fine_cell, int n, const double* fine_macro,           \
+                        double tau_ratio, cudaStream_t s) {                                                      \
+        if (n <= 0) return cudaSuccess;                                                                          \
+        const unsigned blocks = (unsigned)((n + 127) / 128);                                                     \
+        if (dims == 2)                                                                                           \
+            f2c_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp, \
+                                                       coarse_cell, fine_cell, n, fine_macro, tau_ratio);        \
+        else                                                                                                     \
+            f2c_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,    \
+                                                        cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);   \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
     }                                                                                                            \
     const LaunchSet& NAME() {                                                                                    \
         static const LaunchSet set = {(int)sizeof(S), NAME##_impl::step_any, NAME##_impl::neq_any,                \
                                       NAME##_impl::face_any,                                                     \
                                       NAME##_impl::scatter_any, NAME##_impl::gather_any,                         \
-                                      NAME##_impl::conservation_any};                                            \
+                                      NAME##_impl::conservation_any, NAME##_impl::c2f_any,                       \
+                                      NAME##_impl::f2c_any};                                                     \
         return set;                                                                                              \
     }
 

@@ -43,6 +43,19 @@ __device__ __forceinline__ bool code_to_node(uint64_t code, const LevelMap& m, C
     return true;
 }
 
+// Node coordinates of a box cell index (inverse of the box indexing, ghost frame removed).
+__device__ __forceinline__ Coord cell_coord(const LevelGeom& geo, int cell) {
+    Coord c;
+    const int bx = cell % geo.a[0];
+    const int rest = cell / geo.a[0];
+    const int by = rest % geo.a[1];
+    const int bz = rest / geo.a[1];
+    c.x[0] = bx - geo.g[0];
+    c.x[1] = by - geo.g[1];
+    c.x[2] = bz - geo.g[2];
+    return c;
+}
+
 // ---------------------------------------------------------------- deviation-form helpers
 template <class L>
 __device__ __forceinline__ void macro_dev(const float* d, float& rho, float& ux, float& uy, float& uz) {
@@ -191,6 +204,103 @@ __global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParam
         if (!enters_through<L>(q, face)) continue;
         St::store(f + post_stream_slot<L>(geo, fn.c, q, even_layout),
                   St::load(f + post_stream_slot<L>(geo, other, q, even_layout), p), p);
+    }
+}
+
+// ---------------------------------------------------------------- coarse <-> fine transfer
+// Interpolation stencil of one fine ghost node: entries [offset[t], offset[t+1]) of the source
+// arrays, in the reference's loop order (z outer, x inner, grid/grid_interpolation.cpp:485-517).
+struct C2FStencil {
+    const int* target;        // fine cell of every target node
+    const int* offset;        // n_targets + 1
+    const int* src_cell;      // coarse cell (src_fine == 0) or fine cell (src_fine == 1)
+    const uint8_t* src_fine;
+    const double* weight;
+    int n_targets;
+};
+
+// Explosion (TransferInfoFromCoarseGrid, lbm_grid_interface.cpp:408-515): every fine ghost node
+// becomes sum_k w_k g_k with g_k = feq(rho_c, u_c) + tau_c2f (f_c - feq) for a coarse source
+// (NodeInfoCoarse2fine + PostStreamCoarse2Fine, lbm_grid_interface.cpp:570-588,
+// collision_model/lbm_collision_models.cpp:244-251) or the post-stream populations of the
+// coincident fine node when the coarse node is absent or flagged.
+template <class L, class S>
+__global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, const S* __restrict__ fc, LevelGeom cgeo,
+                           int c_even, StepParams fp, StepParams cp, C2FStencil st, double tau_ratio) {
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= st.n_targets) return;
+    T acc[Q];
+#pragma unroll
+    for (int q = 0; q < Q; ++q) acc[q] = (T)0;
+    for (int k = st.offset[t]; k < st.offset[t + 1]; ++k) {
+        const T w = (T)st.weight[k];
+        T g[Q];
+        if (st.src_fine[k]) {
+            const Coord c = cell_coord(fgeo, st.src_cell[k]);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] = St::load(ff + post_stream_slot<L>(fgeo, c, q, f_even), fp);
+        } else {
+            const Coord c = cell_coord(cgeo, st.src_cell[k]);
+            T fcq[Q];
+#pragma unroll
+            for (int q = 0; q < Q; ++q) fcq[q] = St::load(fc + post_stream_slot<L>(cgeo, c, q, c_even), cp);
+            if constexpr (St::kDeviation) {
+                float rho, ux, uy, uz, deq[Q];
+                macro_dev<L>(fcq, rho, ux, uy, uz);
+                feq_dev<L>(rho, ux, uy, uz, deq);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = deq[q] + (float)tau_ratio * (fcq[q] - deq[q]);
+            } else {
+                double rho, ux, uy, uz, feq[Q];
+                macro_exact<L>(fcq, rho, ux, uy, uz);
+                feq_exact<L>(rho, ux, uy, uz, feq);
+#pragma unroll
+                for (int q = 0; q < Q; ++q) g[q] = feq[q] + tau_ratio * (fcq[q] - feq[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < Q; ++q) acc[q] = acc[q] + w * g[q];
+    }
+    const Coord c = cell_coord(fgeo, st.target[t]);
+#pragma unroll
+    for (int q = 0; q < Q; ++q) St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), acc[q], fp);
+}
+
+// Coalescence (TransferInfoToCoarseGrid, lbm_grid_interface.cpp:524-564): a coarse node of the
+// inner coarse-to-fine layer takes rho, u of the coincident fine node (as stored by its last
+// collision) and f = feq + tau_f2c (f_fine - feq) (NodeInfoFine2Coarse + PostStreamFine2Coarse,
+// lbm_grid_interface.cpp:594-610, lbm_collision_models.cpp:259-267).
+template <class L, class S>
+__global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, S* __restrict__ fc, LevelGeom cgeo,
+                           int c_even, StepParams fp, StepParams cp, const int* __restrict__ coarse_cell,
+                           const int* __restrict__ fine_cell, int n, const double* __restrict__ fine_macro,
+                           double tau_ratio) {
+    using St = Storage<S>;
+    constexpr int Q = L::kQ;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const Coord cf = cell_coord(fgeo, fine_cell[t]);
+    const Coord cc = cell_coord(cgeo, coarse_cell[t]);
+    const double* mac = fine_macro + (long long)fine_cell[t] * 4;
+    if constexpr (St::kDeviation) {
+        float deq[Q];
+        feq_dev<L>((float)mac[0], (float)mac[1], (float)mac[2], (float)mac[3], deq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const float v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
+            St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), deq[q] + (float)tau_ratio * (v - deq[q]), cp);
+        }
+    } else {
+        double feq[Q];
+        feq_exact<L>(mac[0], mac[1], mac[2], mac[3], feq);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
+            St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), feq[q] + tau_ratio * (v - feq[q]), cp);
+        }
     }
 }
 
