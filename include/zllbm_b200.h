@@ -94,6 +94,13 @@ typedef struct zl_config {
     double init_velocity[3];   /* default velocity: nodes start at feq(rho0, init_velocity)
                                   (SetDefaultVelocity, lbm_interface.h:300) */
     double storage_scale;      /* scale of FP16/BF16 deviations (0 selects the default 2^13) */
+    int forcing;               /* 1: collide with Guo forcing and per-node forces (SetNumForces /
+                                  SetConstantForce, lbm_interface.h:298-319); needed by immersed boundaries */
+    double constant_force[3];  /* SetConstantForce */
+    int les;                   /* 1: Smagorinsky LES with tau = tau0 + tau_sgs (the reference sets tau = tau_sgs,
+                                  lbm_solver_interface.cpp:291-295, which this library treats as a bug) */
+    double les_cs;             /* Smagorinsky constant (0 selects the reference's 0.16, lbm_les_models.h:49) */
+    double dx;                 /* background grid spacing (SetDomainGridSize); 0 selects 1 */
     int device;                /* CUDA device ordinal */
 } zl_config;
 
@@ -192,6 +199,20 @@ int zl_upstream_index(int lattice, const uint64_t* codes, int64_t n, int64_t* ou
 /* The MRT collision matrix M^-1 S M for relaxation time tau, built in the reference's loop
    order (collision_model/lbm_collision_model_mrt.cpp:63-82); out holds q * q doubles. */
 int zl_mrt_matrix(int lattice, double tau, double* out);
+
+/* ---- immersed boundary (FsiImmersedBoundary, lbm_project/immersed_boundary/immersed_boundary.cpp) ---- */
+
+/* Lagrangian vertices of the immersed-boundary geometries of a level (config->forcing must be 1):
+   coordinates and velocities as the reference's GeometryVertexImmersedBoundary coordinate_ /
+   velocity_ (n * 3 doubles, domain offset included), area_ (n doubles).  Every later step of the
+   level starts with the direct-forcing pass (CalculateBodyForce, :35-364, delta kernel of
+   stencil half-width 2, StencilDisTwo :372-384). */
+int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordinates, const double* velocity,
+                       const double* area);
+
+/* Vertex forces of the last forcing pass (n * 3, may be NULL) and their sum F area / dx^(d-1)
+   in FP64 (total[3], may be NULL; WriteTimeHisLagrangianForce, :596-642). */
+int zl_ib_get_forces(zl_ctx* ctx, int level, double* vertex_forces, double* total);
 
 /* ABI version of the loaded library. */
 int zl_abi_version(void);

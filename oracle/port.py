@@ -173,6 +173,9 @@ class Port:
         self.lib.zlp_mrt_matrix.argtypes = [ctypes.c_int, ctypes.c_double, dp]
         self.lib.zlp_tau.argtypes = [ctypes.c_double, ctypes.c_int]
         self.lib.zlp_tau.restype = ctypes.c_double
+        self.lib.zlp_smag_tau_sgs.argtypes = [ctypes.c_int, dp, dp, ctypes.c_double, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_int, dp, dp]
+        self.lib.zlp_smag_tau_sgs.restype = ctypes.c_double
 
     @staticmethod
     def _ptr(a: np.ndarray):
@@ -209,6 +212,13 @@ class Port:
         out = np.empty(q * q)
         self.lib.zlp_mrt_matrix(dims, tau, self._ptr(out))
         return out.reshape(q, q)
+
+    def smag_tau_sgs(self, dims, f, feq, tau0, dt, cs, force=None, u=None) -> float:
+        f, feq = np.ascontiguousarray(f, dtype=np.float64), np.ascontiguousarray(feq, dtype=np.float64)
+        F = np.zeros(3) if force is None else np.ascontiguousarray(force, dtype=np.float64)
+        uu = np.zeros(3) if u is None else np.ascontiguousarray(u, dtype=np.float64)
+        return float(self.lib.zlp_smag_tau_sgs(dims, self._ptr(f), self._ptr(feq), tau0, dt, cs,
+                                               1 if force is not None else 0, self._ptr(F), self._ptr(uu)))
 
     def tau(self, nu: float, level: int = 0) -> float:
         return float(self.lib.zlp_tau(nu, level))

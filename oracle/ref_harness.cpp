@@ -28,6 +28,9 @@
 #include "d3q19_model/lbm_d3q19.h"
 #include "criterion/geometry_info_origin.h"
 #include "criterion/geometry_default_shape.h"
+#include "immersed_boundary/immersed_boundary.h"
+#include "immersed_boundary/geometry_ib_shape.h"
+#include "les_models/lbm_les_models.h"
 
 using namespace rootproject;
 using amrproject::EDomainBoundaryDirection;
@@ -171,6 +174,53 @@ int morton_mode(int dims, const std::string& in, const std::string& out) {
     return 0;
 }
 
+// mode=les dims=D out=<file>: the reference's Smagorinsky increment (LesModelSmagorinsky,
+// les_models/lbm_les_smagorinsky.cpp:22-94) on deterministic pseudo-random inputs.  Record:
+// double tau0, dt, f[q], feq[q], force[3], u[3], tau_sgs_without_force, tau_sgs_with_force.
+int les_mode(int dims, const std::string& out) {
+    lbmproject::SolverLbmD2Q9 s2;
+    lbmproject::SolverLbmD3Q19 s3;
+    lbmproject::SolverLbmInterface& solver = dims == 2 ? static_cast<lbmproject::SolverLbmInterface&>(s2)
+                                                       : static_cast<lbmproject::SolverLbmInterface&>(s3);
+    const int q = solver.k0NumQ_;
+    lbmproject::LesModelSmagorinsky model;
+    const lbmproject::LesModelInterface& les = model;
+    uint64_t state = 20261203ull;
+    auto next = [&state]() {
+        state = state * 6364136223846793005ull + 1442695040888963407ull;
+        return static_cast<double>(state >> 11) / 9007199254740992.;
+    };
+    FILE* fp = std::fopen(out.c_str(), "wb");
+    for (int sample = 0; sample < 200; ++sample) {
+        lbmproject::GridNodeLbm node;
+        node.f_.resize(q);
+        node.velocity_.assign(dims, 0.);
+        std::vector<double> feq(q), force(3);
+        const double tau0 = 0.5 + next();
+        const double dt = 1. / static_cast<double>(1 << (sample % 3));
+        for (int i = 0; i < q; ++i) {
+            feq[i] = solver.k0Weights_[i] * (1. + 0.1 * (next() - 0.5));
+            node.f_[i] = feq[i] + 0.01 * (next() - 0.5);
+        }
+        for (int a = 0; a < 3; ++a) force[a] = 1e-3 * (next() - 0.5);
+        for (int a = 0; a < dims; ++a) node.velocity_[a] = 0.1 * (next() - 0.5);
+        std::vector<double> fvec(force.begin(), force.begin() + dims);
+        const double without = les.CalSgsRelaxationTimeWithoutForce(dt, tau0, feq, node, solver);
+        const double with = les.CalSgsRelaxationTimeWithForce(dt, tau0, feq, fvec, node, solver);
+        double u3[3] = {node.velocity_[0], node.velocity_[1], dims == 3 ? node.velocity_[2] : 0.};
+        std::fwrite(&tau0, 8, 1, fp);
+        std::fwrite(&dt, 8, 1, fp);
+        std::fwrite(node.f_.data(), 8, q, fp);
+        std::fwrite(feq.data(), 8, q, fp);
+        std::fwrite(force.data(), 8, 3, fp);
+        std::fwrite(u3, 8, 3, fp);
+        std::fwrite(&without, 8, 1, fp);
+        std::fwrite(&with, 8, 1, fp);
+    }
+    std::fclose(fp);
+    return 0;
+}
+
 int main(int argc, char* argv[]) {
     std::map<std::string, std::string> kv;
     std::vector<FaceBc> bcs;
@@ -192,6 +242,7 @@ int main(int argc, char* argv[]) {
     }
     const int dims = kv.count("dims") ? std::atoi(kv["dims"].c_str()) : 2;
     if (kv.count("mode") && kv["mode"] == "morton") return morton_mode(dims, kv["in"], kv["out"]);
+    if (kv.count("mode") && kv["mode"] == "les") return les_mode(dims, kv["out"]);
     const std::vector<double> n = parse_list(kv.count("n") ? kv["n"] : "16,16,16");
     const int steps = kv.count("steps") ? std::atoi(kv["steps"].c_str()) : 1;
     const std::string coll = kv.count("coll") ? kv["coll"] : "srt";
@@ -210,6 +261,48 @@ int main(int argc, char* argv[]) {
     amr->program_name_ = "zl_ref_run";
     // optional refinement around a default shape (no immersed-boundary forcing):
     //   geo=circle:cx,cy,r  or  geo=cube:cx,cy,cz,edge ; ext=<outer layers per level> ; inner=<layers>
+    // immersed-boundary geometry: ib=circle:cx,cy,r (2D) or ib=sphere:cx,cy,cz,r (3D), at level `levels`
+    std::shared_ptr<lbmproject::GeometryInfoImmersedBoundary> ib_geo;
+    if (kv.count("ib")) {
+        const std::string g = kv["ib"];
+        const std::string kind = g.substr(0, g.find(':'));
+        const std::vector<double> gp = parse_list(g.substr(g.find(':') + 1));
+        lbmproject::GeometryInfoImmersedBoundaryCreator creator;
+        amr->ptr_criterion_manager_->vec_ptr_geometries_.push_back(creator.CreateGeometryInfo(dims));
+        ib_geo = std::dynamic_pointer_cast<lbmproject::GeometryInfoImmersedBoundary>(
+            amr->ptr_criterion_manager_->vec_ptr_geometries_.back());
+        if (kind == "circle") {
+            auto shape = std::make_unique<lbmproject::GeoShapeIBCircle2D>(ib_geo);
+            shape->center_ = {gp[0], gp[1]};
+            shape->radius_ = gp[2];
+            ib_geo->ptr_geo_shape_ = std::move(shape);
+        } else {
+            auto shape = std::make_unique<lbmproject::GeoShapeIBSphere3D>(ib_geo);
+            shape->center_ = {gp[0], gp[1], gp[2]};
+            shape->radius_ = gp[3];
+            ib_geo->ptr_geo_shape_ = std::move(shape);
+        }
+        ib_geo->SetGridExtendType(amrproject::EGridExtendType::kInAndOut);
+        ib_geo->SetLevel(max_level);
+        std::vector<DefInt> ext;
+        for (double v : parse_list(kv.count("ext") ? kv["ext"] : "4")) ext.push_back(static_cast<DefInt>(v));
+        ext.resize(max_level + 1, ext.back());
+        std::vector<DefInt> inner;
+        for (double v : parse_list(kv.count("inner") ? kv["inner"] : "4")) inner.push_back(static_cast<DefInt>(v));
+        inner.resize(max_level + 1, inner.back());
+        ib_geo->SetXExtendPositive(ext);
+        ib_geo->SetXExtendNegative(ext);
+        ib_geo->SetYExtendPositive(ext);
+        ib_geo->SetYExtendNegative(ext);
+        if (dims == 3) {
+            ib_geo->SetZExtendPositive(ext);
+            ib_geo->SetZExtendNegative(ext);
+        }
+        ib_geo->SetInnerExtend(inner);
+        amr->ptr_grid_manager_->vec_ptr_tracking_info_creator_.push_back(
+            std::make_unique<amrproject::TrackingGridInfoCreatorInterface>());
+        ib_geo->SetPtrTrackingGridInfoCreator(amr->ptr_grid_manager_->vec_ptr_tracking_info_creator_.back().get());
+    }
     if (kv.count("geo") && max_level > 0) {
         const std::string g = kv["geo"];
         const std::string kind = g.substr(0, g.find(':'));
@@ -275,6 +368,15 @@ int main(int argc, char* argv[]) {
         }
     }
     if (kv.count("les") && kv["les"] == "1") solver.SetLesModel(lbmproject::ELbmLesModelType::kSmagorinsky);
+    if (ib_geo || kv.count("forces")) {
+        for (auto& g : amr->ptr_grid_manager_->vec_ptr_grid_info_) (void)g;
+        solver.SetNumForces(dims);
+    }
+    if (kv.count("cforce")) {
+        std::vector<double> cf = parse_list(kv["cforce"]);
+        cf.resize(dims, 0.);
+        solver.SetConstantForce(cf);
+    }
     solver.SetDefaultViscosity(nu);
     solver.SetDefaultDensity(rho0);
     solver.SetDefaultVelocity(vel0);
@@ -319,6 +421,24 @@ int main(int argc, char* argv[]) {
             it.second->velocity_ = u;
         }
     }
+    auto dump_vertices = [&](const std::string& path) {
+        // int64 n, then per vertex (sorted by key): double coord[3], vel[3], area, force[3]
+        FILE* fp = std::fopen(path.c_str(), "wb");
+        std::vector<std::pair<DefSizet, lbmproject::GeometryVertexImmersedBoundary*>> vs;
+        for (auto& [key, v] : ib_geo->map_vertices_info_)
+            vs.emplace_back(key, dynamic_cast<lbmproject::GeometryVertexImmersedBoundary*>(v.get()));
+        std::sort(vs.begin(), vs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        int64_t n = static_cast<int64_t>(vs.size());
+        std::fwrite(&n, sizeof(n), 1, fp);
+        for (auto& [key, v] : vs) {
+            double rec[10] = {v->coordinate_[0], v->coordinate_[1], dims == 3 ? v->coordinate_[2] : 0.,
+                              v->velocity_[0], v->velocity_[1], v->velocity_[2], v->area_,
+                              v->force_[0], v->force_[1], v->force_[2]};
+            std::fwrite(rec, sizeof(rec), 1, fp);
+        }
+        std::fclose(fp);
+    };
+    if (ib_geo && kv.count("vout0")) dump_vertices(kv["vout0"]);
     if (kv.count("lout0")) dump_levels(kv["lout0"], dims, q, *amr->ptr_grid_manager_);
     if (kv.count("out0")) dump(kv["out0"], dims, q, grid0);
     const int warmup = kv.count("warmup") ? std::atoi(kv["warmup"].c_str()) : 0;
@@ -328,6 +448,7 @@ int main(int argc, char* argv[]) {
     auto t1 = std::chrono::steady_clock::now();
     if (kv.count("out")) dump(kv["out"], dims, q, grid0);
     if (kv.count("lout")) dump_levels(kv["lout"], dims, q, *amr->ptr_grid_manager_);
+    if (ib_geo && kv.count("vout")) dump_vertices(kv["vout"]);
     if (kv.count("timing")) {
         const double sec = std::chrono::duration<double>(t1 - t0).count();
         std::printf("{\"nodes\": %zu, \"steps\": %d, \"seconds\": %.6f}\n", grid0.map_grid_node_.size(), steps, sec);

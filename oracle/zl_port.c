@@ -247,6 +247,18 @@ static double smag_tau_sgs(const lattice* l, const zlp_level* c, double dt, doub
     return 0.5 * (sqrt(tau0 * tau0 + cs * sqrt(2. * pi2)) - tau0);
 }
 
+double zlp_smag_tau_sgs(int dims, const double* f, const double* feq, double tau0, double dt, double cs,
+                        int has_force, const double* force, const double* u) {
+    const lattice l = lattice_of(dims);
+    zlp_level c;
+    memset(&c, 0, sizeof(c));
+    c.dims = dims;
+    c.les_cs = cs;
+    c.has_force = has_force;
+    for (int a = 0; a < 3; ++a) c.force[a] = force ? force[a] : 0.;
+    return smag_tau_sgs(&l, &c, dt, tau0, f, feq, u);
+}
+
 static void forcing_term(const lattice* l, const double* u, const double* F, double* out) {
     for (int iq = 0; iq < l->q; ++iq) {
         if (l->dims == 2) {

@@ -55,6 +55,11 @@ void zlp_feq(int dims, double rho, const double* u, double* feq);
  * (collision_model/lbm_collision_model_mrt.cpp:63-82); out is q*q row-major. */
 void zlp_mrt_matrix(int dims, double tau, double* out);
 
+/* The Smagorinsky increment tau_sgs (les_models/lbm_les_smagorinsky.cpp:22-94) for one node,
+   with the constant C = 18 cs^2; force and u are read only when has_force is set. */
+double zlp_smag_tau_sgs(int dims, const double* f, const double* feq, double tau0, double dt, double cs,
+                        int has_force, const double* force, const double* u);
+
 /* Relaxation time at a level, tau = 3 nu / dt + 0.5 (lbm_collision_models.cpp:114-118). */
 double zlp_tau(double nu, int level);
 

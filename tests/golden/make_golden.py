@@ -74,14 +74,38 @@ AMR_CASES = {
 }
 
 
+# immersed boundary (reference GeometryInfoImmersedBoundary, direct forcing every sub-step of its level)
+AMR_CASES.update({
+    "ib2d_l0": dict(dims=2, n=(40, 32), levels=0, ib="circle:20.5,16.5,3", ext=3, inner=2, coll="srt", nu=0.02,
+                    bc=["xmin:neq:0.05,0", "xmax:neq:0.05,0", "ymin:bb", "ymax:bb"], steps=8),
+    "ib2d_l1": dict(dims=2, n=(48, 40), levels=1, ib="circle:24.3,20.1,2.5", ext=3, inner=2, coll="mrt", nu=0.01,
+                    bc=["xmin:neq:0.04,0", "xmax:neq:0.04,0", "ymin:bb", "ymax:bb"], steps=4),
+    "ib3d_l0": dict(dims=3, n=(20, 16, 16), levels=0, ib="sphere:10.2,8.1,7.9,2.5", ext=2, inner=1, coll="srt",
+                    nu=0.03, bc=["xmin:neq:0.05,0,0", "xmax:neq:0.05,0,0", "ymin:bb", "ymax:bb", "zmin:bb", "zmax:bb"],
+                    steps=4),
+    # constant body force (SetConstantForce), periodic channel
+    "force2d_mrt": dict(dims=2, n=(12, 10), levels=0, coll="mrt", nu=0.05, cforce="1e-4,2e-5",
+                        bc=["xmin:per", "xmax:per", "ymin:bb", "ymax:bb"], steps=40),
+    "force3d_srt": dict(dims=3, n=(8, 9, 7), levels=0, coll="srt", nu=0.05, cforce="1e-4,0,-3e-5",
+                        bc=["xmin:per", "xmax:per", "ymin:bb", "ymax:bb", "zmin:per", "zmax:per"], steps=30),
+})
+
+
 def run_amr(name, case, tmp):
     from oracle.port import load_levels
     wd = os.path.join(tmp, name)
     os.makedirs(wd, exist_ok=True)
     args = [REF_RUN, f"dims={case['dims']}", "n=" + ",".join(str(v) for v in case["n"]), f"levels={case['levels']}",
-            f"geo={case['geo']}", f"ext={case['ext']}", f"inner={case['inner']}", f"coll={case['coll']}",
-            f"nu={case['nu']!r}", f"steps={case['steps']}", "lout0=" + os.path.join(wd, "l0.bin"),
-            "lout=" + os.path.join(wd, "l1.bin")] + [f"bc={b}" for b in case["bc"]]
+            f"coll={case['coll']}", f"nu={case['nu']!r}", f"steps={case['steps']}",
+            "lout0=" + os.path.join(wd, "l0.bin"), "lout=" + os.path.join(wd, "l1.bin")] + \
+           [f"bc={b}" for b in case["bc"]]
+    for key in ("geo", "ib", "ext", "inner", "cforce"):
+        if key in case:
+            args.append(f"{key}={case[key]}")
+    if "ib" in case:
+        args += ["vout0=" + os.path.join(wd, "v0.bin"), "vout=" + os.path.join(wd, "v1.bin")]
+    if "cforce" in case:
+        args.append("forces=1")
     subprocess.run(args, check=True, cwd=wd, stdout=subprocess.DEVNULL)
     dims, q, before = load_levels(os.path.join(wd, "l0.bin"))
     _, _, after = load_levels(os.path.join(wd, "l1.bin"))
@@ -97,6 +121,11 @@ def run_amr(name, case, tmp):
         out[f"c2f_fine{lv}"] = np.union1d(np.union1d(lay.get((2, 1), empty), lay.get((3, 1), empty)),
                                           np.union1d(lay.get((2, 2), empty), lay.get((3, 2), empty)))
         out[f"f2c_coarse{lv}"] = np.union1d(lay.get((0, 1), empty), lay.get((1, 1), empty))
+    if "ib" in case:
+        for tag, fn in (("before", "v0.bin"), ("after", "v1.bin")):
+            raw = open(os.path.join(wd, fn), "rb").read()
+            nv = int(np.frombuffer(raw[:8], np.int64)[0])
+            out[f"vertices_{tag}"] = np.frombuffer(raw[8:], np.float64, count=nv * 10).reshape(nv, 10)
     np.savez_compressed(os.path.join(HERE, f"amr_{name}.npz"), **out)
     print(name, [len(l["nodes"]) for l in before], "nodes per level")
 
@@ -134,6 +163,14 @@ def main():
             print(name, before.size, "nodes")
         for name, case in AMR_CASES.items():
             run_amr(name, case, tmp)
+        for dims in (2, 3):
+            fout = os.path.join(tmp, f"les{dims}.bin")
+            subprocess.run([REF_RUN, "mode=les", f"dims={dims}", f"out={fout}"], check=True, cwd=tmp,
+                           stdout=subprocess.DEVNULL)
+            q = 9 if dims == 2 else 19
+            np.savez_compressed(os.path.join(HERE, f"les_{dims}d.npz"),
+                                records=np.fromfile(fout, np.float64).reshape(-1, 2 + 2 * q + 3 + 3 + 2))
+            print("les", dims)
         rng = np.random.default_rng(20261203)
         for dims in (2, 3):
             codes = morton_cases(dims, rng)

@@ -35,10 +35,13 @@ def config(meta, storage):
             v = [float(x) for x in parts[2].split(",")]
             vels[f] = tuple(v + [0.0] * (3 - len(v)))
     hi = [c + 1 for c in meta["n"]] + [0] * (3 - dims)
+    cforce = [float(x) for x in meta["cforce"].split(",")] if "cforce" in meta else [0.0, 0.0, 0.0]
     return zl.SolverConfig(lattice=zl.D2Q9 if dims == 2 else zl.D3Q19,
                            collision=zl.MRT if meta["coll"] == "mrt" else zl.SRT, storage=storage,
                            max_level=meta["levels"], viscosity=meta["nu"], bc_kind=tuple(kinds),
-                           bc_velocity=tuple(vels), domain_min=(1, 1, 1 if dims == 3 else 0), domain_max=tuple(hi))
+                           bc_velocity=tuple(vels), domain_min=(1, 1, 1 if dims == 3 else 0), domain_max=tuple(hi),
+                           forcing=1 if ("ib" in meta or "cforce" in meta) else 0,
+                           constant_force=tuple(cforce + [0.0] * (3 - len(cforce))))
 
 
 def test_amr_fixture_layers_are_consistent():
@@ -50,7 +53,7 @@ def test_amr_fixture_layers_are_consistent():
             assert z[f"c2f_fine{lv}"].size > 0 and z[f"f2c_coarse{lv - 1}"].size > 0
 
 
-def run(meta, z, storage):
+def run(meta, z, storage, with_forces=False):
     import zllbm_b200 as zl
     levels = meta["levels"]
     with zl.Context(config(meta, storage)) as ctx:
@@ -61,19 +64,36 @@ def run(meta, z, storage):
             coarse_flags = z[f"flags{lv - 1}"]
             excluded = z[f"codes{lv - 1}"][(coarse_flags & 4) != 0]
             ctx.set_level_interface(lv, z[f"c2f_fine{lv}"], z[f"f2c_coarse{lv - 1}"], excluded)
+        if "ib" in meta:
+            v = z["vertices_before"]
+            ctx.ib_set_vertices(levels, v[:, 0:3], v[:, 3:6], v[:, 6])
         ctx.advance(meta["steps"])
-        return [ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)]
+        pops = [ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)]
+        forces = ctx.ib_get_forces(levels) if "ib" in meta else None
+    return (pops, forces) if with_forces else pops
 
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", AMR)
 def test_amr_fp64_bit_exact_against_reference(name):
+    """FP64: bit-exact, except immersed-boundary runs, whose node forces are sums over vertices
+    in an order the reference takes from an unordered_map (tolerance 1e-12 relative)."""
     import zllbm_b200 as zl
     meta, z = load_amr(name)
-    got = run(meta, z, zl.STORAGE_F64)
+    got, forces = run(meta, z, zl.STORAGE_F64, with_forces=True)
     for lv, f in enumerate(got):
         ref = z[f"f_after{lv}"]
-        assert np.array_equal(f, ref), (lv, float(np.abs(f - ref).max()))
+        if "ib" in meta:
+            np.testing.assert_allclose(f, ref, rtol=1e-12, atol=1e-15, err_msg=f"level {lv}")
+        else:
+            assert np.array_equal(f, ref), (lv, float(np.abs(f - ref).max()))
+    if "ib" in meta:
+        vf, total = forces
+        ref = z["vertices_after"][:, 7:10]
+        np.testing.assert_allclose(vf, ref, rtol=1e-10, atol=1e-14)
+        dims = meta["dims"]
+        area = z["vertices_after"][:, 6]
+        np.testing.assert_allclose(total[:dims], (ref * area[:, None]).sum(0)[:dims], rtol=1e-10, atol=1e-14)
 
 
 @pytest.mark.gpu

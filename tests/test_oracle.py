@@ -58,3 +58,17 @@ def test_tau_and_mrt_matrix(port):
     m = port.mrt_matrix(3, 0.55)
     # conserved moments: density and momentum rows of M^-1 S M act on zero rates
     assert np.allclose(m.sum(axis=0), 0.0, atol=1e-13)
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+def test_smagorinsky_increment_against_reference(dims, port):
+    """The oracle's tau_sgs equals the reference's LesModelSmagorinsky on 200 inputs, with and
+    without forces (the reference's use of it, tau_eff = tau_sgs, is not restated: see les)."""
+    q = 9 if dims == 2 else 19
+    recs = np.load(os.path.join(GOLDEN, f"les_{dims}d.npz"))["records"]
+    for r in recs:
+        tau0, dt = r[0], r[1]
+        f, feq = r[2:2 + q], r[2 + q:2 + 2 * q]
+        F, u = r[2 + 2 * q:5 + 2 * q], r[5 + 2 * q:8 + 2 * q]
+        assert port.smag_tau_sgs(dims, f, feq, tau0, dt, 0.16) == r[8 + 2 * q]
+        assert port.smag_tau_sgs(dims, f, feq, tau0, dt, 0.16, force=F, u=u) == r[9 + 2 * q]

@@ -48,6 +48,11 @@ class ZlConfig(ctypes.Structure):
         ("domain_max", ctypes.c_int32 * 3),
         ("init_velocity", ctypes.c_double * 3),
         ("storage_scale", ctypes.c_double),
+        ("forcing", ctypes.c_int),
+        ("constant_force", ctypes.c_double * 3),
+        ("les", ctypes.c_int),
+        ("les_cs", ctypes.c_double),
+        ("dx", ctypes.c_double),
         ("device", ctypes.c_int),
     ]
 
@@ -90,6 +95,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_upstream_index": ([ctypes.c_int, u64p, i64, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
         "zl_mrt_matrix": ([ctypes.c_int, ctypes.c_double, dp], ctypes.c_int),
         "zl_moments_noalloc": ([ctypes.c_int, P, i64, P, P], ctypes.c_int),
+        "zl_ib_set_vertices": ([P, ctypes.c_int, i64, dp, dp, dp], ctypes.c_int),
+        "zl_ib_get_forces": ([P, ctypes.c_int, dp, dp], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -135,6 +142,11 @@ class SolverConfig:
     domain_max: tuple = (2, 2, 2)
     init_velocity: tuple = (0.0, 0.0, 0.0)
     storage_scale: float = 0.0
+    forcing: int = 0
+    constant_force: tuple = (0.0, 0.0, 0.0)
+    les: int = 0
+    les_cs: float = 0.0
+    dx: float = 0.0
     device: int = 0
     extra: dict = field(default_factory=dict)
 
@@ -159,6 +171,12 @@ class SolverConfig:
             c.domain_max[a] = int(self.domain_max[a]) if a < len(self.domain_max) else 0
             c.init_velocity[a] = float(self.init_velocity[a]) if a < len(self.init_velocity) else 0.0
         c.storage_scale = self.storage_scale
+        c.forcing = self.forcing
+        for a in range(3):
+            c.constant_force[a] = float(self.constant_force[a]) if a < len(self.constant_force) else 0.0
+        c.les = self.les
+        c.les_cs = self.les_cs
+        c.dx = self.dx
         c.device = self.device
         return c
 
@@ -245,6 +263,21 @@ class Context:
 
     def synchronize(self):
         self._check(self.lib.zl_synchronize(self.handle))
+
+    def ib_set_vertices(self, level: int, coordinates, velocity, area):
+        c, v, a = _f64(coordinates).reshape(-1, 3), _f64(velocity).reshape(-1, 3), _f64(area).ravel()
+        c, v = np.ascontiguousarray(c), np.ascontiguousarray(v)
+        self._check(self.lib.zl_ib_set_vertices(self.handle, level, a.size, _p(c, ctypes.c_double),
+                                                _p(v, ctypes.c_double), _p(a, ctypes.c_double)))
+        self._nv = {**getattr(self, "_nv", {}), level: a.size}
+
+    def ib_get_forces(self, level: int):
+        n = self._nv[level]
+        forces = np.empty((n, 3))
+        total = np.empty(3)
+        self._check(self.lib.zl_ib_get_forces(self.handle, level, _p(forces, ctypes.c_double),
+                                              _p(total, ctypes.c_double)))
+        return forces, total
 
     def stream(self) -> int:
         """The cudaStream_t the context issues work on (as an integer handle)."""

@@ -57,6 +57,21 @@ struct StepParams {
     double scale_d;         // the same scale in FP64 (1 for FP64 / FP32 storage)
     int fuse_bb;            // bounce back applied inside the step kernel (no ordered face passes needed)
     double* macro;          // rho, ux, uy, uz per cell for nodes flagged kInfoSaveMacro (else unused)
+    // body forces (Guo forcing): F = const_force + force[cell] (GetAllForcesForANode,
+    // lbm_solver_interface.cpp:132-144); force is dims-strided by 3, or nullptr
+    const double* force;
+    double const_force[3];
+    int forced;             // the level collides with forcing (requires the masked layout)
+    double dt;              // time step of the level, 2^-level
+    const double* mrt64_d;  // dense M^-1 (I - S/2) M (FP64 forced MRT)
+    // Smagorinsky: tau = tau + tau_sgs with tau_sgs from the non-equilibrium stress
+    int les;
+    double les_c;           // 18 Cs^2
+};
+
+// Per-node extras handed to the collision.
+struct NodeForce {
+    double F[3];
 };
 
 // ---------------------------------------------------------------- storage
@@ -166,32 +181,161 @@ __device__ __forceinline__ void feq_exact(double rho, double ux, double uy, doub
     }
 }
 
+// Smagorinsky subgrid relaxation increment in the reference's arithmetic
+// (les_models/lbm_les_smagorinsky.cpp:22-94); u is the node velocity used by the collision.
+template <class L>
+__device__ __forceinline__ double smag_tau_sgs_exact(const double* f, const double* feq, double tau0, double c,
+                                                     bool forced, const double* F, double dt, double ux, double uy,
+                                                     double uz) {
+    using Tb = Tables<L>;
+    double pxx = 0., pxy = 0., pyy = 0., pzz = 0., pxz = 0., pyz = 0.;
+#pragma unroll
+    for (int q = 1; q < L::kQ; ++q) {
+        const double cx = Tb::cx(q), cy = Tb::cy(q), cz = Tb::cz(q);
+        const double d = f[q] - feq[q];
+        pxx += cx * cx * d;
+        pxy += cx * cy * d;
+        pyy += cy * cy * d;
+        if (L::kDims == 3) {
+            pzz += cz * cz * d;
+            pxz += cx * cz * d;
+            pyz += cy * cz * d;
+        }
+    }
+    if (forced) {
+        pxx += dt * F[0] * ux;
+        pyy += dt * F[1] * uy;
+        pxy += 0.5 * dt * (F[0] * ux + F[1] * uy);
+        if (L::kDims == 3) {
+            pzz += dt * F[2] * uz;
+            pxz += 0.5 * dt * (F[0] * ux + F[2] * uz);
+            pyz += 0.5 * dt * (F[1] * uy + F[2] * uz);
+        }
+    }
+    const double pi2 = pxx * pxx + pyy * pyy + pzz * pzz + 2. * (pxy * pxy + pxz * pxz + pyz * pyz);
+    return 0.5 * (sqrt(tau0 * tau0 + c * sqrt(2. * pi2)) - tau0);
+}
+
+// Element (q, s) of M^-1 S M (d_matrix: M^-1 (I - S/2) M) for relaxation 1/tau, summed over the
+// moments in the reference's order (collision_model/lbm_collision_model_mrt.cpp:63-107).
+template <class L>
+__device__ __forceinline__ double mrt_element_exact(int q, int s, double relax, bool d_matrix) {
+    using Tb = Tables<L>;
+    double acc = 0.;
+#pragma unroll
+    for (int k = 0; k < L::kQ; ++k) {
+        double sk = Tb::s(k) < 0. ? relax : Tb::s(k);
+        if (d_matrix) sk = 1. - 0.5 * sk;
+        const double im = (double)Tb::M(k, q) / (double)row_norm2<L>(k);
+        acc = acc + im * (sk * (double)Tb::M(k, s));
+    }
+    return acc;
+}
+
 template <class L>
 __device__ __forceinline__ void collide_exact(const double* f, double* out, const StepParams& p, int coll,
-                                              double* mac) {
+                                              double* mac, const NodeForce* nf) {
+    using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     double rho, ux, uy, uz;
-    macro_exact<L>(f, rho, ux, uy, uz);
+    if (nf) {
+        // CalMacroForce*Compressible (lbm_solver_interface.cpp:541-592): u += 0.5 F dt before / rho
+        rho = f[0];
+        ux = 0.;
+        uy = 0.;
+        uz = 0.;
+#pragma unroll
+        for (int q = 1; q < Q; ++q) {
+            rho = rho + f[q];
+            if (Tb::cx(q) == 1) ux = ux + f[q];
+            if (Tb::cx(q) == -1) ux = ux - f[q];
+            if (Tb::cy(q) == 1) uy = uy + f[q];
+            if (Tb::cy(q) == -1) uy = uy - f[q];
+            if (L::kDims == 3) {
+                if (Tb::cz(q) == 1) uz = uz + f[q];
+                if (Tb::cz(q) == -1) uz = uz - f[q];
+            }
+        }
+        ux = ux + 0.5 * nf->F[0] * p.dt;
+        uy = uy + 0.5 * nf->F[1] * p.dt;
+        if (L::kDims == 3) uz = uz + 0.5 * nf->F[2] * p.dt;
+        ux = ux / rho;
+        uy = uy / rho;
+        if (L::kDims == 3) uz = uz / rho;
+    } else {
+        macro_exact<L>(f, rho, ux, uy, uz);
+    }
     mac[0] = rho;
     mac[1] = ux;
     mac[2] = uy;
     mac[3] = uz;
     double feq[Q];
     feq_exact<L>(rho, ux, uy, uz, feq);
+    double fterm[Q];
+    if (nf) {
+        // CalForcingTerming2D/3D (lbm_solver_interface.cpp:443-470)
+        const double* F = nf->F;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            const double cx = Tb::cx(q), cy = Tb::cy(q), cz = Tb::cz(q);
+            if (L::kDims == 2) {
+                fterm[q] = Tb::w(q) * (3. * ((cx - ux) * F[0] + (cy - uy) * F[1])
+                                       + 9. * (ux * cx + uy * cy) * (cx * F[0] + cy * F[1]));
+            } else {
+                fterm[q] = Tb::w(q) * (3. * ((cx - ux) * F[0] + (cy - uy) * F[1] + (cz - uz) * F[2])
+                                       + 9. * (ux * cx + uy * cy + uz * cz) * (cx * F[0] + cy * F[1] + cz * F[2]));
+            }
+        }
+    }
+    double tau = p.tau;
+    if (p.les) tau = p.tau + smag_tau_sgs_exact<L>(f, feq, p.tau, p.les_c, nf != nullptr, nf ? nf->F : nullptr,
+                                                   p.dt, ux, uy, uz);
     if (coll == kSrt) {
 #pragma unroll
-        for (int q = 0; q < Q; ++q) out[q] = f[q] - (f[q] - feq[q]) / p.tau;
+        for (int q = 0; q < Q; ++q) {
+            if (nf)
+                out[q] = f[q] - (f[q] - feq[q]) / tau + (1. - 0.5 / tau) * fterm[q] * p.dt;
+            else
+                out[q] = f[q] - (f[q] - feq[q]) / tau;
+        }
     } else {
         double d[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q] = f[q] - feq[q];
-        const double* A = p.mrt64;
+        if (!p.les) {
+            const double* A = p.mrt64;
+            const double* B = p.mrt64_d;
 #pragma unroll 1
-        for (int q = 0; q < Q; ++q) {
-            double acc = 0.;
+            for (int q = 0; q < Q; ++q) {
+                double acc = 0.;
+                if (nf) {
 #pragma unroll
-            for (int s = 0; s < Q; ++s) acc = acc + __ldg(A + q * Q + s) * d[s];
-            out[q] = f[q] - acc;
+                    for (int s = 0; s < Q; ++s)
+                        acc += __ldg(A + q * Q + s) * d[s] - __ldg(B + q * Q + s) * fterm[s] * p.dt;
+                } else {
+#pragma unroll
+                    for (int s = 0; s < Q; ++s) acc = acc + __ldg(A + q * Q + s) * d[s];
+                }
+                out[q] = f[q] - acc;
+            }
+        } else {
+            // the relaxation time differs per node: build M^-1 S M on the fly
+            const double relax = 1. / tau;
+#pragma unroll 1
+            for (int q = 0; q < Q; ++q) {
+                double acc = 0.;
+#pragma unroll 1
+                for (int s = 0; s < Q; ++s) {
+                    const double a = mrt_element_exact<L>(q, s, relax, false);
+                    if (nf) {
+                        const double b = mrt_element_exact<L>(q, s, relax, true);
+                        acc += a * d[s] - b * fterm[s] * p.dt;
+                    } else {
+                        acc = acc + a * d[s];
+                    }
+                }
+                out[q] = f[q] - acc;
+            }
         }
     }
 }
@@ -215,8 +359,10 @@ __device__ __forceinline__ float signed_dot(int q, float ux, float uy, float uz)
 }
 
 template <class L>
-__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float scale, float inv_scale, float* mac) {
-    // d are deviations times `scale`; neq is returned in the same units
+__device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float scale, float inv_scale, float* mac,
+                                            const float* F = nullptr, float dt = 0.f) {
+    // d are deviations times `scale`; neq is returned in the same units; F (unscaled) shifts the
+    // velocity by F dt / 2 (Guo forcing)
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float drho = 0.f, jx = 0.f, jy = 0.f, jz = 0.f;
@@ -229,7 +375,13 @@ __device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float sc
     }
     const float rho = fmaf(drho, inv_scale, 1.f);
     const float k = inv_scale / rho;
-    const float ux = jx * k, uy = jy * k, uz = jz * k;
+    float ux = jx * k, uy = jy * k, uz = jz * k;
+    if (F) {
+        const float h = 0.5f * dt / rho;
+        ux = fmaf(h, F[0], ux);
+        uy = fmaf(h, F[1], uy);
+        uz = fmaf(h, F[2], uz);
+    }
     mac[0] = rho;
     mac[1] = ux;
     mac[2] = uy;
@@ -255,7 +407,7 @@ __device__ __forceinline__ void feq_neq_dev(const float* d, float* neq, float sc
 }
 
 __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, float* out, float omega,
-                                              const StepParams& p) {
+                                              const float* lam) {
     // pair sums / differences over opposite directions
     const float S1 = n[1] + n[2], D1 = n[1] - n[2];
     const float S2 = n[3] + n[4], D2 = n[3] - n[4];
@@ -279,11 +431,11 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
     const float m4 = -4.f * D1 + X1 + X2, m16 = X1 - X2;
     const float m6 = -4.f * D2 + Y1 + Y2, m17 = -Y1 + Y2;
     const float m8 = -4.f * D3 + Z1 + Z2, m18 = Z1 - Z2;
-    // lambda_k = (s_k - omega) / |M_k|^2 (p.mrt_coef holds them per moment)
-    const float a1 = p.mrt_coef[1] * m1, a2 = p.mrt_coef[2] * m2;
-    const float a4 = p.mrt_coef[4] * m4, a6 = p.mrt_coef[6] * m6, a8 = p.mrt_coef[8] * m8;
-    const float a10 = p.mrt_coef[10] * m10, a12 = p.mrt_coef[12] * m12;
-    const float a16 = p.mrt_coef[16] * m16, a17 = p.mrt_coef[17] * m17, a18 = p.mrt_coef[18] * m18;
+    // lambda_k = (s_k - omega) / |M_k|^2
+    const float a1 = lam[1] * m1, a2 = lam[2] * m2;
+    const float a4 = lam[4] * m4, a6 = lam[6] * m6, a8 = lam[8] * m8;
+    const float a10 = lam[10] * m10, a12 = lam[12] * m12;
+    const float a16 = lam[16] * m16, a17 = lam[17] * m17, a18 = lam[18] * m18;
     const float e_ax = -11.f * a1 - 4.f * a2;
     const float e_dg = 8.f * a1 + a2;
     float c[19];
@@ -329,48 +481,142 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
     for (int q = 0; q < 19; ++q) out[q] = fmaf(-omega, n[q], d[q]) - c[q];
 }
 
+// out_q = sum_k coef_k (M_k . x) M_kq over the moments flagged in `use` (compile-time folded basis).
+template <class L, class Use>
+__device__ __forceinline__ void moment_apply(const float* x, const float* coef, float* out, Use use) {
+    using Tb = Tables<L>;
+    constexpr int Q = L::kQ;
+    float a[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        float acc = 0.f;
+        if (use(k)) {
+#pragma unroll
+            for (int j = 0; j < Q; ++j) {
+                const int m = Tb::M(k, j);
+                if (m == 1) acc += x[j];
+                else if (m == -1) acc -= x[j];
+                else if (m != 0) acc += (float)m * x[j];
+            }
+        }
+        a[k] = acc * coef[k];
+    }
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float acc = 0.f;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            if (!use(k)) continue;
+            const int m = Tb::M(k, q);
+            if (m == 1) acc += a[k];
+            else if (m == -1) acc -= a[k];
+            else if (m != 0) acc += (float)m * a[k];
+        }
+        out[q] = acc;
+    }
+}
+
 template <class L>
-__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll, float* mac) {
+__device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll, float* mac,
+                                            const NodeForce* nf) {
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float neq[Q];
-    feq_neq_dev<L>(d, neq, p.scale, p.inv_scale, mac);
-    const float omega = p.omega32;
-    if (coll == kSrt) {
+    float F[3] = {0.f, 0.f, 0.f};
+    if (nf) {
+        F[0] = (float)nf->F[0];
+        F[1] = (float)nf->F[1];
+        F[2] = (float)nf->F[2];
+    }
+    const float dt = (float)p.dt;
+    feq_neq_dev<L>(d, neq, p.scale, p.inv_scale, mac, nf ? F : nullptr, dt);
+    float omega = p.omega32;
+    if (p.les) {
+        // non-equilibrium stress (unscaled) and Smagorinsky tau = tau0 + tau_sgs
+        float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
 #pragma unroll
-        for (int q = 0; q < Q; ++q) out[q] = fmaf(-omega, neq[q], d[q]);
-    } else if constexpr (L::kQ == 19) {
-        mrt_d3q19_dev(d, neq, out, omega, p);
-    } else {
-        // generic orthogonal-basis MRT (D2Q9): m_k for non-shear moments, mapped back with M^T
-        float ak[Q];
-#pragma unroll
-        for (int k = 0; k < Q; ++k) {
-            float acc = 0.f;
-            if (Tb::s(k) > 0.) {
-#pragma unroll
-                for (int j = 0; j < Q; ++j) {
-                    const int m = Tb::M(k, j);
-                    if (m == 1) acc += neq[j];
-                    else if (m == -1) acc -= neq[j];
-                    else if (m != 0) acc += (float)m * neq[j];
-                }
-            }
-            ak[k] = acc * p.mrt_coef[k];
+        for (int q = 1; q < Q; ++q) {
+            const int cx = Tb::cx(q), cy = Tb::cy(q), cz = Tb::cz(q);
+            if (cx) pxx += neq[q];
+            if (cy) pyy += neq[q];
+            if (cz) pzz += neq[q];
+            if (cx * cy) pxy += cx * cy > 0 ? neq[q] : -neq[q];
+            if (cx * cz) pxz += cx * cz > 0 ? neq[q] : -neq[q];
+            if (cy * cz) pyz += cy * cz > 0 ? neq[q] : -neq[q];
         }
+        const float is = p.inv_scale;
+        pxx *= is; pyy *= is; pzz *= is; pxy *= is; pxz *= is; pyz *= is;
+        if (nf) {
+            pxx += dt * F[0] * mac[1];
+            pyy += dt * F[1] * mac[2];
+            pzz += dt * F[2] * mac[3];
+            pxy += 0.5f * dt * (F[0] * mac[1] + F[1] * mac[2]);
+            pxz += 0.5f * dt * (F[0] * mac[1] + F[2] * mac[3]);
+            pyz += 0.5f * dt * (F[1] * mac[2] + F[2] * mac[3]);
+        }
+        const float pi2 = pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz);
+        const float tau0 = (float)p.tau;
+        const float tau = tau0 + 0.5f * (sqrtf(tau0 * tau0 + (float)p.les_c * sqrtf(2.f * pi2)) - tau0);
+        omega = 1.f / tau;
+    }
+    float fq[Q];
+    if (nf) {
+        // Guo forcing term, scaled to the storage units
+        const float ux = mac[1], uy = mac[2], uz = mac[3];
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
-            float acc = 0.f;
-#pragma unroll
-            for (int k = 0; k < Q; ++k) {
-                if (!(Tb::s(k) > 0.)) continue;
-                const int m = Tb::M(k, q);
-                if (m == 1) acc += ak[k];
-                else if (m == -1) acc -= ak[k];
-                else if (m != 0) acc += (float)m * ak[k];
-            }
-            out[q] = fmaf(-omega, neq[q], d[q]) - acc;
+            const float cx = (float)Tb::cx(q), cy = (float)Tb::cy(q), cz = (float)Tb::cz(q);
+            const float cu = signed_dot<L>(q, ux, uy, uz);
+            const float cF = signed_dot<L>(q, F[0], F[1], F[2]);
+            const float t = 3.f * ((cx - ux) * F[0] + (cy - uy) * F[1] + (cz - uz) * F[2]) + 9.f * cu * cF;
+            fq[q] = (float)Tb::w(q) * t * p.scale;
         }
+    }
+    if (coll == kSrt) {
+        const float g = (1.f - 0.5f * omega) * dt;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            out[q] = fmaf(-omega, neq[q], d[q]);
+            if (nf) out[q] = fmaf(g, fq[q], out[q]);
+        }
+        return;
+    }
+    float lam[Q];
+#pragma unroll
+    for (int k = 0; k < Q; ++k) {
+        if (p.les) lam[k] = Tb::s(k) > 0. ? ((float)Tb::s(k) - omega) / (float)row_norm2<L>(k) : 0.f;
+        else lam[k] = p.mrt_coef[k];
+    }
+    if constexpr (L::kQ == 19) {
+        mrt_d3q19_dev(d, neq, out, omega, lam);
+    } else {
+        float corr[Q];
+        moment_apply<L>(neq, lam, corr, [](int k) { return Tables<L>::s(k) > 0.; });
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] = fmaf(-omega, neq[q], d[q]) - corr[q];
+    }
+    if (nf) {
+        // With forcing, feq uses the force-shifted velocity, so the momentum of neq is -F dt / 2
+        // rather than zero: M^-1 S M neq = omega neq - omega P_conserved(neq) + sum_K ...
+        float cc[Q], pc[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) cc[k] = omega / (float)row_norm2<L>(k);
+        moment_apply<L>(neq, cc, pc, [](int k) { return Tables<L>::s(k) == 0.; });
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] += pc[q];
+        // M^-1 (I - S/2) M F = (1 - omega/2) F + (omega/2) P_conserved F - sum_k (s_k - omega)/2 / |M_k|^2 m^F_k M_k
+        float coef[Q];
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
+            const double sk = Tb::s(k);
+            coef[k] = sk == 0. ? 0.5f * omega / (float)row_norm2<L>(k)
+                    : (sk > 0. ? -0.5f * ((float)sk - omega) / (float)row_norm2<L>(k) : 0.f);
+        }
+        float src[Q];
+        moment_apply<L>(fq, coef, src, [](int k) { return !(Tables<L>::s(k) < 0.); });
+        const float g = 1.f - 0.5f * omega;
+#pragma unroll
+        for (int q = 0; q < Q; ++q) out[q] += dt * fmaf(g, fq[q], src[q]);
     }
 }
 
@@ -430,7 +676,7 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
 // ---------------------------------------------------------------- the step kernel
 // One thread per node of the level box.  Odd selects the layout read (see file comment).
 // Bnd: the level has at least one non-periodic axis.  Masked: the box holds absent cells.
-template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked>
+template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, bool Forced = false>
 __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
     using Tb = Tables<L>;
     using St = Storage<S>;
@@ -480,10 +726,16 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
     }
 
     T mac[4];
+    NodeForce nf;
+    if (Forced) {
+        // GetAllForcesForANode (lbm_solver_interface.cpp:132-144): constant force plus node forces
+#pragma unroll
+        for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
+    }
     if constexpr (St::kDeviation) {
-        collide_dev<L>(pre, post, p, Coll, mac);
+        collide_dev<L>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     } else {
-        collide_exact<L>(pre, post, p, Coll, mac);
+        collide_exact<L>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     }
     if (Masked && (info & kInfoSaveMacro)) {
         double* m = p.macro + (long long)self * 4;

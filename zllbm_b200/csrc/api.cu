@@ -49,6 +49,12 @@ struct Level {
     int n_f2c = 0;
     bool has_transfer = false;
     double tau_c2f = 0., tau_f2c = 0.;
+    // body forces and immersed boundary
+    DeviceBuffer force;      // node forces, 3 doubles per cell
+    DeviceBuffer mrt64_d;    // M^-1 (I - S/2) M (FP64 forced MRT)
+    DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
+    DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
+    int n_vertices = 0;
 };
 
 }  // namespace
@@ -330,7 +336,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     if ((rc = read_flag(ctx, &bad))) return rc;
     if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
     const long long box_nodes = (long long)geo.n[0] * geo.n[1] * geo.n[2];
-    if ((long long)present == box_nodes && ctx->cfg.max_level == 0) {
+    if ((long long)present == box_nodes && ctx->cfg.max_level == 0 && !ctx->cfg.forcing) {
         L.info.release();
     } else {
         geo.info = (const uint32_t*)L.info.ptr;
@@ -349,6 +355,14 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     p.tau = ctx->cfg.viscosity * 3. / dt + 0.5;
     p.rho0 = ctx->cfg.rho0;
     p.fuse_bb = L.ordered ? 0 : 1;
+    p.dt = dt;
+    p.forced = ctx->cfg.forcing ? 1 : 0;
+    for (int a = 0; a < 3; ++a) p.const_force[a] = ctx->cfg.forcing ? ctx->cfg.constant_force[a] : 0.;
+    p.les = ctx->cfg.les ? 1 : 0;
+    {
+        const double cs = ctx->cfg.les_cs > 0. ? ctx->cfg.les_cs : 0.16;
+        p.les_c = 18. * cs * cs;
+    }
     for (int f = 0; f < 6; ++f) p.face_kind[f] = ctx->cfg.bc_kind[f];
     for (int f = 0; f < 2 * dims; ++f) {
         const double* U = ctx->cfg.bc_velocity[f];
@@ -375,7 +389,19 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
         if ((rc = alloc(ctx, L.mrt64, m.size() * sizeof(double)))) return rc;
         ZL_CUDA(ctx, cudaMemcpy(L.mrt64.ptr, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
         p.mrt64 = (const double*)L.mrt64.ptr;
+        if (ctx->cfg.forcing) {
+            host_mrt_matrix(dims, 1. / p.tau, true, m.data());
+            if ((rc = alloc(ctx, L.mrt64_d, m.size() * sizeof(double)))) return rc;
+            ZL_CUDA(ctx, cudaMemcpy(L.mrt64_d.ptr, m.data(), m.size() * sizeof(double), cudaMemcpyHostToDevice));
+            p.mrt64_d = (const double*)L.mrt64_d.ptr;
+        }
     }
+    if (ctx->cfg.forcing) {
+        if ((rc = alloc(ctx, L.force, (size_t)cells * 3 * sizeof(double)))) return rc;
+        ZL_CUDA(ctx, cudaMemset(L.force.ptr, 0, (size_t)cells * 3 * sizeof(double)));
+        p.force = (const double*)L.force.ptr;
+    }
+    L.n_vertices = 0;
     std::vector<double> feq_face(6 * q, 0.);
     for (int f = 0; f < 2 * dims; ++f) host_feq(dims, ctx->cfg.rho0, ctx->cfg.bc_velocity[f], &feq_face[f * q]);
     if ((rc = alloc(ctx, L.feq_face, feq_face.size() * sizeof(double)))) return rc;
@@ -465,10 +491,13 @@ int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, do
     return exchange(ctx, level, codes, nullptr, rho, u, n, false);
 }
 
+static int ib_pass(zl_ctx* ctx, Level& L, int level);
+
 int zl_step_level(zl_ctx* ctx, int level) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
     Level& L = ctx->levels[level];
+    if (L.n_vertices > 0 && (rc = ib_pass(ctx, L, level))) return rc;
     const bool odd = L.even_layout == 1;
     ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr, L.geo,
                                 L.params, ctx->stream));
@@ -728,6 +757,97 @@ int zl_conservation(zl_ctx* ctx, int level, double* out) {
     for (int k = 0; k <= ctx->dims; ++k) out[k] = host[k];
     for (int k = 0; k <= ctx->dims; ++k)
         if (!std::isfinite(host[k])) return fail(ctx, ZL_ENAN, "non-finite conservation sum on level %d", level);
+    return ZL_OK;
+}
+
+static IbVertices ib_view(zl_ctx* ctx, Level& L, int level) {
+    IbVertices v;
+    v.coord = (const double*)L.ib_coord.ptr;
+    v.vel = (const double*)L.ib_uvel.ptr;
+    v.area = (const double*)L.ib_area.ptr;
+    v.force = (double*)L.ib_force.ptr;
+    v.n = L.n_vertices;
+    const double dx0 = ctx->cfg.dx > 0. ? ctx->cfg.dx : 1.;
+    v.dx = dx0 / (double)(1u << level);
+    return v;
+}
+
+static int ib_pass(zl_ctx* ctx, Level& L, int level) {
+    IbVertices v = ib_view(ctx, L, level);
+    int rc = reset_flag(ctx);
+    if (rc) return rc;
+    ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.map, L.params, L.even_layout, v,
+                                    (double*)L.force.ptr, (double*)L.ib_vel.ptr, (int*)ctx->scratch_flag.ptr,
+                                    ctx->stream));
+    const unsigned blocks = (unsigned)((v.n + 127) / 128);
+    if (ctx->dims == 2) {
+        ib_force_kernel<2><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<2><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+    } else {
+        ib_force_kernel<3><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<3><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+    }
+    ZL_CUDA(ctx, cudaGetLastError());
+    return ZL_OK;
+}
+
+int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordinates, const double* velocity,
+                       const double* area) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (!ctx->cfg.forcing) return fail(ctx, ZL_ESTATE, "immersed boundaries need config->forcing = 1");
+    if (n < 0 || (n > 0 && (!coordinates || !velocity || !area))) return fail(ctx, ZL_EINVAL, "bad vertex arrays");
+    Level& L = ctx->levels[level];
+    if ((rc = alloc(ctx, L.ib_coord, (size_t)n * 3 * 8)) || (rc = alloc(ctx, L.ib_uvel, (size_t)n * 3 * 8)) ||
+        (rc = alloc(ctx, L.ib_area, (size_t)n * 8)) || (rc = alloc(ctx, L.ib_force, (size_t)n * 3 * 8)) ||
+        (rc = alloc(ctx, L.ib_total, 3 * 8)))
+        return rc;
+    const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
+    if (!L.ib_vel.ptr && (rc = alloc(ctx, L.ib_vel, (size_t)cells * 3 * 8))) return rc;
+    if (n > 0) {
+        ZL_CUDA(ctx, cudaMemcpy(L.ib_coord.ptr, coordinates, (size_t)n * 3 * 8, cudaMemcpyHostToDevice));
+        ZL_CUDA(ctx, cudaMemcpy(L.ib_uvel.ptr, velocity, (size_t)n * 3 * 8, cudaMemcpyHostToDevice));
+        ZL_CUDA(ctx, cudaMemcpy(L.ib_area.ptr, area, (size_t)n * 8, cudaMemcpyHostToDevice));
+        ZL_CUDA(ctx, cudaMemset(L.ib_force.ptr, 0, (size_t)n * 3 * 8));
+    }
+    L.n_vertices = (int)n;
+    // every stencil node must exist on the level (the reference logs an error otherwise)
+    if (n > 0) {
+        IbVertices v = ib_view(ctx, L, level);
+        if ((rc = reset_flag(ctx))) return rc;
+        DeviceBuffer scratch_force, scratch_vel;
+        if ((rc = alloc(ctx, scratch_force, (size_t)cells * 3 * 8)) || (rc = alloc(ctx, scratch_vel, (size_t)cells * 3 * 8)))
+            return rc;
+        ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.map, L.params, L.even_layout, v,
+                                        (double*)scratch_force.ptr, (double*)scratch_vel.ptr,
+                                        (int*)ctx->scratch_flag.ptr, ctx->stream));
+        int bad = 0;
+        if ((rc = read_flag(ctx, &bad))) return rc;
+        if (bad) {
+            L.n_vertices = 0;
+            return fail(ctx, ZL_ETOPOLOGY, "level %d: an immersed-boundary stencil node is not on the level", level);
+        }
+    }
+    return ZL_OK;
+}
+
+int zl_ib_get_forces(zl_ctx* ctx, int level, double* vertex_forces, double* total) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    if (L.n_vertices <= 0) return fail(ctx, ZL_ESTATE, "level %d has no immersed-boundary vertices", level);
+    if (vertex_forces)
+        ZL_CUDA(ctx, cudaMemcpyAsync(vertex_forces, L.ib_force.ptr, (size_t)L.n_vertices * 3 * 8,
+                                     cudaMemcpyDeviceToHost, ctx->stream));
+    if (total) {
+        IbVertices v = ib_view(ctx, L, level);
+        const double dx0 = ctx->cfg.dx > 0. ? ctx->cfg.dx : 1.;
+        const double scale = ctx->dims == 3 ? 1. / dx0 / dx0 : 1. / dx0;
+        ib_total_kernel<<<1, 32, 0, ctx->stream>>>(v, scale, (double*)L.ib_total.ptr);
+        ZL_CUDA(ctx, cudaGetLastError());
+        ZL_CUDA(ctx, cudaMemcpyAsync(total, L.ib_total.ptr, 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return ZL_OK;
 }
 

@@ -3,7 +3,7 @@
 // arithmetic follows the reference's rounding step for step).
 #pragma once
 #include <cuda_runtime.h>
-#include "level_ops.cuh"
+#include "ib.cuh"
 
 namespace zl {
 
@@ -30,6 +30,9 @@ struct LaunchSet {
     cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const int* coarse_cell,
                        const int* fine_cell, int n, const double* fine_macro, double tau_ratio, cudaStream_t s);
+    cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const LevelMap& m, const StepParams& p,
+                            int even_layout, const IbVertices& v, double* node_force, double* node_vel, int* bad,
+                            cudaStream_t s);
 };
 
 const LaunchSet& launch_set_f64();
@@ -47,16 +50,20 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
 
 #define ZL_DEFINE_LAUNCH_SET(NAME, S)                                                                            \
     namespace NAME##_impl {                                                                                      \
-    template <class L, int C, bool O, bool B, bool M>                                                            \
+    template <class L, int C, bool O, bool B, bool M, bool F = false>                                            \
     cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {                      \
         dim3 g, b;                                                                                               \
         step_shape(geo, L::kDims, g, b);                                                                         \
-        aa_step_kernel<L, S, C, O, B, M><<<g, b, 0, s>>>(f, geo, p);                                             \
+        aa_step_kernel<L, S, C, O, B, M, F><<<g, b, 0, s>>>(f, geo, p);                                          \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     template <class L, int C>                                                                                    \
     cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,        \
                         cudaStream_t s) {                                                                        \
+        if (p.forced) {                                                                                          \
+            return odd ? step_one<L, C, true, true, true, true>(f, geo, p, s)                                    \
+                       : step_one<L, C, false, true, true, true>(f, geo, p, s);                                  \
+        }                                                                                                        \
         if (masked) {                                                                                            \
             return odd ? step_one<L, C, true, true, true>(f, geo, p, s)                                          \
                        : step_one<L, C, false, true, true>(f, geo, p, s);                                        \
@@ -169,13 +176,27 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
                                                         cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);   \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
+    cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const LevelMap& m,                   \
+                             const StepParams& p, int even, const IbVertices& v, double* node_force,             \
+                             double* node_vel, int* bad, cudaStream_t s) {                                       \
+        if (v.n <= 0) return cudaSuccess;                                                                        \
+        const int k = dims == 3 ? 64 : 16;                                                                       \
+        const unsigned blocks = (unsigned)(((long long)v.n * k + 127) / 128);                                    \
+        if (dims == 2)                                                                                           \
+            ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, m, p, even, v, node_force,         \
+                                                            node_vel, bad);                                      \
+        else                                                                                                     \
+            ib_touch_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)f, geo, m, p, even, v, node_force,        \
+                                                             node_vel, bad);                                     \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
     }                                                                                                            \
     const LaunchSet& NAME() {                                                                                    \
         static const LaunchSet set = {(int)sizeof(S), NAME##_impl::step_any, NAME##_impl::neq_any,                \
                                       NAME##_impl::face_any,                                                     \
                                       NAME##_impl::scatter_any, NAME##_impl::gather_any,                         \
                                       NAME##_impl::conservation_any, NAME##_impl::c2f_any,                       \
-                                      NAME##_impl::f2c_any};                                                     \
+                                      NAME##_impl::f2c_any, NAME##_impl::ib_touch_any};                          \
         return set;                                                                                              \
     }
 

@@ -120,9 +120,22 @@ __global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, 
     T fi[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) fi[q] = St::load(f + post_stream_slot<L>(geo, ci, q, even_layout), p);
+    // inner node macros through func_macro_ (with the node's forces when the solver has forces)
+    double F[3] = {0., 0., 0.};
+    if (p.forced) {
+        const long long inner = (long long)(ci.x[0] + geo.g[0]) +
+                                (long long)geo.a[0] * ((ci.x[1] + geo.g[1]) + (long long)geo.a[1] * (ci.x[2] + geo.g[2]));
+        for (int a = 0; a < 3; ++a) F[a] = p.const_force[a] + (p.force ? p.force[inner * 3 + a] : 0.);
+    }
     if constexpr (St::kDeviation) {
         float rho, ux, uy, uz, deq[Q];
         macro_dev<L>(fi, rho, ux, uy, uz);
+        if (p.forced) {
+            const float h = 0.5f * (float)p.dt / rho;
+            ux += h * (float)F[0];
+            uy += h * (float)F[1];
+            uz += h * (float)F[2];
+        }
         feq_dev<L>(rho, ux, uy, uz, deq);
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
@@ -131,7 +144,33 @@ __global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, 
         }
     } else {
         double rho, ux, uy, uz, feq[Q];
-        macro_exact<L>(fi, rho, ux, uy, uz);
+        if (p.forced) {
+            using Tb = Tables<L>;
+            rho = fi[0];
+            ux = 0.;
+            uy = 0.;
+            uz = 0.;
+#pragma unroll
+            for (int q = 1; q < Q; ++q) {
+                rho = rho + fi[q];
+                if (Tb::cx(q) == 1) ux = ux + fi[q];
+                if (Tb::cx(q) == -1) ux = ux - fi[q];
+                if (Tb::cy(q) == 1) uy = uy + fi[q];
+                if (Tb::cy(q) == -1) uy = uy - fi[q];
+                if (L::kDims == 3) {
+                    if (Tb::cz(q) == 1) uz = uz + fi[q];
+                    if (Tb::cz(q) == -1) uz = uz - fi[q];
+                }
+            }
+            ux = ux + 0.5 * F[0] * p.dt;
+            uy = uy + 0.5 * F[1] * p.dt;
+            if (L::kDims == 3) uz = uz + 0.5 * F[2] * p.dt;
+            ux = ux / rho;
+            uy = uy / rho;
+            if (L::kDims == 3) uz = uz / rho;
+        } else {
+            macro_exact<L>(fi, rho, ux, uy, uz);
+        }
         feq_exact<L>(rho, ux, uy, uz, feq);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
