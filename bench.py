@@ -247,16 +247,20 @@ def run_reference_arm(args):
 
 
 # ---------------------------------------------------------------- GPU arm
-def time_steps(ctx, steps: int):
-    """Device time of `steps` calls of zl_step_level on the context's stream (CUDA events)."""
+def time_steps(ctx, steps: int, graph: bool = False):
+    """Device time of `steps` time steps on the context's stream (CUDA events): zl_step_level
+    per step, or zl_advance replaying the captured two-step graph."""
     import torch
     stream = torch.cuda.ExternalStream(ctx.stream())
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
     ctx.synchronize()
     start.record(stream)
-    for _ in range(steps):
-        ctx.step_level(0)
+    if graph:
+        ctx.advance(steps)
+    else:
+        for _ in range(steps):
+            ctx.step_level(0)
     end.record(stream)
     end.synchronize()
     return start.elapsed_time(end)
@@ -277,14 +281,22 @@ def run_ours(args):
     ctx = zl.Context(solver_config(storage, local))
     ctx.set_level_nodes(0, codes)
     ctx.set_populations(0, codes, f0)
-    for _ in range(args.warmup):
-        ctx.step_level(0)
+    block = ctx.autotune(0) if args.tune else None
+    if args.tune:
+        ctx.set_populations(0, codes, f0)
+    ctx.set_graph(args.graph)
+    # the graph is captured by the first zl_advance of two or more steps, inside the warm-up
+    if args.graph:
+        ctx.advance(args.warmup)
+    else:
+        for _ in range(args.warmup):
+            ctx.step_level(0)
     ctx.synchronize()
 
     barrier(dist)
     torch.cuda.synchronize()
     with ClockSampler(local) as clocks:
-        ms = time_steps(ctx, args.steps)
+        ms = time_steps(ctx, args.steps, args.graph)
     torch.cuda.synchronize()
     barrier(dist)
     ms = max_over_ranks(dist, ms)
@@ -305,14 +317,18 @@ def run_ours(args):
             with zl.Context(solver_config(zl.STORAGE_NAMES[name], local)) as c2:
                 c2.set_level_nodes(0, codes)
                 c2.set_populations(0, codes, f0)
-                for _ in range(args.warmup):
-                    c2.step_level(0)
-                vms = time_steps(c2, args.steps)
+                vblock = c2.autotune(0) if args.tune else None
+                if args.tune:
+                    c2.set_populations(0, codes, f0)
+                c2.set_graph(args.graph)
+                c2.advance(args.warmup)
+                vms = time_steps(c2, args.steps, args.graph)
                 b = nodes * 2 * 19 * STORAGE_BYTES[name]
                 variants[name] = {"mlups": nodes * args.steps / (vms / 1e3) / 1e6,
                                   "ms_per_step": vms / args.steps,
                                   "hbm_gbs": b / (vms / args.steps / 1e3) / 1e9,
-                                  "frac": b / (vms / args.steps / 1e3) / 1e9 / peak}
+                                  "frac": b / (vms / args.steps / 1e3) / 1e9 / peak,
+                                  "block": vblock}
     # end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
@@ -328,8 +344,7 @@ def run_ours(args):
         ctx.synchronize()
         t0 = time.perf_counter()
         ctx._check(lib.zl_set_populations(ctx.handle, 0, cp, ctypes.cast(f_h.data_ptr(), dp), codes.size))
-        for _ in range(args.steps):
-            ctx._check(lib.zl_step_level(ctx.handle, 0))
+        ctx._check(lib.zl_advance(ctx.handle, args.steps))
         ctx._check(lib.zl_get_macros(ctx.handle, 0, cp, ctypes.cast(rho_h.data_ptr(), dp),
                                      ctypes.cast(u_h.data_ptr(), dp), codes.size))
         ctx.synchronize()
@@ -352,8 +367,9 @@ def run_ours(args):
             "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
             "config": {"workload": f"D3Q19 {COLLISION.upper()} Taylor-Green vortex, periodic {CELLS}^3 "
                                    f"(reference stores {CELLS + 1}^3), u0={U0}, tau={TAU}, "
-                                   f"{args.storage} population storage, FP32 collision"
-                                   if args.storage != "f64" else "FP64 collision",
+                                   f"{args.storage} population storage, "
+                                   + ("FP64 collision" if args.storage == "f64" else "FP32 collision"),
+                       "block": block, "cuda_graph": args.graph,
                        "nodes_per_gpu": nodes, "storage": args.storage, "collision": COLLISION.upper(),
                        "l2": f"inputs larger than L2 ({alg_bytes / 2 / 1e9:.2f} GB of populations)",
                        "parallelism": f"{world} independent replica(s)" if world > 1 else "single GPU"},
@@ -386,6 +402,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--tune", type=int, default=1, help="autotune the step kernel's block shape")
+    ap.add_argument("--graph", type=int, default=1, help="replay steps as a captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:

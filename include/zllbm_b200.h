@@ -161,6 +161,15 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level);
    sub-step of a fine level. */
 int zl_advance(zl_ctx* ctx, int steps);
 
+/* Replay zl_advance as a captured CUDA graph of two background steps (every launch of the
+   sub-cycled order, transfers and boundary passes included).  The graph is re-captured after any
+   change of levels, interfaces, vertices or tuning.  Off by default. */
+int zl_set_graph(zl_ctx* ctx, int enabled);
+
+/* Choose the thread-block shape of a level's step kernel by timing candidate shapes (on a saved
+   copy of the populations, which are restored).  chosen[2] (may be NULL) receives {x, y}. */
+int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen);
+
 /* Sum over a level's nodes of rho and rho*u, accumulated in FP64 on the device:
    out[0] = mass, out[1..dims] = momentum.  Non-finite sums return ZL_ENAN. */
 int zl_conservation(zl_ctx* ctx, int level, double* out);

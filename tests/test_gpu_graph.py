@@ -1,0 +1,121 @@
+"""CUDA-graph replay of the sub-cycled step and the block-shape autotuner change no result.
+
+A graph holds two background steps (every level back to the same population layout); odd step
+counts finish with one direct step.  FP64 runs are compared bit for bit with the direct
+(launch-by-launch) path and, where the step count matches, with the reference's own dumps.
+Immersed-boundary runs accumulate node forces with atomics, so they are compared to 1e-12.
+"""
+import numpy as np
+import pytest
+
+from test_gpu_amr import AMR, config, load_amr
+
+
+def run(meta, z, storage, steps, graph=False, tune=False):
+    import zllbm_b200 as zl
+    levels = meta["levels"]
+    with zl.Context(config(meta, storage)) as ctx:
+        for lv in range(levels + 1):
+            ctx.set_level_nodes(lv, z[f"codes{lv}"])
+            ctx.set_populations(lv, z[f"codes{lv}"], z[f"f_before{lv}"])
+        for lv in range(1, levels + 1):
+            excluded = z[f"codes{lv - 1}"][(z[f"flags{lv - 1}"] & 4) != 0]
+            ctx.set_level_interface(lv, z[f"c2f_fine{lv}"], z[f"f2c_coarse{lv - 1}"], excluded)
+        if "ib" in meta:
+            v = z["vertices_before"]
+            ctx.ib_set_vertices(levels, v[:, 0:3], v[:, 3:6], v[:, 6])
+        shapes = [ctx.autotune(lv, trials=2) for lv in range(levels + 1)] if tune else None
+        ctx.set_graph(graph)
+        # two calls: the second replays the graph captured by the first
+        ctx.advance(steps // 2)
+        ctx.advance(steps - steps // 2)
+        pops = [ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)]
+    return pops, shapes
+
+
+def compare(a, b, ib):
+    for x, y in zip(a, b):
+        if ib:
+            np.testing.assert_allclose(x, y, rtol=1e-12, atol=1e-15)
+        else:
+            assert np.array_equal(x, y)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", AMR)
+def test_graph_replay_matches_direct_fp64(name):
+    import zllbm_b200 as zl
+    meta, z = load_amr(name)
+    ib = "ib" in meta
+    for steps in (meta["steps"], 5):
+        direct, _ = run(meta, z, zl.STORAGE_F64, steps)
+        graphed, _ = run(meta, z, zl.STORAGE_F64, steps, graph=True)
+        compare(graphed, direct, ib)
+        if steps == meta["steps"]:
+            compare(graphed, [z[f"f_after{lv}"] for lv in range(meta["levels"] + 1)], ib)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", AMR)
+def test_graph_replay_matches_direct_fp32(name):
+    import zllbm_b200 as zl
+    meta, z = load_amr(name)
+    direct, _ = run(meta, z, zl.STORAGE_F32, 6)
+    graphed, _ = run(meta, z, zl.STORAGE_F32, 6, graph=True)
+    compare(graphed, direct, "ib" in meta)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["amr2d_l2", "amr3d_l1"])
+def test_autotuned_block_shape_keeps_results(name):
+    import zllbm_b200 as zl
+    meta, z = load_amr(name)
+    direct, _ = run(meta, z, zl.STORAGE_F64, meta["steps"])
+    tuned, shapes = run(meta, z, zl.STORAGE_F64, meta["steps"], graph=True, tune=True)
+    compare(tuned, direct, False)
+    for bx, by in shapes:
+        assert bx >= 32 and by >= 1 and bx * by <= 256
+
+
+@pytest.mark.gpu
+def test_autotune_on_periodic_box_keeps_results():
+    """A 3D periodic TGV box (odd extents, so blocks overhang on x and y) tuned then stepped."""
+    import zllbm_b200 as zl
+    from fixtures import load_lbm, solver_config
+    meta, codes, f0, f1 = load_lbm("tgv3d_mrt")
+    results = []
+    for tune in (False, True):
+        with zl.Context(solver_config(meta, zl.STORAGE_F64)) as ctx:
+            ctx.set_level_nodes(0, codes)
+            ctx.set_populations(0, codes, f0)
+            if tune:
+                ctx.autotune(0, trials=2)
+            ctx.set_graph(True)
+            ctx.advance(meta["steps"])
+            results.append(ctx.get_populations(0, codes))
+    assert np.array_equal(results[0], results[1])
+    assert np.array_equal(results[1], f1)
+
+
+@pytest.mark.gpu
+def test_graph_recaptured_after_direct_step():
+    """A direct zl_step_level between zl_advance calls flips the layout; the replayed graph must
+    follow it (and a new node set must drop the old graph)."""
+    import zllbm_b200 as zl
+    from fixtures import load_lbm, solver_config
+    meta, codes, f0, _ = load_lbm("cavity2d_mrt")
+    results = []
+    for graph in (False, True):
+        with zl.Context(solver_config(meta, zl.STORAGE_F64)) as ctx:
+            ctx.set_level_nodes(0, codes)
+            ctx.set_populations(0, codes, f0)
+            ctx.set_graph(graph)
+            ctx.advance(4)
+            ctx.step_level(0)
+            ctx.advance(4)
+            ctx.advance(3)
+            ctx.set_level_nodes(0, codes)
+            ctx.set_populations(0, codes, f0)
+            ctx.advance(6)
+            results.append(ctx.get_populations(0, codes))
+    assert np.array_equal(results[0], results[1])

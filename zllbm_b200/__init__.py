@@ -84,6 +84,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_advance": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_level_interface": ([P, ctypes.c_int, u64p, i64, u64p, i64, u64p, i64], ctypes.c_int),
         "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
         "zl_conservation": ([P, ctypes.c_int, dp], ctypes.c_int),
         "zl_synchronize": ([P], ctypes.c_int),
         "zl_get_stream": ([P, ctypes.POINTER(P)], ctypes.c_int),
@@ -249,6 +251,14 @@ class Context:
 
     def transfer_levels(self, fine_level: int):
         self._check(self.lib.zl_transfer_levels(self.handle, fine_level))
+
+    def set_graph(self, enabled: bool):
+        self._check(self.lib.zl_set_graph(self.handle, 1 if enabled else 0))
+
+    def autotune(self, level: int = 0, trials: int = 8):
+        out = (ctypes.c_int32 * 2)()
+        self._check(self.lib.zl_autotune(self.handle, level, trials, out))
+        return tuple(out)
 
     def step_level(self, level: int = 0):
         self._check(self.lib.zl_step_level(self.handle, level))

@@ -34,6 +34,10 @@ constexpr uint32_t kInfoPresent = 1u << 31;
 constexpr uint32_t kInfoSaveMacro = 1u << 30;  // keep rho, u of the last collision (coarse/fine transfer source)
 constexpr int kInfoFaceShift = 24;  // 6 bits: on face xmin..zmax (reference boundary node sets)
 
+// extended-physics bits of the step kernel's Ext template argument
+constexpr int kExtForce = 1;
+constexpr int kExtLes = 2;
+
 struct LevelGeom {
     int n[3];          // nodes per axis (periodic axes hold each plane once)
     int g[3];          // ghost frame width per axis (0 on periodic axes, 1 otherwise)
@@ -41,6 +45,7 @@ struct LevelGeom {
     int periodic[3];   // wrap-around per axis
     long long stride;  // elements between population planes (>= a0 a1 a2)
     int face_on_box;   // bit f: box edge f lies on domain face f (non-periodic faces only)
+    int block[2];      // thread-block shape of the step kernel (x, y); {0, 0}: default
     const uint32_t* info;  // per-cell info (masked levels), nullptr for full boxes
 };
 
@@ -232,7 +237,7 @@ __device__ __forceinline__ double mrt_element_exact(int q, int s, double relax, 
     return acc;
 }
 
-template <class L>
+template <class L, bool Les>
 __device__ __forceinline__ void collide_exact(const double* f, double* out, const StepParams& p, int coll,
                                               double* mac, const NodeForce* nf) {
     using Tb = Tables<L>;
@@ -288,7 +293,7 @@ __device__ __forceinline__ void collide_exact(const double* f, double* out, cons
         }
     }
     double tau = p.tau;
-    if (p.les) tau = p.tau + smag_tau_sgs_exact<L>(f, feq, p.tau, p.les_c, nf != nullptr, nf ? nf->F : nullptr,
+    if (Les) tau = p.tau + smag_tau_sgs_exact<L>(f, feq, p.tau, p.les_c, nf != nullptr, nf ? nf->F : nullptr,
                                                    p.dt, ux, uy, uz);
     if (coll == kSrt) {
 #pragma unroll
@@ -302,7 +307,7 @@ __device__ __forceinline__ void collide_exact(const double* f, double* out, cons
         double d[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) d[q] = f[q] - feq[q];
-        if (!p.les) {
+        if (!Les) {
             const double* A = p.mrt64;
             const double* B = p.mrt64_d;
 #pragma unroll 1
@@ -516,7 +521,7 @@ __device__ __forceinline__ void moment_apply(const float* x, const float* coef, 
     }
 }
 
-template <class L>
+template <class L, bool Les>
 __device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll, float* mac,
                                             const NodeForce* nf) {
     using Tb = Tables<L>;
@@ -531,7 +536,7 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
     const float dt = (float)p.dt;
     feq_neq_dev<L>(d, neq, p.scale, p.inv_scale, mac, nf ? F : nullptr, dt);
     float omega = p.omega32;
-    if (p.les) {
+    if (Les) {
         // non-equilibrium stress (unscaled) and Smagorinsky tau = tau0 + tau_sgs
         float pxx = 0.f, pyy = 0.f, pzz = 0.f, pxy = 0.f, pxz = 0.f, pyz = 0.f;
 #pragma unroll
@@ -584,7 +589,7 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
     float lam[Q];
 #pragma unroll
     for (int k = 0; k < Q; ++k) {
-        if (p.les) lam[k] = Tb::s(k) > 0. ? ((float)Tb::s(k) - omega) / (float)row_norm2<L>(k) : 0.f;
+        if (Les) lam[k] = Tb::s(k) > 0. ? ((float)Tb::s(k) - omega) / (float)row_norm2<L>(k) : 0.f;
         else lam[k] = p.mrt_coef[k];
     }
     if constexpr (L::kQ == 19) {
@@ -676,17 +681,20 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
 // ---------------------------------------------------------------- the step kernel
 // One thread per node of the level box.  Odd selects the layout read (see file comment).
 // Bnd: the level has at least one non-periodic axis.  Masked: the box holds absent cells.
-template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, bool Forced = false>
+// Ext: extended physics compiled in, kExtForce (Guo forcing) and / or kExtLes (Smagorinsky).
+template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext = 0>
 __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    constexpr bool Forced = (Ext & kExtForce) != 0;
+    constexpr bool Les = (Ext & kExtLes) != 0;
     using Tb = Tables<L>;
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
     Coord c;
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
-    c.x[1] = blockIdx.y;
+    c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
     c.x[2] = blockIdx.z;
-    if (c.x[0] >= geo.n[0]) return;
+    if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
 
     // box coordinates of x-1, x, x+1 along each axis; cell indices fit in 32 bits (checked at set-up)
     int bx[3], row[3][3];
@@ -733,9 +741,9 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
         for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
     }
     if constexpr (St::kDeviation) {
-        collide_dev<L>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
+        collide_dev<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     } else {
-        collide_exact<L>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
+        collide_exact<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     }
     if (Masked && (info & kInfoSaveMacro)) {
         double* m = p.macro + (long long)self * 4;

@@ -69,6 +69,12 @@ struct zl_ctx {
     Level levels[ZL_MAX_LEVELS];
     std::string last_error;
     DeviceBuffer scratch_flag;  // int error flag for kernels that validate codes
+    // CUDA graph of two background steps (zl_set_graph)
+    bool use_graph = false;
+    cudaGraphExec_t graph_exec = nullptr;
+    long long graph_generation = -1;
+    long long generation = 0;   // bumped by every change of levels, interfaces or vertices
+    int graph_layouts = 0;      // bit l: level l's layout when the graph was captured
 };
 
 namespace {
@@ -237,6 +243,7 @@ int zl_destroy(zl_ctx* ctx) {
         l.partial.release();
     }
     ctx->scratch_flag.release();
+    if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return ZL_OK;
@@ -250,6 +257,7 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     const int dims = ctx->dims, q = ctx->q;
     Level& L = ctx->levels[level];
     L.active = false;
+    ++ctx->generation;
 
     DeviceBuffer dcodes, dminmax;
     if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
@@ -336,7 +344,8 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     if ((rc = read_flag(ctx, &bad))) return rc;
     if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
     const long long box_nodes = (long long)geo.n[0] * geo.n[1] * geo.n[2];
-    if ((long long)present == box_nodes && ctx->cfg.max_level == 0 && !ctx->cfg.forcing) {
+    // forcing and LES run the extended step variant, which reads the per-cell info array
+    if ((long long)present == box_nodes && ctx->cfg.max_level == 0 && !ctx->cfg.forcing && !ctx->cfg.les) {
         L.info.release();
     } else {
         geo.info = (const uint32_t*)L.info.ptr;
@@ -552,13 +561,7 @@ static void time_stepping_order(int level, int max_level, std::vector<int>* orde
     }
 }
 
-int zl_advance(zl_ctx* ctx, int steps) {
-    if (!ctx || steps < 0) return ZL_EINVAL;
-    std::vector<int> order;
-    time_stepping_order(0, ctx->cfg.max_level, &order);
-    for (int l = 1; l <= ctx->cfg.max_level; ++l)
-        if (!ctx->levels[l].has_transfer)
-            return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface before zl_advance", l);
+static int advance_direct(zl_ctx* ctx, int steps, const std::vector<int>& order) {
     for (int s = 0; s < steps; ++s) {
         int count[ZL_MAX_LEVELS] = {0};
         for (int l : order) {
@@ -571,6 +574,110 @@ int zl_advance(zl_ctx* ctx, int steps) {
                 if (rc) return rc;
             }
         }
+    }
+    return ZL_OK;
+}
+
+int zl_advance(zl_ctx* ctx, int steps) {
+    if (!ctx || steps < 0) return ZL_EINVAL;
+    std::vector<int> order;
+    time_stepping_order(0, ctx->cfg.max_level, &order);
+    for (int l = 1; l <= ctx->cfg.max_level; ++l)
+        if (!ctx->levels[l].has_transfer)
+            return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface before zl_advance", l);
+    if (!ctx->use_graph || steps < 2) return advance_direct(ctx, steps, order);
+    // Two background steps bring every level back to the same population layout, so one captured
+    // graph of two steps replays for any number of pairs.
+    // the captured launches bake in every level's current population layout
+    int layouts = 0;
+    for (int l = 0; l <= ctx->cfg.max_level; ++l) layouts |= ctx->levels[l].even_layout << l;
+    if (!ctx->graph_exec || ctx->graph_generation != ctx->generation || ctx->graph_layouts != layouts) {
+        if (ctx->graph_exec) {
+            cudaGraphExecDestroy(ctx->graph_exec);
+            ctx->graph_exec = nullptr;
+        }
+        cudaGraph_t graph = nullptr;
+        long long steps_before[ZL_MAX_LEVELS];
+        for (int l = 0; l < ZL_MAX_LEVELS; ++l) steps_before[l] = ctx->levels[l].steps;
+        ZL_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = advance_direct(ctx, 2, order);
+        const cudaError_t e = cudaStreamEndCapture(ctx->stream, &graph);
+        for (int l = 0; l < ZL_MAX_LEVELS; ++l) ctx->levels[l].steps = steps_before[l];
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        ZL_CUDA(ctx, e);
+        // capture recorded the launches without running them: the host-side layouts went through
+        // two full steps and are back where they started
+        const cudaError_t ie = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+        cudaGraphDestroy(graph);
+        ZL_CUDA(ctx, ie);
+        ctx->graph_generation = ctx->generation;
+        ctx->graph_layouts = layouts;
+    }
+    for (int s = 0; s + 1 < steps; s += 2) {
+        ZL_CUDA(ctx, cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+        for (int l : order) ctx->levels[l].steps += 2;
+    }
+    if (steps % 2) return advance_direct(ctx, 1, order);
+    return ZL_OK;
+}
+
+int zl_set_graph(zl_ctx* ctx, int enabled) {
+    if (!ctx) return ZL_EINVAL;
+    ctx->use_graph = enabled != 0;
+    return ZL_OK;
+}
+
+int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (trials < 1) trials = 8;
+    Level& L = ctx->levels[level];
+    // time the step kernel (both layouts) for candidate block shapes on a copy of the populations
+    DeviceBuffer saved;
+    if ((rc = alloc(ctx, saved, L.f.bytes))) return rc;
+    ZL_CUDA(ctx, cudaMemcpyAsync(saved.ptr, L.f.ptr, L.f.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    const int shapes[][2] = {{256, 1}, {128, 2}, {128, 1}, {64, 4}, {64, 2}, {32, 8}, {32, 4}};
+    cudaEvent_t t0, t1;
+    ZL_CUDA(ctx, cudaEventCreate(&t0));
+    ZL_CUDA(ctx, cudaEventCreate(&t1));
+    float best = 1e30f;
+    int best_i = 0;
+    const int nshapes = (int)(sizeof(shapes) / sizeof(shapes[0]));
+    for (int i = 0; i < nshapes; ++i) {
+        LevelGeom g = L.geo;
+        g.block[0] = shapes[i][0];
+        g.block[1] = shapes[i][1];
+        if (g.block[0] > 2 * std::max(32, g.n[0])) continue;
+        const bool odd0 = L.even_layout == 1;
+        for (int warm = 0; warm < 2; ++warm)
+            ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd0 != (warm & 1), L.bnd,
+                                        L.geo.info != nullptr, L.f.ptr, g, L.params, ctx->stream));
+        ZL_CUDA(ctx, cudaEventRecord(t0, ctx->stream));
+        for (int k = 0; k < 2 * trials; ++k)
+            ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd0 != (k & 1), L.bnd,
+                                        L.geo.info != nullptr, L.f.ptr, g, L.params, ctx->stream));
+        ZL_CUDA(ctx, cudaEventRecord(t1, ctx->stream));
+        ZL_CUDA(ctx, cudaEventSynchronize(t1));
+        float ms = 0.f;
+        ZL_CUDA(ctx, cudaEventElapsedTime(&ms, t0, t1));
+        if (ms < best) {
+            best = ms;
+            best_i = i;
+        }
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    ZL_CUDA(ctx, cudaMemcpyAsync(L.f.ptr, saved.ptr, L.f.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    L.geo.block[0] = shapes[best_i][0];
+    L.geo.block[1] = shapes[best_i][1];
+    ++ctx->generation;
+    if (chosen) {
+        chosen[0] = L.geo.block[0];
+        chosen[1] = L.geo.block[1];
     }
     return ZL_OK;
 }
@@ -739,6 +846,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
     }
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     F.has_transfer = true;
+    ++ctx->generation;
     return ZL_OK;
 }
 
@@ -811,6 +919,7 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         ZL_CUDA(ctx, cudaMemset(L.ib_force.ptr, 0, (size_t)n * 3 * 8));
     }
     L.n_vertices = (int)n;
+    ++ctx->generation;
     // every stencil node must exist on the level (the reference logs an error otherwise)
     if (n > 0) {
         IbVertices v = ib_view(ctx, L, level);

@@ -40,29 +40,41 @@ const LaunchSet& launch_set_f32();
 const LaunchSet& launch_set_f16();
 const LaunchSet& launch_set_bf16();
 
-// Block size and grid of the fused step: one thread per node, x fastest.
+// Block shape and grid of the fused step: one thread per node, x fastest.  The shape is the
+// level's autotuned choice (zl_autotune) or a default of up to 256 threads along x.
 inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) {
-    int bx = 256;
-    while (bx > 32 && bx / 2 >= geo.n[0]) bx /= 2;
-    block = dim3(bx, 1, 1);
-    grid = dim3((geo.n[0] + bx - 1) / bx, geo.n[1], dims == 3 ? geo.n[2] : 1);
+    int bx = geo.block[0], by = geo.block[1];
+    if (bx <= 0 || by <= 0) {
+        bx = 256;
+        while (bx > 32 && bx / 2 >= geo.n[0]) bx /= 2;
+        by = 1;
+    }
+    block = dim3(bx, by, 1);
+    grid = dim3((geo.n[0] + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? geo.n[2] : 1);
 }
 
 #define ZL_DEFINE_LAUNCH_SET(NAME, S)                                                                            \
     namespace NAME##_impl {                                                                                      \
-    template <class L, int C, bool O, bool B, bool M, bool F = false>                                            \
+    template <class L, int C, bool O, bool B, bool M, int X = 0>                                                 \
     cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {                      \
         dim3 g, b;                                                                                               \
         step_shape(geo, L::kDims, g, b);                                                                         \
-        aa_step_kernel<L, S, C, O, B, M, F><<<g, b, 0, s>>>(f, geo, p);                                          \
+        aa_step_kernel<L, S, C, O, B, M, X><<<g, b, 0, s>>>(f, geo, p);                                          \
         return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    template <class L, int C, int X>                                                                             \
+    cudaError_t step_ext(bool odd, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {            \
+        return odd ? step_one<L, C, true, true, true, X>(f, geo, p, s)                                           \
+                   : step_one<L, C, false, true, true, X>(f, geo, p, s);                                         \
     }                                                                                                            \
     template <class L, int C>                                                                                    \
     cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,        \
                         cudaStream_t s) {                                                                        \
-        if (p.forced) {                                                                                          \
-            return odd ? step_one<L, C, true, true, true, true>(f, geo, p, s)                                    \
-                       : step_one<L, C, false, true, true, true>(f, geo, p, s);                                  \
+        if (p.forced || p.les) {                                                                                 \
+            if (!masked) return cudaErrorInvalidValue;                                                           \
+            if (p.forced && p.les) return step_ext<L, C, kExtForce | kExtLes>(odd, f, geo, p, s);                \
+            if (p.forced) return step_ext<L, C, kExtForce>(odd, f, geo, p, s);                                   \
+            return step_ext<L, C, kExtLes>(odd, f, geo, p, s);                                                   \
         }                                                                                                        \
         if (masked) {                                                                                            \
             return odd ? step_one<L, C, true, true, true>(f, geo, p, s)                                          \

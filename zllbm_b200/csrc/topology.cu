@@ -50,9 +50,9 @@ __global__ void node_info_kernel(LevelGeom geo, uint32_t* __restrict__ info) {
     using Tb = Tables<L>;
     Coord c;
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
-    c.x[1] = blockIdx.y;
+    c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
     c.x[2] = blockIdx.z;
-    if (c.x[0] >= geo.n[0]) return;
+    if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
     auto cell_of = [&](const int* x) -> long long {
         int b[3];
         for (int a = 0; a < 3; ++a) b[a] = wrap_or_ghost(x[a], geo.n[a], geo.g[a], geo.periodic[a]);
