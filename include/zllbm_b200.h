@@ -97,8 +97,10 @@ typedef struct zl_config {
     int forcing;               /* 1: collide with Guo forcing and per-node forces (SetNumForces /
                                   SetConstantForce, lbm_interface.h:298-319); needed by immersed boundaries */
     double constant_force[3];  /* SetConstantForce */
-    int les;                   /* 1: Smagorinsky LES with tau = tau0 + tau_sgs (the reference sets tau = tau_sgs,
-                                  lbm_solver_interface.cpp:291-295, which this library treats as a bug) */
+    int les;                   /* ZL_LES_SMAGORINSKY: tau = tau0 + tau_sgs (the reference sets tau = tau_sgs,
+                                  lbm_solver_interface.cpp:291-295, which this library treats as a bug);
+                                  ZL_LES_LEARNED: the same increment with a per-node constant from the
+                                  closure network (zl_set_closure), Smagorinsky when none is set */
     double les_cs;             /* Smagorinsky constant (0 selects the reference's 0.16, lbm_les_models.h:49) */
     double dx;                 /* background grid spacing (SetDomainGridSize); 0 selects 1 */
     int device;                /* CUDA device ordinal */
@@ -243,6 +245,84 @@ int zl_abi_version(void);
    ordering) race on it.  The call is asynchronous on `stream`; read out_device after
    synchronizing. */
 int zl_moments_noalloc(int lattice, const double* f_device, int64_t n, double* out_device, void* stream);
+
+/* ---------------------------------------------------------------- full-box levels, device I/O
+   No counterpart in the reference, whose levels are always hash maps of nodes; these let a
+   periodic box of 10^9 nodes be set up and read without host node lists. */
+
+/* Make `level` the full box of n[0] x n[1] x n[2] nodes starting at level index lo (like
+   zl_set_level_nodes given every code of the box).  On a periodic axis a box spanning the whole
+   domain (n = (domain_max - domain_min) << level) wraps around and stores each plane once. */
+int zl_set_level_box(zl_ctx* ctx, int level, const int32_t lo[3], const int32_t n[3]);
+
+/* Set every node of a full-box level to feq(rho, u), from device arrays in box order (x fastest):
+   rho_device[n], u_device[n * 3] (FP32). */
+int zl_set_equilibrium_dense(zl_ctx* ctx, int level, const float* rho_device, const float* u_device);
+
+/* Density and velocity of every node of a full-box level into device arrays (box order, FP32). */
+int zl_get_macros_dense(zl_ctx* ctx, int level, float* rho_device, float* u_device);
+
+/* ---------------------------------------------------------------- learned LES closure
+   No counterpart in the reference (it hard-wires Smagorinsky, lbm_les_smagorinsky.cpp:22-94).
+   A per-node network y = MLP(x) with x the 24 node features (the 19 non-equilibrium MRT moments
+   / rho, tr S, S:S, tr(Sd^3), |Sd| and the Cs = 0.1 Smagorinsky increment, S = -3 Pi / (2 rho tau0))
+   gives the Smagorinsky constant C = 18 c with c = 0.01 * clamp(y, 0, 8):
+       tau = tau0 + 0.5 * (sqrt(tau0^2 + C sqrt(2 Pi:Pi)) - tau0).
+   Network: 24 -> 64 -> 64 -> 1, tanh-form GELU, BF16 tensor-core operands, FP32 accumulation. */
+#define ZL_LES_OFF 0
+#define ZL_LES_SMAGORINSKY 1
+#define ZL_LES_LEARNED 2
+#define ZL_MLP_IN 24
+#define ZL_MLP_HIDDEN 64
+#define ZL_MLP_TRAINABLE 5825 /* w1 .. b3 */
+
+typedef struct zl_mlp {
+    float w1[ZL_MLP_HIDDEN * ZL_MLP_IN];     /* w1[j * 24 + f] */
+    float b1[ZL_MLP_HIDDEN];
+    float w2[ZL_MLP_HIDDEN * ZL_MLP_HIDDEN]; /* w2[j * 64 + i] */
+    float b2[ZL_MLP_HIDDEN];
+    float w3[ZL_MLP_HIDDEN];
+    float b3;
+    float in_mean[ZL_MLP_IN];                /* input normalisation x_hat = (x - mean) * inv_std */
+    float in_inv_std[ZL_MLP_IN];
+} zl_mlp;
+
+/* Network used by levels with les == ZL_LES_LEARNED (copied; NULL returns to Smagorinsky). */
+int zl_set_closure(zl_ctx* ctx, const zl_mlp* net);
+
+/* Run the network on every `every`-th step of a level only (default 1: every step); the steps in
+   between relax with each node's c from the last evaluation.  Amortises the network's cost. */
+int zl_set_closure_interval(zl_ctx* ctx, int every);
+
+/* The 24 closure features of every node of a full-box level (device array, box order, n * 24). */
+int zl_closure_features(zl_ctx* ctx, int level, float* x_device);
+
+/* Box filter of a full-box level over factor^3 blocks of nodes: per block (box order of the
+   blocks) 29 FP32 values: rho, u (3), <u_a u_b> (xx yy zz xy xz yz), <f - feq> (19). */
+int zl_filter_level(zl_ctx* ctx, int level, int factor, float* out_device);
+
+/* Training pairs on the filtered (coarse) periodic grid of nc[0] x nc[1] x nc[2] blocks:
+   target y = c / 0.01 of the least-squares Smagorinsky constant of the exact subgrid stress over
+   each 3^3 neighbourhood (clipped to [0, 8]); features of a coarse node holding
+   feq(<rho>, <u>) + r <f - feq>, r = factor * tau_eff / tau_fine, tau_eff = tau_coarse + 3 c |S|.
+   x_device: n * 24, y_device: n; scratch_device: n * 3 floats. */
+int zl_closure_pairs(const int32_t nc[3], const float* filtered_device, double tau_fine, double tau_coarse,
+                     int factor, float* x_device, float* y_device, float* scratch_device, void* stream);
+
+/* Network outputs y for n feature rows (device arrays; tensor-core forward of the closure). */
+int zl_mlp_forward(const zl_mlp* net, const float* x_device, int64_t n, float* y_device, void* stream);
+
+/* Trainer: FP32 master weights and Adam moments on the device; each step runs the fused
+   forward + backward tensor-core kernel over n samples (mean-square error on y) and one Adam
+   update (beta1 0.9, beta2 0.999, eps 1e-8). */
+typedef struct zl_trainer zl_trainer;
+int zl_trainer_create(const zl_mlp* init, int device, zl_trainer** out);
+int zl_trainer_set_stream(zl_trainer* tr, void* stream); /* cudaStream_t to issue on (NULL: own stream) */
+int zl_trainer_step(zl_trainer* tr, const float* x_device, const float* y_device, int64_t n, float lr);
+int zl_trainer_loss(zl_trainer* tr, double* loss);       /* mean-square error of the last step */
+int zl_trainer_gradients(zl_trainer* tr, zl_mlp* grad); /* gradients of the last step (w1 .. b3) */
+int zl_trainer_weights(zl_trainer* tr, zl_mlp* out);
+void zl_trainer_destroy(zl_trainer* tr);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,271 @@
+"""GPU parity of the learned LES closure against the CPU oracle (oracle/closure.py).
+
+Tolerances: the device and the oracle round the same operands to BF16 (x_hat, W1, A1, W2, dZ2,
+dZ1) and accumulate in FP32 (device) / FP64 (oracle); tanhf against numpy's tanh can flip a BF16
+rounding of A1 now and then, which moves y by ~1e-4.  Hence y within 2e-3, gradients within 1e-2
+relative per tensor (cosine > 0.9999), and populations after a learned step within 1e-7 (FP32 storage) / 4e-6 (FP16, two half-ulps of
+the scaled deviations).
+"""
+import numpy as np
+import pytest
+
+from oracle import closure as C
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def _net(seed, x=None):
+    mean = inv = None
+    if x is not None:
+        mean = x.mean(axis=0)
+        sd = x.std(axis=0)
+        inv = np.where(sd > 0, 1.0 / np.where(sd > 0, sd, 1.0), 1.0)
+    return C.Mlp.random(seed, mean, inv)
+
+
+def _zl_net(net):
+    import zllbm_b200 as zl
+    return zl.ZlMlp.from_flat(net.flat())
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 1000, 128 * 149 + 5])
+def test_mlp_forward_matches_oracle(n):
+    import zllbm_b200 as zl
+    torch = _torch()
+    rng = np.random.default_rng(n)
+    x = (rng.normal(size=(n, 24)) * rng.uniform(0.1, 3.0, 24) + rng.normal(size=24)).astype(np.float32)
+    net = _net(11, x)
+    y_ref, _ = net.forward(x)
+    xd = torch.from_numpy(x).cuda()
+    yd = torch.empty(n, dtype=torch.float32, device="cuda")
+    zl.mlp_forward(_zl_net(net), xd.data_ptr(), n, yd.data_ptr())
+    y = yd.cpu().numpy()
+    err = np.abs(y - y_ref)
+    assert err.max() < 2e-3 * max(1.0, np.abs(y_ref).max()), err.max()
+    assert np.median(err) < 2e-5
+
+
+def _train_data(n, seed):
+    rng = np.random.default_rng(seed)
+    x = rng.normal(size=(n, 24)).astype(np.float32)
+    t = (1.0 + 0.5 * np.tanh(x[:, 0]) - 0.3 * x[:, 1] * x[:, 2] / (1 + x[:, 2] ** 2)).astype(np.float32)
+    return x, t
+
+
+@pytest.mark.parametrize("n", [100, 128 * 148 * 2 + 77])
+def test_trainer_gradients_match_oracle(n):
+    import zllbm_b200 as zl
+    torch = _torch()
+    x, t = _train_data(n, 3)
+    net = _net(12, x)
+    loss_ref, g_ref = net.gradients(x, t)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    with zl.Trainer(_zl_net(net)) as tr:
+        tr.step(xd.data_ptr(), td.data_ptr(), n, 0.0)
+        g = C.Mlp.from_flat(tr.gradients().flat())
+        loss = tr.loss()
+        w = C.Mlp.from_flat(tr.weights().flat())
+    assert loss == pytest.approx(loss_ref, rel=2e-3)
+    for name in ("w1", "b1", "w2", "b2", "w3"):
+        a = np.asarray(getattr(g, name), np.float64).ravel()
+        b = np.asarray(g_ref[name], np.float64).ravel()
+        rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+        cos = a @ b / (np.linalg.norm(a) * np.linalg.norm(b))
+        assert rel < 1e-2 and cos > 0.9999, (name, rel, cos)
+    assert float(g.b3) == pytest.approx(float(g_ref["b3"]), rel=1e-3, abs=1e-7)
+    # lr = 0 leaves the weights as they were
+    np.testing.assert_array_equal(w.w2, net.w2)
+
+
+def test_trainer_adam_follows_oracle_and_learns():
+    import zllbm_b200 as zl
+    torch = _torch()
+    n = 128 * 148
+    x, t = _train_data(n, 4)
+    net = _net(13, x)
+    ref = C.Mlp.from_flat(net.flat())
+    opt = C.Adam(ref)
+    xd, td = torch.from_numpy(x).cuda(), torch.from_numpy(t).cuda()
+    with zl.Trainer(_zl_net(net)) as tr:
+        for _ in range(3):
+            _, g = ref.gradients(x, t)
+            opt.step(g, 1e-3)
+            tr.step(xd.data_ptr(), td.data_ptr(), n, 1e-3)
+        w = C.Mlp.from_flat(tr.weights().flat())
+        for name in ("w1", "w2", "w3"):
+            # Adam normalises each gradient, so a near-zero gradient whose sign differs between
+            # device and oracle moves that weight by up to 2 lr per step: compare the bulk
+            d = np.abs(np.asarray(getattr(w, name)) - np.asarray(getattr(ref, name)))
+            assert np.mean(d < 2e-5) > 0.99 and d.max() <= 6.1e-3, (name, np.mean(d < 2e-5), d.max())
+        first = None
+        for it in range(300):
+            tr.step(xd.data_ptr(), td.data_ptr(), n, 3e-3)
+            if it == 0:
+                first = tr.loss()
+        last = tr.loss()
+    assert last < 0.2 * first, (first, last)
+
+
+def _box_ctx(storage, n, tau=0.51, les=0, cs=0.0, coll=None):
+    import zllbm_b200 as zl
+    cfg = zl.SolverConfig(lattice=zl.D3Q19, collision=zl.SRT if coll is None else coll, storage=storage,
+                          viscosity=(tau - 0.5) / 3.0, bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(0, 0, 0),
+                          domain_max=(n, n, n), les=les, les_cs=cs)
+    ctx = zl.Context(cfg)
+    ctx.set_level_box(0, (0, 0, 0), (n, n, n))
+    return ctx
+
+
+def _random_field(n, seed, amp=0.04):
+    """A smooth periodic random velocity field (a few Fourier modes), rho = 1."""
+    rng = np.random.default_rng(seed)
+    g = np.arange(n) * 2 * np.pi / n
+    z, y, x = np.meshgrid(g, g, g, indexing="ij")
+    u = np.zeros((n, n, n, 3))
+    for _ in range(6):
+        k = rng.integers(1, 4, 3)
+        ph = rng.uniform(0, 2 * np.pi, 3)
+        a = rng.normal(size=3)
+        arg = k[0] * x + k[1] * y + k[2] * z
+        for c in range(3):
+            u[..., c] += a[c] * np.sin(arg + ph[c])
+    u *= amp / np.abs(u).max()
+    rho = np.ones((n, n, n))
+    return rho.reshape(-1).astype(np.float32), u.reshape(-1, 3).astype(np.float32)
+
+
+def _codes(n):
+    import zllbm_b200 as zl
+    return zl.box_codes(3, (0, 0, 0), (n - 1, n - 1, n - 1))
+
+
+def test_dense_equilibrium_roundtrip_and_codes_agree():
+    import zllbm_b200 as zl
+    torch = _torch()
+    n = 16
+    rho, u = _random_field(n, 1)
+    with _box_ctx(zl.STORAGE_F32, n) as ctx:
+        rd, ud = torch.from_numpy(rho).cuda(), torch.from_numpy(u).cuda()
+        ctx.set_equilibrium_dense(0, rd.data_ptr(), ud.data_ptr())
+        r2, u2 = torch.empty_like(rd), torch.empty_like(ud)
+        ctx.get_macros_dense(0, r2.data_ptr(), u2.data_ptr())
+        ctx.synchronize()
+        np.testing.assert_allclose(r2.cpu().numpy(), rho, rtol=0, atol=2e-7)
+        np.testing.assert_allclose(u2.cpu().numpy(), u, rtol=0, atol=2e-7)
+        f = ctx.get_populations(0, _codes(n))
+    np.testing.assert_allclose(f, C.feq19(rho.astype(np.float64), u.astype(np.float64)), rtol=0, atol=1e-7)
+
+
+def _run_box(ctx, n, seed, steps):
+    torch = _torch()
+    rho, u = _random_field(n, seed)
+    rd, ud = torch.from_numpy(rho).cuda(), torch.from_numpy(u).cuda()
+    ctx.set_equilibrium_dense(0, rd.data_ptr(), ud.data_ptr())
+    for _ in range(steps):
+        ctx.step_level(0)
+    ctx.synchronize()
+
+
+def test_closure_features_match_oracle():
+    import zllbm_b200 as zl
+    torch = _torch()
+    n = 16
+    with _box_ctx(zl.STORAGE_F32, n, tau=0.55) as ctx:
+        _run_box(ctx, n, 2, 5)
+        xd = torch.empty((n ** 3, 24), dtype=torch.float32, device="cuda")
+        ctx.closure_features(0, xd.data_ptr())
+        ctx.synchronize()
+        f = ctx.get_populations(0, _codes(n))
+    x_ref = C.node_features(f, 0.55)
+    x = xd.cpu().numpy()
+    # the conserved moments (mass, momentum) of neq are rounding noise on both sides
+    scale = np.maximum(np.abs(x_ref).max(axis=0), 1e-3 * np.abs(x_ref[:, 1:19]).max())
+    assert (np.abs(x - x_ref) / scale).max() < 2e-3
+
+
+@pytest.mark.parametrize("coll", [0, 1])
+def test_learned_step_with_constant_output_is_smagorinsky(coll):
+    """w = 0, b3 = 1 gives y = 1, c = 0.01: the learned step is Smagorinsky with Cs = 0.1."""
+    import zllbm_b200 as zl
+    n = 16
+    net = _net(14)
+    net.w1[:] = 0
+    net.w2[:] = 0
+    net.w3[:] = 0
+    net.b3 = np.float32(1.0)
+    out = []
+    for les in (zl.LES_SMAGORINSKY, zl.LES_LEARNED):
+        with _box_ctx(zl.STORAGE_F32, n, tau=0.505, les=les, cs=0.1, coll=coll) as ctx:
+            if les == zl.LES_LEARNED:
+                ctx.set_closure(_zl_net(net))
+            _run_box(ctx, n, 3, 6)
+            out.append(ctx.get_populations(0, _codes(n)))
+    np.testing.assert_allclose(out[1], out[0], rtol=2e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("storage,atol", [(1, 1e-7), (2, 4e-6)])
+def test_learned_step_matches_oracle(storage, atol):
+    """One learned SRT step on a 16^3 periodic box: features, network, relaxation time, collision
+    and periodic streaming against the oracle from the same populations."""
+    import zllbm_b200 as zl
+    n = 16
+    tau0 = 0.505
+    with _box_ctx(storage, n, tau=tau0) as ctx:
+        _run_box(ctx, n, 4, 4)
+        codes = _codes(n)
+        f0 = ctx.get_populations(0, codes)
+        x0 = C.node_features(f0, tau0)
+        net = _net(15, x0)
+    with _box_ctx(storage, n, tau=tau0, les=zl.LES_LEARNED) as ctx2:
+        ctx2.set_populations(0, codes, f0)
+        ctx2.set_closure(_zl_net(net))
+        ctx2.step_level(0)
+        ctx2.synchronize()
+        f1 = ctx2.get_populations(0, codes)
+    # oracle: relax with the network's c, then stream on the periodic box
+    rho, u = C.macros19(f0)
+    neq = f0 - C.feq19(rho, u)
+    c = net.predict_c(x0.astype(np.float32))
+    tau = C.learned_tau(C.stress(neq), tau0, c)
+    post = f0 - neq / tau[:, None]
+    grid = post.reshape(n, n, n, 19)
+    ref = np.empty_like(grid)
+    for q in range(19):
+        cx, cy, cz = C.C19[q].astype(int)
+        ref[..., q] = np.roll(grid[..., q], (cz, cy, cx), axis=(0, 1, 2))
+    ref = ref.reshape(-1, 19)
+    np.testing.assert_allclose(f1, ref, rtol=0, atol=atol)
+
+
+def test_filter_and_training_pairs_match_oracle():
+    import zllbm_b200 as zl
+    torch = _torch()
+    n, fac = 32, 4
+    nc = n // fac
+    tau_f, tau_c = 0.53, 0.5075
+    with _box_ctx(zl.STORAGE_F32, n, tau=tau_f) as ctx:
+        _run_box(ctx, n, 5, 10)
+        filt = torch.empty((nc ** 3, 29), dtype=torch.float32, device="cuda")
+        ctx.filter_level(0, fac, filt.data_ptr())
+        ctx.synchronize()
+        f = ctx.get_populations(0, _codes(n))
+    ref = C.box_filter(f, (n, n, n), fac)
+    got = filt.cpu().numpy()
+    scale = np.abs(ref).max(axis=0) + 1e-30
+    assert (np.abs(got - ref) / scale).max() < 1e-4
+    xd = torch.empty((nc ** 3, 24), dtype=torch.float32, device="cuda")
+    yd = torch.empty(nc ** 3, dtype=torch.float32, device="cuda")
+    sd = torch.empty((nc ** 3, 3), dtype=torch.float32, device="cuda")
+    zl.closure_pairs((nc, nc, nc), filt.data_ptr(), tau_f, tau_c, fac, xd.data_ptr(), yd.data_ptr(), sd.data_ptr())
+    torch.cuda.synchronize()
+    x_ref, y_ref = C.training_pairs(got.astype(np.float64), (nc, nc, nc), tau_f, tau_c, fac)
+    y = yd.cpu().numpy()
+    assert np.abs(y - y_ref).max() < 1e-3 * max(1.0, np.abs(y_ref).max())
+    x = xd.cpu().numpy()
+    xs = np.maximum(np.abs(x_ref).max(axis=0), 1e-3 * np.abs(x_ref[:, 1:19]).max())
+    assert (np.abs(x - x_ref) / xs).max() < 5e-3

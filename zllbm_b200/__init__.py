@@ -57,6 +57,37 @@ class ZlConfig(ctypes.Structure):
     ]
 
 
+MLP_IN, MLP_HIDDEN, MLP_TRAINABLE = 24, 64, 5825
+LES_OFF, LES_SMAGORINSKY, LES_LEARNED = 0, 1, 2
+
+
+class ZlMlp(ctypes.Structure):
+    """zl_mlp: the closure network's parameters (FP32), flat order w1 b1 w2 b2 w3 b3 mean inv_std."""
+    _fields_ = [
+        ("w1", ctypes.c_float * (MLP_HIDDEN * MLP_IN)),
+        ("b1", ctypes.c_float * MLP_HIDDEN),
+        ("w2", ctypes.c_float * (MLP_HIDDEN * MLP_HIDDEN)),
+        ("b2", ctypes.c_float * MLP_HIDDEN),
+        ("w3", ctypes.c_float * MLP_HIDDEN),
+        ("b3", ctypes.c_float),
+        ("in_mean", ctypes.c_float * MLP_IN),
+        ("in_inv_std", ctypes.c_float * MLP_IN),
+    ]
+
+    @staticmethod
+    def from_flat(v) -> "ZlMlp":
+        v = np.ascontiguousarray(np.asarray(v, dtype=np.float32))
+        assert v.size == ctypes.sizeof(ZlMlp) // 4
+        m = ZlMlp()
+        ctypes.memmove(ctypes.addressof(m), v.ctypes.data, v.nbytes)
+        return m
+
+    def flat(self) -> np.ndarray:
+        out = np.empty(ctypes.sizeof(ZlMlp) // 4, dtype=np.float32)
+        ctypes.memmove(out.ctypes.data, ctypes.addressof(self), out.nbytes)
+        return out
+
+
 _lib = None
 
 
@@ -99,6 +130,24 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_moments_noalloc": ([ctypes.c_int, P, i64, P, P], ctypes.c_int),
         "zl_ib_set_vertices": ([P, ctypes.c_int, i64, dp, dp, dp], ctypes.c_int),
         "zl_ib_get_forces": ([P, ctypes.c_int, dp, dp], ctypes.c_int),
+        "zl_set_level_box": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
+                             ctypes.c_int),
+        "zl_set_equilibrium_dense": ([P, ctypes.c_int, P, P], ctypes.c_int),
+        "zl_get_macros_dense": ([P, ctypes.c_int, P, P], ctypes.c_int),
+        "zl_set_closure": ([P, ctypes.POINTER(ZlMlp)], ctypes.c_int),
+        "zl_set_closure_interval": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_closure_features": ([P, ctypes.c_int, P], ctypes.c_int),
+        "zl_filter_level": ([P, ctypes.c_int, ctypes.c_int, P], ctypes.c_int),
+        "zl_closure_pairs": ([ctypes.POINTER(ctypes.c_int32), P, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                              P, P, P, P], ctypes.c_int),
+        "zl_mlp_forward": ([ctypes.POINTER(ZlMlp), P, i64, P, P], ctypes.c_int),
+        "zl_trainer_create": ([ctypes.POINTER(ZlMlp), ctypes.c_int, ctypes.POINTER(P)], ctypes.c_int),
+        "zl_trainer_step": ([P, P, P, i64, ctypes.c_float], ctypes.c_int),
+        "zl_trainer_set_stream": ([P, P], ctypes.c_int),
+        "zl_trainer_loss": ([P, dp], ctypes.c_int),
+        "zl_trainer_gradients": ([P, ctypes.POINTER(ZlMlp)], ctypes.c_int),
+        "zl_trainer_weights": ([P, ctypes.POINTER(ZlMlp)], ctypes.c_int),
+        "zl_trainer_destroy": ([P], None),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -113,7 +162,7 @@ def header_symbols(path: str = HEADER) -> list[str]:
     import re
 
     text = open(path).read()
-    return sorted(set(re.findall(r"^\s*int\s+(zl_\w+)\s*\(", text, flags=re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void)\s+(zl_\w+)\s*\(", text, flags=re.M)))
 
 
 def _u64(a) -> np.ndarray:
@@ -298,6 +347,31 @@ class Context:
     def set_stream(self, stream: int | None):
         self._check(self.lib.zl_set_stream(self.handle, ctypes.c_void_p(stream) if stream else None))
 
+    # full-box levels and device I/O (device pointers as integers, e.g. torch tensor data_ptr())
+    def set_level_box(self, level: int, lo, n):
+        lo_c = (ctypes.c_int32 * 3)(*[int(v) for v in lo])
+        n_c = (ctypes.c_int32 * 3)(*[int(v) for v in n])
+        self._check(self.lib.zl_set_level_box(self.handle, level, lo_c, n_c))
+
+    def set_equilibrium_dense(self, level: int, rho_ptr: int, u_ptr: int):
+        self._check(self.lib.zl_set_equilibrium_dense(self.handle, level, ctypes.c_void_p(rho_ptr),
+                                                      ctypes.c_void_p(u_ptr)))
+
+    def get_macros_dense(self, level: int, rho_ptr: int, u_ptr: int):
+        self._check(self.lib.zl_get_macros_dense(self.handle, level, ctypes.c_void_p(rho_ptr), ctypes.c_void_p(u_ptr)))
+
+    def closure_features(self, level: int, x_ptr: int):
+        self._check(self.lib.zl_closure_features(self.handle, level, ctypes.c_void_p(x_ptr)))
+
+    def filter_level(self, level: int, factor: int, out_ptr: int):
+        self._check(self.lib.zl_filter_level(self.handle, level, factor, ctypes.c_void_p(out_ptr)))
+
+    def set_closure_interval(self, every: int):
+        self._check(self.lib.zl_set_closure_interval(self.handle, every))
+
+    def set_closure(self, net: "ZlMlp | None"):
+        self._check(self.lib.zl_set_closure(self.handle, ctypes.byref(net) if net is not None else None))
+
     def level_info(self, level: int = 0):
         n = ctypes.c_int64()
         ext = (ctypes.c_int32 * 3)()
@@ -347,3 +421,77 @@ def box_codes(dims: int, lo, hi) -> np.ndarray:
         for a in range(dims):
             out |= ((idx[:, a] >> np.uint64(i)) & np.uint64(1)) << np.uint64(dims * i + a)
     return out
+
+
+def closure_pairs(nc, filtered_ptr: int, tau_fine: float, tau_coarse: float, factor: int, x_ptr: int, y_ptr: int,
+                  scratch_ptr: int, stream: int = 0):
+    lib = load_library()
+    n3 = (ctypes.c_int32 * 3)(*[int(v) for v in nc])
+    rc = lib.zl_closure_pairs(n3, ctypes.c_void_p(filtered_ptr), tau_fine, tau_coarse, factor, ctypes.c_void_p(x_ptr),
+                              ctypes.c_void_p(y_ptr), ctypes.c_void_p(scratch_ptr), ctypes.c_void_p(stream or None))
+    if rc:
+        raise ZlError(rc, "zl_closure_pairs")
+
+
+def mlp_forward(net: ZlMlp, x_ptr: int, n: int, y_ptr: int, stream: int = 0):
+    lib = load_library()
+    rc = lib.zl_mlp_forward(ctypes.byref(net), ctypes.c_void_p(x_ptr), n, ctypes.c_void_p(y_ptr),
+                            ctypes.c_void_p(stream or None))
+    if rc:
+        raise ZlError(rc, "zl_mlp_forward")
+
+
+class Trainer:
+    """zl_trainer: tensor-core training of the closure network (device arrays as integer pointers)."""
+
+    def __init__(self, init: ZlMlp, device: int = 0):
+        self.lib = load_library()
+        h = ctypes.c_void_p()
+        rc = self.lib.zl_trainer_create(ctypes.byref(init), device, ctypes.byref(h))
+        if rc:
+            raise ZlError(rc, "zl_trainer_create")
+        self.handle = h
+
+    def _check(self, rc, what):
+        if rc:
+            raise ZlError(rc, what)
+
+    def set_stream(self, stream: int | None):
+        self._check(self.lib.zl_trainer_set_stream(self.handle, ctypes.c_void_p(stream) if stream else None),
+                    "zl_trainer_set_stream")
+
+    def step(self, x_ptr: int, y_ptr: int, n: int, lr: float):
+        self._check(self.lib.zl_trainer_step(self.handle, ctypes.c_void_p(x_ptr), ctypes.c_void_p(y_ptr), n, lr),
+                    "zl_trainer_step")
+
+    def loss(self) -> float:
+        v = ctypes.c_double()
+        self._check(self.lib.zl_trainer_loss(self.handle, ctypes.byref(v)), "zl_trainer_loss")
+        return v.value
+
+    def gradients(self) -> ZlMlp:
+        g = ZlMlp()
+        self._check(self.lib.zl_trainer_gradients(self.handle, ctypes.byref(g)), "zl_trainer_gradients")
+        return g
+
+    def weights(self) -> ZlMlp:
+        w = ZlMlp()
+        self._check(self.lib.zl_trainer_weights(self.handle, ctypes.byref(w)), "zl_trainer_weights")
+        return w
+
+    def close(self):
+        if getattr(self, "handle", None):
+            self.lib.zl_trainer_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -31,6 +31,7 @@ SOURCES = {
     "kernels_f32.cu": [],
     "kernels_f16.cu": [],
     "static_scratch.cu": [],
+    "closure.cu": [],
 }
 
 

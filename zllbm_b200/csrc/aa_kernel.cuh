@@ -72,6 +72,7 @@ struct StepParams {
     // Smagorinsky: tau = tau + tau_sgs with tau_sgs from the non-equilibrium stress
     int les;
     double les_c;           // 18 Cs^2
+    const float* c_node;    // learned closure: per-cell constant c (C = 18 c), or nullptr
 };
 
 // Per-node extras handed to the collision.
@@ -523,7 +524,7 @@ __device__ __forceinline__ void moment_apply(const float* x, const float* coef, 
 
 template <class L, bool Les>
 __device__ __forceinline__ void collide_dev(const float* d, float* out, const StepParams& p, int coll, float* mac,
-                                            const NodeForce* nf) {
+                                            const NodeForce* nf, float les_c = 0.f) {
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
     float neq[Q];
@@ -561,7 +562,7 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
         }
         const float pi2 = pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz);
         const float tau0 = (float)p.tau;
-        const float tau = tau0 + 0.5f * (sqrtf(tau0 * tau0 + (float)p.les_c * sqrtf(2.f * pi2)) - tau0);
+        const float tau = tau0 + 0.5f * (sqrtf(tau0 * tau0 + les_c * sqrtf(2.f * pi2)) - tau0);
         omega = 1.f / tau;
     }
     float fq[Q];
@@ -741,7 +742,9 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
         for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
     }
     if constexpr (St::kDeviation) {
-        collide_dev<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
+        // Smagorinsky constant C: the level's, or 18 c of the learned closure's last evaluation
+        const float les_c = Les ? (p.c_node ? 18.f * __ldg(p.c_node + self) : (float)p.les_c) : 0.f;
+        collide_dev<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr, les_c);
     } else {
         collide_exact<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     }

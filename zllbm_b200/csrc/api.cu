@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <vector>
 #include "zllbm_b200.h"
+#include "closure_launch.cuh"
 #include "topology.cuh"
 
 using namespace zl;
@@ -55,6 +56,7 @@ struct Level {
     DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
     DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
     int n_vertices = 0;
+    DeviceBuffer c_node;     // learned closure: c of the last network evaluation per cell
 };
 
 }  // namespace
@@ -75,6 +77,9 @@ struct zl_ctx {
     long long graph_generation = -1;
     long long generation = 0;   // bumped by every change of levels, interfaces or vertices
     int graph_layouts = 0;      // bit l: level l's layout when the graph was captured
+    DeviceBuffer closure_net;   // zl_mlp of the learned LES closure (zl_set_closure)
+    DeviceBuffer closure_err;   // int: a tensor-core wait of the closure step gave up
+    int closure_every = 1;      // the network runs on every closure_every-th step of a level
 };
 
 namespace {
@@ -198,6 +203,7 @@ int zl_create(const zl_config* config, zl_ctx** out) {
     if (config->storage < ZL_STORAGE_F64 || config->storage > ZL_STORAGE_BF16) return ZL_EINVAL;
     if (config->max_level < 0 || config->max_level >= ZL_MAX_LEVELS) return ZL_EINVAL;
     if (!(config->viscosity > 0.)) return ZL_EINVAL;
+    if (config->les < ZL_LES_OFF || config->les > ZL_LES_LEARNED) return ZL_EINVAL;
     for (int f = 0; f < 6; ++f)
         if (config->bc_kind[f] < ZL_BC_NONE || config->bc_kind[f] > ZL_BC_NONEQ_EXTRAPOLATION) return ZL_EINVAL;
     const int dims = config->lattice == ZL_D2Q9 ? 2 : 3;
@@ -249,10 +255,11 @@ int zl_destroy(zl_ctx* ctx) {
     return ZL_OK;
 }
 
-int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n) {
+// Level set-up from a node list (codes) or, with codes == nullptr, from the full box whose
+// index range is box_mm {min x, min y, min z, max x, max y, max z}.
+static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n, const int* box_mm) {
     int rc = check_level(ctx, level, false);
     if (rc) return rc;
-    if (!codes || n <= 0) return fail(ctx, ZL_EINVAL, "empty node set for level %d", level);
     ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
     const int dims = ctx->dims, q = ctx->q;
     Level& L = ctx->levels[level];
@@ -260,14 +267,18 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     ++ctx->generation;
 
     DeviceBuffer dcodes, dminmax;
-    if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
-    if ((rc = alloc(ctx, dminmax, 6 * sizeof(int)))) return rc;
-    int init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, 0, 0, 0};
-    ZL_CUDA(ctx, cudaMemcpyAsync(dminmax.ptr, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
-    ZL_CUDA(ctx, launch_decode_minmax((const uint64_t*)dcodes.ptr, n, dims, (int*)dminmax.ptr, ctx->stream));
     int mm[6];
-    ZL_CUDA(ctx, cudaMemcpyAsync(mm, dminmax.ptr, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
-    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (codes) {
+        if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
+        if ((rc = alloc(ctx, dminmax, 6 * sizeof(int)))) return rc;
+        int init[6] = {INT32_MAX, INT32_MAX, INT32_MAX, 0, 0, 0};
+        ZL_CUDA(ctx, cudaMemcpyAsync(dminmax.ptr, init, sizeof(init), cudaMemcpyHostToDevice, ctx->stream));
+        ZL_CUDA(ctx, launch_decode_minmax((const uint64_t*)dcodes.ptr, n, dims, (int*)dminmax.ptr, ctx->stream));
+        ZL_CUDA(ctx, cudaMemcpyAsync(mm, dminmax.ptr, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
+        ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    } else {
+        std::memcpy(mm, box_mm, sizeof(mm));
+    }
 
     // Level box.  A periodic axis the level spans completely wraps around (each plane stored
     // once) unless the level also has a non-equilibrium face: the reference then reads its
@@ -328,24 +339,32 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     geo.info = nullptr;
 
     // presence mask; a full box drops it and uses the coordinate-only kernels
-    if ((rc = alloc(ctx, L.info, (size_t)cells * sizeof(uint32_t)))) return rc;
-    ZL_CUDA(ctx, cudaMemsetAsync(L.info.ptr, 0, (size_t)cells * sizeof(uint32_t), ctx->stream));
-    if ((rc = reset_flag(ctx))) return rc;
-    ZL_CUDA(ctx, launch_mark_present((const uint64_t*)dcodes.ptr, n, map, geo, (uint32_t*)L.info.ptr,
-                                     (int*)ctx->scratch_flag.ptr, ctx->stream));
-    DeviceBuffer dcount;
-    if ((rc = alloc(ctx, dcount, sizeof(unsigned long long)))) return rc;
-    ZL_CUDA(ctx, cudaMemsetAsync(dcount.ptr, 0, sizeof(unsigned long long), ctx->stream));
-    ZL_CUDA(ctx, launch_count_present((const uint32_t*)L.info.ptr, cells, (unsigned long long*)dcount.ptr,
-                                      ctx->stream));
-    unsigned long long present = 0;
-    ZL_CUDA(ctx, cudaMemcpyAsync(&present, dcount.ptr, sizeof(present), cudaMemcpyDeviceToHost, ctx->stream));
-    int bad = 0;
-    if ((rc = read_flag(ctx, &bad))) return rc;
-    if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
     const long long box_nodes = (long long)geo.n[0] * geo.n[1] * geo.n[2];
     // forcing and LES run the extended step variant, which reads the per-cell info array
-    if ((long long)present == box_nodes && ctx->cfg.max_level == 0 && !ctx->cfg.forcing && !ctx->cfg.les) {
+    const bool need_info = ctx->cfg.max_level > 0 || ctx->cfg.forcing || ctx->cfg.les;
+    unsigned long long present = 0;
+    if (codes || need_info) {
+        if ((rc = alloc(ctx, L.info, (size_t)cells * sizeof(uint32_t)))) return rc;
+        ZL_CUDA(ctx, cudaMemsetAsync(L.info.ptr, 0, (size_t)cells * sizeof(uint32_t), ctx->stream));
+    }
+    if (codes) {
+        if ((rc = reset_flag(ctx))) return rc;
+        ZL_CUDA(ctx, launch_mark_present((const uint64_t*)dcodes.ptr, n, map, geo, (uint32_t*)L.info.ptr,
+                                         (int*)ctx->scratch_flag.ptr, ctx->stream));
+        DeviceBuffer dcount;
+        if ((rc = alloc(ctx, dcount, sizeof(unsigned long long)))) return rc;
+        ZL_CUDA(ctx, cudaMemsetAsync(dcount.ptr, 0, sizeof(unsigned long long), ctx->stream));
+        ZL_CUDA(ctx, launch_count_present((const uint32_t*)L.info.ptr, cells, (unsigned long long*)dcount.ptr,
+                                          ctx->stream));
+        ZL_CUDA(ctx, cudaMemcpyAsync(&present, dcount.ptr, sizeof(present), cudaMemcpyDeviceToHost, ctx->stream));
+        int bad = 0;
+        if ((rc = read_flag(ctx, &bad))) return rc;
+        if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a node code falls outside the level box", level);
+    } else {
+        present = (unsigned long long)box_nodes;
+        if (need_info) ZL_CUDA(ctx, launch_mark_box(geo, (uint32_t*)L.info.ptr, ctx->stream));
+    }
+    if ((long long)present == box_nodes && !need_info) {
         L.info.release();
     } else {
         geo.info = (const uint32_t*)L.info.ptr;
@@ -437,13 +456,48 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
     L.has_transfer = false;
     L.codes.clear();
     if (ctx->cfg.max_level > 0) {
-        L.codes.assign(codes, codes + n);
+        if (codes) {
+            L.codes.assign(codes, codes + n);
+        } else {
+            // the box's codes, for the interface look-ups of a multi-level context
+            L.codes.reserve((size_t)box_nodes);
+            for (int z = mm[2]; z <= (dims == 3 ? mm[5] : mm[2]); ++z)
+                for (int y = mm[1]; y <= mm[4]; ++y)
+                    for (int x = mm[0]; x <= mm[3]; ++x) {
+                        const uint32_t idx[3] = {(uint32_t)x, (uint32_t)y, (uint32_t)z};
+                        L.codes.push_back(morton_encode(idx, dims));
+                    }
+        }
         std::sort(L.codes.begin(), L.codes.end());
         L.codes.erase(std::unique(L.codes.begin(), L.codes.end()), L.codes.end());
     }
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     L.active = true;
     return ZL_OK;
+}
+
+int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n) {
+    if (!codes || n <= 0) return fail(ctx, ZL_EINVAL, "empty node set for level %d", level);
+    return setup_level(ctx, level, codes, n, nullptr);
+}
+
+int zl_set_level_box(zl_ctx* ctx, int level, const int32_t lo[3], const int32_t n[3]) {
+    int rc = check_level(ctx, level, false);
+    if (rc) return rc;
+    if (!lo || !n) return fail(ctx, ZL_EINVAL, "null box");
+    int mm[6] = {0, 0, 0, 0, 0, 0};
+    for (int a = 0; a < ctx->dims; ++a) {
+        if (n[a] < 1 || lo[a] < 0) return fail(ctx, ZL_EINVAL, "box axis %d: lo %d, n %d", a, lo[a], n[a]);
+        const long long dlo = (long long)ctx->cfg.domain_min[a] << level;
+        const long long dhi = (long long)ctx->cfg.domain_max[a] << level;
+        const bool wraps = ctx->cfg.bc_kind[2 * a] == ZL_BC_PERIODIC && lo[a] == dlo && lo[a] + (long long)n[a] == dhi;
+        mm[a] = lo[a];
+        // a periodic box spanning the domain reads like a node list with the duplicated max plane
+        const long long hi = wraps ? dhi : (long long)lo[a] + n[a] - 1;
+        if (hi > INT32_MAX) return fail(ctx, ZL_EINVAL, "box axis %d too large", a);
+        mm[3 + a] = (int)hi;
+    }
+    return setup_level(ctx, level, nullptr, 0, mm);
 }
 
 static int exchange(zl_ctx* ctx, int level, const uint64_t* codes, double* f_host, double* rho, double* u, int64_t n,
@@ -508,8 +562,32 @@ int zl_step_level(zl_ctx* ctx, int level) {
     Level& L = ctx->levels[level];
     if (L.n_vertices > 0 && (rc = ib_pass(ctx, L, level))) return rc;
     const bool odd = L.even_layout == 1;
-    ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr, L.geo,
-                                L.params, ctx->stream));
+    if (ctx->cfg.les == ZL_LES_LEARNED && ctx->closure_net.ptr) {
+        // the network runs inside the collision of a full periodic D3Q19 box
+        if (ctx->dims != 3 || ctx->cfg.storage == ZL_STORAGE_F64 || L.bnd || ctx->cfg.forcing ||
+            L.nodes != (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2])
+            return fail(ctx, ZL_EINVAL, "the learned closure runs on full periodic D3Q19 boxes, unforced, "
+                                        "in FP32/FP16/BF16 storage");
+        const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
+        if (ctx->closure_every > 1 && L.c_node.bytes != (size_t)cells * sizeof(float)) {
+            if ((rc = alloc(ctx, L.c_node, (size_t)cells * sizeof(float)))) return rc;
+        }
+        if (ctx->closure_every <= 1 || L.steps % ctx->closure_every == 0) {
+            ZL_CUDA(ctx, closure_learned_step(ctx->cfg.storage, ctx->cfg.collision, odd, L.f.ptr, L.geo, L.params,
+                                              (const float*)ctx->closure_net.ptr, (float)(L.params.les_c / 18.),
+                                              ctx->closure_every > 1 ? (float*)L.c_node.ptr : nullptr,
+                                              (int*)ctx->closure_err.ptr, ctx->stream));
+        } else {
+            // steps in between reuse each node's c in the Smagorinsky step kernel
+            StepParams p = L.params;
+            p.c_node = (const float*)L.c_node.ptr;
+            ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr,
+                                        L.geo, p, ctx->stream));
+        }
+    } else {
+        ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd, L.bnd, L.geo.info != nullptr, L.f.ptr,
+                                    L.geo, L.params, ctx->stream));
+    }
     L.even_layout ^= 1;
     // domain faces in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
     // (lbm_grid_interface.cpp:225-314); bounce back is fused into the step kernel unless
@@ -585,7 +663,9 @@ int zl_advance(zl_ctx* ctx, int steps) {
     for (int l = 1; l <= ctx->cfg.max_level; ++l)
         if (!ctx->levels[l].has_transfer)
             return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface before zl_advance", l);
-    if (!ctx->use_graph || steps < 2) return advance_direct(ctx, steps, order);
+    // a closure evaluated every k-th step repeats with period k, not with the graph's two steps
+    const bool periodic_closure = ctx->cfg.les == ZL_LES_LEARNED && ctx->closure_net.ptr && ctx->closure_every > 1;
+    if (!ctx->use_graph || steps < 2 || periodic_closure) return advance_direct(ctx, steps, order);
     // Two background steps bring every level back to the same population layout, so one captured
     // graph of two steps replays for any number of pairs.
     // the captured launches bake in every level's current population layout
@@ -963,6 +1043,11 @@ int zl_ib_get_forces(zl_ctx* ctx, int level, double* vertex_forces, double* tota
 int zl_synchronize(zl_ctx* ctx) {
     if (!ctx) return ZL_EINVAL;
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (ctx->closure_err.ptr) {
+        int e = 0;
+        ZL_CUDA(ctx, cudaMemcpy(&e, ctx->closure_err.ptr, sizeof(int), cudaMemcpyDeviceToHost));
+        if (e) return fail(ctx, ZL_ETIMEOUT, "a tensor-core wait of the learned closure step timed out");
+    }
     return ZL_OK;
 }
 
@@ -1049,6 +1134,93 @@ int zl_upstream_index(int lattice, const uint64_t* codes, int64_t n, int64_t* ou
 int zl_mrt_matrix(int lattice, double tau, double* out) {
     if ((lattice != ZL_D2Q9 && lattice != ZL_D3Q19) || !out || !(tau > 0.)) return ZL_EINVAL;
     host_mrt_matrix(lattice == ZL_D2Q9 ? 2 : 3, 1. / tau, false, out);
+    return ZL_OK;
+}
+
+}  // extern "C"
+
+// A full-box D3Q19 level in FP32 / FP16 / BF16 storage (the dense device I/O and closure kernels)
+static int check_box_level(zl_ctx* ctx, int level) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    const Level& L = ctx->levels[level];
+    if (ctx->dims != 3) return fail(ctx, ZL_EINVAL, "dense level I/O and the closure need D3Q19");
+    if (ctx->cfg.storage == ZL_STORAGE_F64) return fail(ctx, ZL_EINVAL, "dense level I/O needs FP32/FP16/BF16 storage");
+    if (L.nodes != (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2])
+        return fail(ctx, ZL_EINVAL, "level %d is not a full box", level);
+    return ZL_OK;
+}
+
+extern "C" {
+
+int zl_set_equilibrium_dense(zl_ctx* ctx, int level, const float* rho_device, const float* u_device) {
+    int rc = check_box_level(ctx, level);
+    if (rc) return rc;
+    if (!rho_device || !u_device) return fail(ctx, ZL_EINVAL, "null field");
+    Level& L = ctx->levels[level];
+    ZL_CUDA(ctx, closure_box_op(kBoxSetEq, ctx->cfg.storage, L.f.ptr, L.geo, L.params, L.even_layout, rho_device,
+                                const_cast<float*>(u_device), nullptr, 0, nullptr, ctx->stream));
+    return ZL_OK;
+}
+
+int zl_get_macros_dense(zl_ctx* ctx, int level, float* rho_device, float* u_device) {
+    int rc = check_box_level(ctx, level);
+    if (rc) return rc;
+    if (!rho_device || !u_device) return fail(ctx, ZL_EINVAL, "null field");
+    Level& L = ctx->levels[level];
+    ZL_CUDA(ctx, closure_box_op(kBoxGetMacros, ctx->cfg.storage, L.f.ptr, L.geo, L.params, L.even_layout, nullptr,
+                                rho_device, u_device, 0, nullptr, ctx->stream));
+    return ZL_OK;
+}
+
+int zl_closure_features(zl_ctx* ctx, int level, float* x_device) {
+    int rc = check_box_level(ctx, level);
+    if (rc) return rc;
+    if (!x_device) return fail(ctx, ZL_EINVAL, "null output");
+    Level& L = ctx->levels[level];
+    ZL_CUDA(ctx, closure_box_op(kBoxFeatures, ctx->cfg.storage, L.f.ptr, L.geo, L.params, L.even_layout, nullptr,
+                                x_device, nullptr, 0, nullptr, ctx->stream));
+    return ZL_OK;
+}
+
+int zl_filter_level(zl_ctx* ctx, int level, int factor, float* out_device) {
+    int rc = check_box_level(ctx, level);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    if (!out_device || factor < 1) return fail(ctx, ZL_EINVAL, "bad filter arguments");
+    int nc[3];
+    for (int a = 0; a < 3; ++a) {
+        if (L.geo.n[a] % factor) return fail(ctx, ZL_EINVAL, "axis %d: %d nodes not a multiple of %d", a, L.geo.n[a], factor);
+        nc[a] = L.geo.n[a] / factor;
+    }
+    ZL_CUDA(ctx, closure_box_op(kBoxFilter, ctx->cfg.storage, L.f.ptr, L.geo, L.params, L.even_layout, nullptr,
+                                out_device, nullptr, factor, nc, ctx->stream));
+    return ZL_OK;
+}
+
+int zl_set_closure_interval(zl_ctx* ctx, int every) {
+    if (!ctx || every < 1) return ZL_EINVAL;
+    ctx->closure_every = every;
+    ++ctx->generation;
+    return ZL_OK;
+}
+
+int zl_set_closure(zl_ctx* ctx, const zl_mlp* net) {
+    if (!ctx) return ZL_EINVAL;
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    ++ctx->generation;
+    if (!net) {
+        ctx->closure_net.release();
+        return ZL_OK;
+    }
+    int rc = ctx->closure_net.ptr ? ZL_OK : alloc(ctx, ctx->closure_net, sizeof(zl_mlp));
+    if (rc) return rc;
+    if (!ctx->closure_err.ptr) {
+        if ((rc = alloc(ctx, ctx->closure_err, sizeof(int)))) return rc;
+        ZL_CUDA(ctx, cudaMemsetAsync(ctx->closure_err.ptr, 0, sizeof(int), ctx->stream));
+    }
+    ZL_CUDA(ctx, cudaMemcpyAsync(ctx->closure_net.ptr, net, sizeof(zl_mlp), cudaMemcpyHostToDevice, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return ZL_OK;
 }
 

@@ -210,6 +210,22 @@ cudaError_t launch_mark_present(const uint64_t* codes, long long n, const LevelM
     return cudaGetLastError();
 }
 
+// every node of the box is present (ghost frame cells stay absent)
+__global__ void mark_box_kernel(LevelGeom geo, uint32_t* __restrict__ info) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long nn = (long long)geo.n[0] * geo.n[1] * geo.n[2];
+    if (i >= nn) return;
+    const long long x = i % geo.n[0], r = i / geo.n[0], y = r % geo.n[1], z = r / geo.n[1];
+    const long long cell = (x + geo.g[0]) + (long long)geo.a[0] * ((y + geo.g[1]) + (long long)geo.a[1] * (z + geo.g[2]));
+    info[cell] = kInfoPresent;
+}
+
+cudaError_t launch_mark_box(const LevelGeom& geo, uint32_t* info, cudaStream_t s) {
+    const long long nn = (long long)geo.n[0] * geo.n[1] * geo.n[2];
+    mark_box_kernel<<<(unsigned)((nn + 255) / 256), 256, 0, s>>>(geo, info);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_count_present(const uint32_t* info, long long cells, unsigned long long* count, cudaStream_t s) {
     const long long blocks = std::min<long long>((cells + 255) / 256, 148 * 8);
     count_present_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(info, cells, count);
