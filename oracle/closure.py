@@ -15,7 +15,10 @@ reference's Smagorinsky increment with the constant C = 18 c taken per node from
 so y = 1 reproduces Smagorinsky with Cs = 0.1.
 
 Rounding points shared with the device (everything else FP32):
-  * network inputs x_hat = (x - mean) * inv_std, W1, A1 = gelu(Z1), W2 are BF16 tensor-core operands;
+  * network inputs x_hat = (x - mean) * inv_std, W1, A1 = gelu(Z1), W2 are BF16 tensor-core operands,
+    and so are the biases b1, b2 (they ride on a ones column of the products);
+  * inference evaluates GELU on packed BF16 pairs, every operation rounded to BF16 (gelu_bf16);
+    training uses the FP32 GELU;
   * backward: dZ2 and dZ1 are BF16 operands of the gradient products (the bias gradients come
     from a ones column of those products, so they sum the BF16 values); dZ1 uses the FP32 dA1.
 """
@@ -78,6 +81,23 @@ def gelu(z):
     """Tanh-form GELU (Hendrycks and Gimpel, 2016): 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3)))."""
     z = np.asarray(z, dtype=np.float64)
     return 0.5 * z * (1.0 + np.tanh(GELU_K * (z + GELU_A * z ** 3)))
+
+
+A_BF16 = 0.044677734375   # 0.044715 rounded to BFloat16
+K_BF16 = 0.796875         # sqrt(2 / pi) rounded to BFloat16
+
+
+def gelu_bf16(z):
+    """The device's inference GELU on BF16 pairs: z^2, fma(z^2, a, 1), k z, k z (1 + a z^2), tanh,
+    z / 2, fma(z / 2, t, z / 2), each result rounded to BF16 (tanh by numpy in place of the hardware
+    approximation)."""
+    r = lambda v: bf16(np.asarray(v, np.float64).astype(np.float32)).astype(np.float64)
+    zb = r(z)
+    p = r(r(zb * zb) * A_BF16 + 1.0)
+    arg = r(r(zb * K_BF16) * p)
+    t = r(np.tanh(arg))
+    hz = r(zb * 0.5)
+    return r(hz * t + hz)
 
 
 def gelu_grad(z):
@@ -183,19 +203,23 @@ class Mlp:
 
     # forward with the device's rounding points (rounding=False: plain FP64, for finite-difference
     # checks of the backward formulas); returns y and the intermediates of backward
-    def forward(self, x, rounding: bool = True):
+    def forward(self, x, rounding: bool = True, inference: bool = False):
+        """inference=True: the GELU of the device's inference kernels (gelu_bf16)."""
         r = bf16 if rounding else (lambda v: np.asarray(v, np.float64))
         x = np.asarray(x, np.float32 if rounding else np.float64)
         xh = np.asarray(r((x - self.mean) * self.inv_std), np.float64)
-        z1 = xh @ np.asarray(r(self.w1), np.float64).T + self.b1
-        a1 = np.asarray(r(gelu(z1).astype(np.float32) if rounding else gelu(z1)), np.float64)
-        z2 = a1 @ np.asarray(r(self.w2), np.float64).T + self.b2
-        a2 = gelu(z2)
+        z1 = xh @ np.asarray(r(self.w1), np.float64).T + np.asarray(r(self.b1), np.float64)
+        if inference:
+            a1 = gelu_bf16(z1)
+        else:
+            a1 = np.asarray(r(gelu(z1).astype(np.float32) if rounding else gelu(z1)), np.float64)
+        z2 = a1 @ np.asarray(r(self.w2), np.float64).T + np.asarray(r(self.b2), np.float64)
+        a2 = gelu_bf16(z2) if inference else gelu(z2)
         y = a2 @ self.w3.astype(np.float64) + float(self.b3)
         return y, (xh, z1, a1, z2, a2)
 
     def predict_c(self, x, fallback_c=C_UNIT):
-        y, _ = self.forward(x)
+        y, _ = self.forward(x, inference=True)
         c = C_UNIT * np.clip(y, 0.0, Y_MAX)
         return np.where(np.isfinite(y), c, fallback_c)
 

@@ -105,3 +105,11 @@ def test_adam_first_step_moves_by_lr_times_sign():
     g = {k: np.ones_like(np.asarray(getattr(net, k), dtype=np.float64)) * 0.3 for k in opt.m}
     opt.step(g, 1e-2)
     np.testing.assert_allclose(net.w2, before - 1e-2, rtol=0, atol=1e-6)
+
+
+def test_bf16_gelu_constants_and_accuracy():
+    assert C.bf16(np.float32(C.GELU_A)) == np.float32(C.A_BF16)
+    assert C.bf16(np.float32(C.GELU_K)) == np.float32(C.K_BF16)
+    z = np.linspace(-6, 6, 1001)
+    err = np.abs(C.gelu_bf16(z) - C.gelu(z))
+    assert err.max() < 0.03 * max(1.0, np.abs(z).max()) and np.median(err) < 5e-3

@@ -27,12 +27,13 @@ def test_hit_initial_field_is_solenoidal_with_the_requested_rms():
 def test_hit_pipeline_small_box_network_beats_smagorinsky_a_priori():
     from zllbm_b200.hit import HitConfig, run
     cfg = HitConfig(fine=128, factor=4, nu_fine=0.002, coarse_steps=400, checkpoints=4, train_snapshots=2,
-                    train_steps=300, batch=128 * 64, closure_every=4)
+                    train_steps=300, batch=128 * 64, closure_every=4, calibrate_alpha=(0.8, 1.0),
+                    calibrate_cs=(0.1,))
     res = run(cfg, log=lambda m: None)
     tr = res.training
     assert tr["val_loss"] < tr["val_loss_smagorinsky_y1"]
     assert tr["val_loss"] < tr["val_loss_best_constant"]
-    for name in ("smagorinsky", "learned", "learned_every4"):
-        assert res.errors[name]["log_spectrum_rms_k1_to_n/2-1"] is not None
-        assert np.isfinite(res.errors[name]["log_spectrum_rms_k1_to_n/2-1"])
+    for name in ("smagorinsky", "learned", "learned_calibrated", "learned_calibrated_every4"):
+        assert res.errors[name]["error"] is not None
+        assert np.isfinite(res.errors[name]["error"])
         assert res.mlups[name] > 0

@@ -31,15 +31,6 @@ constexpr uint32_t kTmemCols = 256, kColZ1 = 0, kColZ2 = 64, kColDw2 = 128, kCol
 //   MMA5  [dW1 | db1] += dZ1^T [X | 1]
 // with the epilogues (bias, GELU, output, loss, dZ) on the CUDA cores between them.  The weight
 // gradients accumulate in TMEM over the CTA's tiles and are added to `grad` once at the end.
-__device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& phase, int* err) {
-    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    if (ok) phase ^= 1u;
-    const bool failed = __syncthreads_or(!ok) != 0;
-    if (failed && threadIdx.x == 0) atomicExch(err, 1);
-    tc::fence_after_sync();
-    return !failed;
-}
-
 __device__ __forceinline__ float warp_sum(float v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -53,19 +44,16 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
     extern __shared__ __align__(1024) uint8_t sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     float* fs = reinterpret_cast<float*>(sm + kTrF);
-    float *b1 = fs, *b2 = fs + 64, *w3 = fs + 128, *b3 = fs + 192, *mean = fs + 200, *istd = fs + 224;
+    float *w3 = fs + 128, *b3 = fs + 192, *mean = fs + 200, *istd = fs + 224;
     float* red = fs + 256;  // dw3 [64], db3, loss
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kTrBar);
     uint32_t* tbase = reinterpret_cast<uint32_t*>(sm + kTrBar + 8);
 
-    stage_weights(net, sm + kTrW1, sm + kTrW2, b1, b2, w3, b3, mean, istd);
+    stage_weights(net, sm + kTrW1, sm + kTrW2, w3, b3, mean, istd, sm + kTrA1);
     if (tid < 66) red[tid] = 0.f;
     {
-        // constant columns: A1's ones column and zero padding, the zero halves of the dZ tiles
-        float v[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        st_row_chunk(sm + kTrA1, tid, 64, kSboA1, v);
-        v[0] = 0.f;
-        st_row_chunk(sm + kTrA1, tid, 72, kSboA1, v);
+        // the zero halves of the dZ tiles
+        const float v[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int c = 64; c < 128; c += 8) {
             st_row_chunk(sm + kTrDz2, tid, c, kSboDz, v);
             st_row_chunk(sm + kTrDz1, tid, c, kSboDz, v);
@@ -100,7 +88,7 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
         }
         const float t = valid ? target[g] : 0.f;
 
-        // MMA1: Z1 = X W1^T
+        // MMA1: Z1 = [X | 1] [W1 | b1]^T
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
@@ -119,19 +107,19 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 float th;
-                v[i] = gelu(v[i] + b1[16 * c + i], th);
+                v[i] = gelu(v[i], th);
             }
             st_row_chunk(sm + kTrA1, tid, 16 * c, kSboA1, v);
             st_row_chunk(sm + kTrA1, tid, 16 * c + 8, kSboA1, v + 8);
         }
 
-        // MMA2: Z2 = A1 W2^T
+        // MMA2: Z2 = [A1 | 1] [W2 | b2]^T
         tc::fence_proxy_async();
         tc::fence_before_sync();
         __syncthreads();
         if (tid == 0) {
             tc::fence_after_sync();
-            for (int s = 0; s < 4; ++s)
+            for (int s = 0; s < 5; ++s)
                 tc::mma_bf16(tmem + kColZ2, tc::desc_kmajor(sA1, kSboA1, s), tc::desc_kmajor(sW2, kSboW2, s),
                              kIdescFwd, s > 0);
             tc::commit(bar);
@@ -145,7 +133,7 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 float th;
-                y = fmaf(gelu(v[i] + b2[16 * c + i], th), w3[16 * c + i], y);
+                y = fmaf(gelu(v[i], th), w3[16 * c + i], y);
             }
         }
         const float e = valid ? y - t : 0.f;
@@ -159,7 +147,7 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
                 const int j = 16 * c + i;
-                const float z = v[i] + b2[j];
+                const float z = v[i];
                 float th;
                 const float a2 = gelu(z, th);
                 const float s = warp_sum(dy * a2);
@@ -192,7 +180,7 @@ __global__ void __launch_bounds__(128, 1) mlp_train_kernel(const float* __restri
             tc::tmem_ld16(tmem + lane_addr + kColZ1 + 16 * c, z1);
 #pragma unroll
             for (int i = 0; i < 16; ++i) {
-                const float z = z1[i] + b1[16 * c + i];
+                const float z = z1[i];
                 float th;
                 gelu(z, th);
                 da[i] *= gelu_grad(z, th);
@@ -282,92 +270,84 @@ __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, 
 
 // ---------------------------------------------------------------- forward (inference)
 // Shared memory of the inference kernels (bytes); TMEM: 64 columns, Z1 then Z2
-constexpr uint32_t kFwX = 0, kFwA1 = kFwX + kBytesX, kFwW1 = kFwA1 + kBytesA1f, kFwW2 = kFwW1 + kBytesW1,
+constexpr uint32_t kFwX = 0, kFwA1 = kFwX + kBytesX, kFwW1 = kFwA1 + kBytesA1, kFwW2 = kFwW1 + kBytesW1,
                    kFwF = kFwW2 + kBytesW2, kFwBar = kFwF + 1024, kFwSmem = kFwBar + 64;
 constexpr uint32_t kFwSmemLaunch = kFwSmem;
 constexpr uint32_t kInferCols = 64;
 constexpr int kMaxCtaPerSm = 512 / kInferCols;
 
-__global__ void __launch_bounds__(128) mlp_forward_kernel(const float* __restrict__ net, const float* __restrict__ x,
-                                                          long long n, float* __restrict__ out, int* __restrict__ err) {
-    extern __shared__ __align__(1024) uint8_t sm[];
-    const int tid = threadIdx.x, warp = tid >> 5;
+// Set-up shared by the inference kernels: weights staged, TMEM allocated, barrier initialised.
+__device__ __forceinline__ InferTile infer_setup(uint8_t* sm, const float* net, float*& mean, float*& istd) {
+    const int warp = threadIdx.x >> 5;
     float* fs = reinterpret_cast<float*>(sm + kFwF);
-    float *b1 = fs, *b2 = fs + 64, *w3 = fs + 128, *b3 = fs + 192, *mean = fs + 200, *istd = fs + 224;
+    float *w3 = fs + 128, *b3 = fs + 192;
+    mean = fs + 200;
+    istd = fs + 224;
     uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kFwBar);
     uint32_t* tbase = reinterpret_cast<uint32_t*>(sm + kFwBar + 8);
-    stage_weights(net, sm + kFwW1, sm + kFwW2, b1, b2, w3, b3, mean, istd);
+    stage_weights(net, sm + kFwW1, sm + kFwW2, w3, b3, mean, istd, sm + kFwA1);
     if (warp == 0) tc::tmem_alloc(tbase, kInferCols);
-    if (tid == 0) tc::mbar_init(bar, 1);
+    if (threadIdx.x == 0) tc::mbar_init(bar, 1);
     tc::fence_before_sync();
     __syncthreads();
     tc::fence_after_sync();
-    const uint32_t tmem = *tbase;
-    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
-    const uint32_t sX = tc::smem_u32(sm + kFwX), sA1 = tc::smem_u32(sm + kFwA1), sW1 = tc::smem_u32(sm + kFwW1),
-                   sW2 = tc::smem_u32(sm + kFwW2);
+    InferTile it;
+    it.a1s = sm + kFwA1;
+    it.sX = tc::smem_u32(sm + kFwX);
+    it.sA1 = tc::smem_u32(sm + kFwA1);
+    it.sW1 = tc::smem_u32(sm + kFwW1);
+    it.sW2 = tc::smem_u32(sm + kFwW2);
+    it.tmem = *tbase;
+    it.lane_addr = (uint32_t)(warp * 32) << 16;
+    it.bar = bar;
+    it.w3 = w3;
+    it.b3 = *b3;
+    return it;
+}
+
+__device__ __forceinline__ void infer_teardown(const InferTile& it, bool ok, uint32_t phase) {
+    if (!ok) tc::mbar_wait(it.bar, phase, kWaitLimit);  // give the tensor cores a last bounded wait
+    tc::fence_before_sync();
+    __syncthreads();
+    if ((threadIdx.x >> 5) == 0) {
+        tc::fence_after_sync();
+        tc::tmem_dealloc(it.tmem, kInferCols);
+    }
+}
+
+// Write this thread's normalised feature row [x_hat | 1 | 0] into the X tile.
+__device__ __forceinline__ void write_x_row(uint8_t* xs, const float* x, const float* mean, const float* istd,
+                                            bool valid) {
+    float v[32];
+#pragma unroll
+    for (int k = 0; k < kIn; ++k) v[k] = valid ? (x[k] - mean[k]) * istd[k] : 0.f;
+    v[kIn] = 1.f;
+#pragma unroll
+    for (int k = kIn + 1; k < 32; ++k) v[k] = 0.f;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) st_row_chunk(xs, threadIdx.x, 8 * c, kSboX, v + 8 * c);
+}
+
+__global__ void __launch_bounds__(128) mlp_forward_kernel(const float* __restrict__ net, const float* __restrict__ x,
+                                                          long long n, float* __restrict__ out, int* __restrict__ err) {
+    extern __shared__ __align__(1024) uint8_t sm[];
+    float *mean, *istd;
+    const InferTile it = infer_setup(sm, net, mean, istd);
     uint32_t phase = 0;
     bool ok = true;
     const long long tiles = (n + kTile - 1) / kTile;
     for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const long long g = tile * kTile + tid;
+        const long long g = tile * kTile + threadIdx.x;
         const bool valid = g < n;
-        {
-            float v[32];
+        float xv[kIn];
 #pragma unroll
-            for (int k = 0; k < kIn; ++k) v[k] = valid ? (x[g * kIn + k] - mean[k]) * istd[k] : 0.f;
-#pragma unroll
-            for (int k = 24; k < 32; ++k) v[k] = 0.f;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) st_row_chunk(sm + kFwX, tid, 8 * c, kSboX, v + 8 * c);
-        }
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            for (int s = 0; s < 2; ++s)
-                tc::mma_bf16(tmem, tc::desc_kmajor(sX, kSboX, s), tc::desc_kmajor(sW1, kSboW1, s), kIdescFwd, s > 0);
-            tc::commit(bar);
-        }
-        if (!(ok = wait_mma(bar, phase, err))) break;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float v[16];
-            tc::tmem_ld16(tmem + lane_addr + 16 * c, v);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) v[i] = gelu_fast(v[i] + b1[16 * c + i]);
-            st_row_chunk(sm + kFwA1, tid, 16 * c, kSboA1f, v);
-            st_row_chunk(sm + kFwA1, tid, 16 * c + 8, kSboA1f, v + 8);
-        }
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            for (int s = 0; s < 4; ++s)
-                tc::mma_bf16(tmem, tc::desc_kmajor(sA1, kSboA1f, s), tc::desc_kmajor(sW2, kSboW2, s), kIdescFwd,
-                             s > 0);
-            tc::commit(bar);
-        }
-        if (!(ok = wait_mma(bar, phase, err))) break;
-        float y = *b3;
-#pragma unroll
-        for (int c = 0; c < 4; ++c) {
-            float v[16];
-            tc::tmem_ld16(tmem + lane_addr + 16 * c, v);
-#pragma unroll
-            for (int i = 0; i < 16; ++i) y = fmaf(gelu_fast(v[i] + b2[16 * c + i]), w3[16 * c + i], y);
-        }
+        for (int k = 0; k < kIn; ++k) xv[k] = valid ? x[g * kIn + k] : 0.f;
+        write_x_row(sm + kFwX, xv, mean, istd, valid);
+        float y;
+        if (!(ok = infer_tile(it, phase, err, y))) break;
         if (valid) out[g] = y;
     }
-    if (!ok) tc::mbar_wait(bar, phase, kWaitLimit);
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) {
-        tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, kInferCols);
-    }
+    infer_teardown(it, ok, phase);
 }
 
 // ---------------------------------------------------------------- full-box I/O, features, filter
@@ -427,9 +407,7 @@ __global__ void features_kernel(const S* __restrict__ f, LevelGeom geo, StepPara
     float d[19], neq[19], mac[4], v[kIn];
     load_node(f, geo, box_coord(geo, i), even, d);
     feq_neq_dev<D3Q19>(d, neq, p.scale, p.inv_scale, mac);
-#pragma unroll
-    for (int q = 0; q < 19; ++q) neq[q] *= p.inv_scale;
-    features(mac[0], neq, (float)p.tau, v);
+    features(mac[0], neq, (float)p.tau, v, nullptr, p.inv_scale);
 #pragma unroll
     for (int k = 0; k < kIn; ++k) x[i * kIn + k] = v[k];
 }
@@ -575,31 +553,18 @@ __global__ void pairs_stage2_kernel(Grid3 g, const float* __restrict__ filt, con
 // layers, and each thread relaxes with tau = tau0 + 0.5 (sqrt(tau0^2 + 18 c sqrt(2 Pi:Pi)) - tau0)
 // and streams; c is also stored per node (c_node) for the steps that reuse it.  The grid is the
 // number of CTAs that fit on the GPU (shared memory 37 KiB, TMEM 64 columns per CTA).
-constexpr uint32_t kLsX = kFwX, kLsA1 = kFwA1, kLsW1 = kFwW1, kLsW2 = kFwW2, kLsF = kFwF, kLsBar = kFwBar;
 constexpr uint32_t kLsSmemLaunch = kFwSmem;
 
 template <class S, int Coll, bool Odd>
-__global__ void __launch_bounds__(128) learned_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p,
+__global__ void __launch_bounds__(128, 5) learned_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p,
                                                            const float* __restrict__ net, float fallback_c,
                                                            float* __restrict__ c_node, int* __restrict__ err) {
     using Tb = Tables<D3Q19>;
     using St = Storage<S>;
     extern __shared__ __align__(1024) uint8_t sm[];
-    const int tid = threadIdx.x, warp = tid >> 5;
-    float* fs = reinterpret_cast<float*>(sm + kLsF);
-    float *b1 = fs, *b2 = fs + 64, *w3 = fs + 128, *b3 = fs + 192, *mean = fs + 200, *istd = fs + 224;
-    uint64_t* bar = reinterpret_cast<uint64_t*>(sm + kLsBar);
-    uint32_t* tbase = reinterpret_cast<uint32_t*>(sm + kLsBar + 8);
-    stage_weights(net, sm + kLsW1, sm + kLsW2, b1, b2, w3, b3, mean, istd);
-    if (warp == 0) tc::tmem_alloc(tbase, kInferCols);
-    if (tid == 0) tc::mbar_init(bar, 1);
-    tc::fence_before_sync();
-    __syncthreads();
-    tc::fence_after_sync();
-    const uint32_t tmem = *tbase;
-    const uint32_t lane_addr = (uint32_t)(warp * 32) << 16;
-    const uint32_t sX = tc::smem_u32(sm + kLsX), sA1 = tc::smem_u32(sm + kLsA1), sW1 = tc::smem_u32(sm + kLsW1),
-                   sW2 = tc::smem_u32(sm + kLsW2);
+    float *mean, *istd;
+    const InferTile it = infer_setup(sm, net, mean, istd);
+    const int tid = threadIdx.x;
     const float tau0 = (float)p.tau;
     const long long nn = (long long)geo.n[0] * geo.n[1] * geo.n[2];
     const long long tiles = (nn + kTile - 1) / kTile;
@@ -643,65 +608,21 @@ __global__ void __launch_bounds__(128) learned_step_kernel(S* __restrict__ f, Le
             else pre[q] = St::load_raw(f + q * st + self);
         }
         float pp;  // sqrt(2 Pi:Pi) of the unscaled non-equilibrium part
+        float neq[19], mac[4];
+        feq_neq_dev<D3Q19>(pre, neq, p.scale, p.inv_scale, mac);
         {
-            float neq[19], mac[4], x[kIn];
-            feq_neq_dev<D3Q19>(pre, neq, p.scale, p.inv_scale, mac);
-#pragma unroll
-            for (int q = 0; q < 19; ++q) neq[q] *= p.inv_scale;
-            features(mac[0], neq, tau0, x, &pp);
-            float v[32];
-#pragma unroll
-            for (int k = 0; k < kIn; ++k) v[k] = valid ? (x[k] - mean[k]) * istd[k] : 0.f;
-#pragma unroll
-            for (int k = kIn; k < 32; ++k) v[k] = 0.f;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) st_row_chunk(sm + kLsX, tid, 8 * k, kSboX, v + 8 * k);
+            float x[kIn];
+            features(mac[0], neq, tau0, x, &pp, p.inv_scale);
+            write_x_row(sm + kFwX, x, mean, istd, valid);
         }
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            for (int s = 0; s < 2; ++s)
-                tc::mma_bf16(tmem, tc::desc_kmajor(sX, kSboX, s), tc::desc_kmajor(sW1, kSboW1, s), kIdescFwd, s > 0);
-            tc::commit(bar);
-        }
-        if (!(ok = wait_mma(bar, phase, err))) break;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            float v[16];
-            tc::tmem_ld16(tmem + lane_addr + 16 * k, v);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = gelu_fast(v[j] + b1[16 * k + j]);
-            st_row_chunk(sm + kLsA1, tid, 16 * k, kSboA1f, v);
-            st_row_chunk(sm + kLsA1, tid, 16 * k + 8, kSboA1f, v + 8);
-        }
-        tc::fence_proxy_async();
-        tc::fence_before_sync();
-        __syncthreads();
-        if (tid == 0) {
-            tc::fence_after_sync();
-            for (int s = 0; s < 4; ++s)
-                tc::mma_bf16(tmem, tc::desc_kmajor(sA1, kSboA1f, s), tc::desc_kmajor(sW2, kSboW2, s), kIdescFwd,
-                             s > 0);
-            tc::commit(bar);
-        }
-        if (!(ok = wait_mma(bar, phase, err))) break;
-        float y = *b3;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            float v[16];
-            tc::tmem_ld16(tmem + lane_addr + 16 * k, v);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) y = fmaf(gelu_fast(v[j] + b2[16 * k + j]), w3[16 * k + j], y);
-        }
+        float y;
+        if (!(ok = infer_tile(it, phase, err, y))) break;
         if (!valid) continue;
         const float cc = isfinite(y) ? kCUnit * fminf(fmaxf(y, 0.f), kYMax) : fallback_c;
         if (c_node) c_node[self] = cc;
         const float tau = tau0 + 0.5f * (sqrtf(fmaf(tau0, tau0, 18.f * cc * pp)) - tau0);
         const float omega = 1.f / tau;
-        float neq[19], mac[4], post[19];
-        feq_neq_dev<D3Q19>(pre, neq, p.scale, p.inv_scale, mac);
+        float post[19];
         if (Coll == kSrt) {
 #pragma unroll
             for (int q = 0; q < 19; ++q) post[q] = fmaf(-omega, neq[q], pre[q]);
@@ -718,13 +639,7 @@ __global__ void __launch_bounds__(128) learned_step_kernel(S* __restrict__ f, Le
             else St::store_raw(f + Tb::opp(q) * st + self, post[q]);
         }
     }
-    if (!ok) tc::mbar_wait(bar, phase, kWaitLimit);
-    tc::fence_before_sync();
-    __syncthreads();
-    if (warp == 0) {
-        tc::fence_after_sync();
-        tc::tmem_dealloc(tmem, kInferCols);
-    }
+    infer_teardown(it, ok, phase);
 }
 
 template <class S>

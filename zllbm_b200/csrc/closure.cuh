@@ -34,24 +34,21 @@ constexpr uint32_t kWaitLimit = 1u << 22;  // mbarrier polls before a wait gives
 // X  [128 samples x 32]: x_hat (24), a ones column (24), zeros        row groups 512 B apart
 // A1 [128 samples x 80]: A1 (64), a ones column (64), zeros           1280 B
 // DZ [128 samples x 128]: dZ (64), zeros (the M = 128 padding of the weight-gradient products)
-// W1 [64 x 32], W2 [64 x 64]
-constexpr uint32_t kSboX = 512, kSboA1 = 1280, kSboDz = 2048, kSboW1 = 512, kSboW2 = 1024;
+// W1 [64 x 32]: W1 (24), b1 (24), zeros;  W2 [64 x 80]: W2 (64), b2 (64), zeros
+// The ones columns carry the biases through the products: Z1 = [X | 1] [W1 | b1]^T, likewise Z2.
+constexpr uint32_t kSboX = 512, kSboA1 = 1280, kSboDz = 2048, kSboW1 = 512, kSboW2 = 1280;
 constexpr uint32_t kBytesX = 128 * kSboX / 8, kBytesA1 = 128 * kSboA1 / 8, kBytesDz = 128 * kSboDz / 8,
                    kBytesW1 = 64 * kSboW1 / 8, kBytesW2 = 64 * kSboW2 / 8;
 // every descriptor stays inside its buffer
 static_assert(tc::extent_kmajor(128, kSboX, 2) <= kBytesX, "X as A (K = 32)");
 static_assert(tc::extent_mnmajor(32, kSboX, 8) <= kBytesX, "X as B of dW1 (N = 32, K = 128)");
-static_assert(tc::extent_kmajor(128, kSboA1, 4) <= kBytesA1, "A1 as A (K = 64)");
+static_assert(tc::extent_kmajor(128, kSboA1, 5) <= kBytesA1, "[A1 | 1] as A (K = 80)");
 static_assert(tc::extent_mnmajor(80, kSboA1, 8) <= kBytesA1, "A1 as B of dW2 (N = 80, K = 128)");
 static_assert(tc::extent_kmajor(128, kSboDz, 4) <= kBytesDz, "dZ2 as A of dA1 (K = 64)");
 static_assert(tc::extent_mnmajor(128, kSboDz, 8) <= kBytesDz, "dZ as A of dW (M = 128, K = 128)");
 static_assert(tc::extent_kmajor(64, kSboW1, 2) <= kBytesW1, "W1 as B (N = 64, K = 32)");
-static_assert(tc::extent_kmajor(64, kSboW2, 4) <= kBytesW2, "W2 as B (N = 64, K = 64)");
+static_assert(tc::extent_kmajor(64, kSboW2, 5) <= kBytesW2, "[W2 | b2] as B (N = 64, K = 80)");
 static_assert(tc::extent_mnmajor(64, kSboW2, 4) <= kBytesW2, "W2^T as B of dA1 (N = 64, K = 64)");
-
-// inference keeps A1 without the ones column: 64 columns, row groups 1024 B apart
-constexpr uint32_t kSboA1f = 1024, kBytesA1f = 128 * kSboA1f / 8;
-static_assert(tc::extent_kmajor(128, kSboA1f, 4) <= kBytesA1f, "A1 as A of the inference (K = 64)");
 
 constexpr uint32_t kIdescFwd = tc::idesc_bf16(128, 64, false, false);   // X W1^T, A1 W2^T
 constexpr uint32_t kIdescDa1 = tc::idesc_bf16(128, 64, false, true);    // dZ2 W2
@@ -62,11 +59,20 @@ __device__ __forceinline__ float gelu(float z, float& t) {
     t = tanhf(kGeluK * fmaf(kGeluA * z, z * z, z));
     return 0.5f * z * (1.f + t);
 }
-// inference: the tanh of the same formula by the hardware approximation (tanh.approx.f32)
-__device__ __forceinline__ float gelu_fast(float z) {
-    float t;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(t) : "f"(kGeluK * fmaf(kGeluA * z, z * z, z)));
-    return 0.5f * z * (1.f + t);
+// Inference: the same GELU on packed BF16 pairs (the result is a BF16 operand anyway):
+// z^2, 1 + a z^2, k z, k z (1 + a z^2), tanh.approx.bf16x2, z/2, z/2 + z/2 t -- every step rounds to
+// BF16 (constants a, k rounded to BF16 too).
+__device__ __forceinline__ uint32_t gelu_bf16x2(float z0, float z1) {
+    const __nv_bfloat162 z = __floats2bfloat162_rn(z0, z1);
+    const __nv_bfloat162 a = __float2bfloat162_rn(kGeluA), k = __float2bfloat162_rn(kGeluK),
+                         one = __float2bfloat162_rn(1.f), half = __float2bfloat162_rn(0.5f);
+    const __nv_bfloat162 p = __hfma2(__hmul2(z, z), a, one);
+    const __nv_bfloat162 arg = __hmul2(__hmul2(z, k), p);
+    uint32_t t;
+    asm("tanh.approx.bf16x2 %0, %1;" : "=r"(t) : "r"(*reinterpret_cast<const uint32_t*>(&arg)));
+    const __nv_bfloat162 hz = __hmul2(z, half);
+    const __nv_bfloat162 out = __hfma2(hz, *reinterpret_cast<const __nv_bfloat162*>(&t), hz);
+    return *reinterpret_cast<const uint32_t*>(&out);
 }
 __device__ __forceinline__ float gelu_grad(float z, float t) {
     return fmaf(0.5f, 1.f + t, 0.5f * z * (1.f - t * t) * kGeluK * fmaf(3.f * kGeluA, z * z, 1.f));
@@ -76,29 +82,107 @@ __device__ __forceinline__ void st_row_chunk(uint8_t* tile, uint32_t row, uint32
     *reinterpret_cast<uint4*>(tile + tc::tile_offset(row, col, sbo)) = tc::pack_bf16x8(v);
 }
 
-// Stage W1 and W2 as BF16 tiles (W1's columns 24 .. 31 zero) and the FP32 vectors.
-__device__ __forceinline__ void stage_weights(const float* __restrict__ net, uint8_t* w1s, uint8_t* w2s, float* b1,
-                                              float* b2, float* w3, float* b3, float* mean, float* istd) {
+// Stage [W1 | b1] and [W2 | b2] as BF16 tiles and the FP32 vectors; write this thread's row of
+// A1's constant columns (the ones column and the zero padding).
+__device__ __forceinline__ void stage_weights(const float* __restrict__ net, uint8_t* w1s, uint8_t* w2s, float* w3,
+                                              float* b3, float* mean, float* istd, uint8_t* a1s) {
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int e = tid; e < kHid * 32; e += nt) {
         const int j = e >> 5, k = e & 31;
-        *reinterpret_cast<__nv_bfloat16*>(w1s + tc::tile_offset(j, k, kSboW1)) =
-            __float2bfloat16_rn(k < kIn ? net[oW1 + j * kIn + k] : 0.f);
+        const float v = k < kIn ? net[oW1 + j * kIn + k] : (k == kIn ? net[oB1 + j] : 0.f);
+        *reinterpret_cast<__nv_bfloat16*>(w1s + tc::tile_offset(j, k, kSboW1)) = __float2bfloat16_rn(v);
     }
-    for (int e = tid; e < kHid * kHid; e += nt) {
-        const int j = e >> 6, i = e & 63;
-        *reinterpret_cast<__nv_bfloat16*>(w2s + tc::tile_offset(j, i, kSboW2)) = __float2bfloat16_rn(net[oW2 + e]);
+    for (int e = tid; e < kHid * 80; e += nt) {
+        const int j = e / 80, i = e % 80;
+        const float v = i < kHid ? net[oW2 + j * kHid + i] : (i == kHid ? net[oB2 + j] : 0.f);
+        *reinterpret_cast<__nv_bfloat16*>(w2s + tc::tile_offset(j, i, kSboW2)) = __float2bfloat16_rn(v);
     }
-    for (int e = tid; e < kHid; e += nt) {
-        b1[e] = net[oB1 + e];
-        b2[e] = net[oB2 + e];
-        w3[e] = net[oW3 + e];
-    }
+    for (int e = tid; e < kHid; e += nt) w3[e] = net[oW3 + e];
     for (int e = tid; e < kIn; e += nt) {
         mean[e] = net[oMean + e];
         istd[e] = net[oInvStd + e];
     }
     if (tid == 0) *b3 = net[oB3];
+    float v[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    st_row_chunk(a1s, tid, 64, kSboA1, v);
+    v[0] = 0.f;
+    st_row_chunk(a1s, tid, 72, kSboA1, v);
+}
+
+__device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& phase, int* err) {
+    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
+    if (ok) phase ^= 1u;
+    const bool failed = __syncthreads_or(!ok) != 0;
+    if (failed && threadIdx.x == 0) atomicExch(err, 1);
+    tc::fence_after_sync();
+    return !failed;
+}
+
+// Inference of one tile: X (this thread's row written by the caller) -> y of this thread's row.
+// 64 TMEM columns (Z1, then Z2); returns false if a tensor-core wait gave up.
+struct InferTile {
+    uint8_t* a1s;
+    uint32_t sX, sA1, sW1, sW2, tmem, lane_addr;
+    uint64_t* bar;
+    const float* w3;
+    float b3;
+};
+
+__device__ __forceinline__ bool infer_tile(const InferTile& it, uint32_t& phase, int* err, float& y) {
+    const int tid = threadIdx.x;
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        tc::fence_after_sync();
+        for (int s = 0; s < 2; ++s)
+            tc::mma_bf16(it.tmem, tc::desc_kmajor(it.sX, kSboX, s), tc::desc_kmajor(it.sW1, kSboW1, s), kIdescFwd,
+                         s > 0);
+        tc::commit(it.bar);
+    }
+    if (!wait_mma(it.bar, phase, err)) return false;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float v[16];
+        tc::tmem_ld16(it.tmem + it.lane_addr + 16 * c, v);
+        uint4 lo, hi;
+        lo.x = gelu_bf16x2(v[0], v[1]);
+        lo.y = gelu_bf16x2(v[2], v[3]);
+        lo.z = gelu_bf16x2(v[4], v[5]);
+        lo.w = gelu_bf16x2(v[6], v[7]);
+        hi.x = gelu_bf16x2(v[8], v[9]);
+        hi.y = gelu_bf16x2(v[10], v[11]);
+        hi.z = gelu_bf16x2(v[12], v[13]);
+        hi.w = gelu_bf16x2(v[14], v[15]);
+        *reinterpret_cast<uint4*>(it.a1s + tc::tile_offset(tid, 16 * c, kSboA1)) = lo;
+        *reinterpret_cast<uint4*>(it.a1s + tc::tile_offset(tid, 16 * c + 8, kSboA1)) = hi;
+    }
+    tc::fence_proxy_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {
+        tc::fence_after_sync();
+        for (int s = 0; s < 5; ++s)
+            tc::mma_bf16(it.tmem, tc::desc_kmajor(it.sA1, kSboA1, s), tc::desc_kmajor(it.sW2, kSboW2, s), kIdescFwd,
+                         s > 0);
+        tc::commit(it.bar);
+    }
+    if (!wait_mma(it.bar, phase, err)) return false;
+    float acc = it.b3;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float v[16];
+        tc::tmem_ld16(it.tmem + it.lane_addr + 16 * c, v);
+#pragma unroll
+        for (int i = 0; i < 16; i += 2) {
+            const uint32_t g = gelu_bf16x2(v[i], v[i + 1]);
+            const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&g));
+            acc = fmaf(a.x, it.w3[16 * c + i], acc);
+            acc = fmaf(a.y, it.w3[16 * c + i + 1], acc);
+        }
+    }
+    y = acc;
+    return true;
 }
 
 // ---------------------------------------------------------------- features
@@ -106,39 +190,51 @@ __device__ __forceinline__ void stage_weights(const float* __restrict__ net, uin
 // the 19 MRT moments of f - feq over rho (the conserved four are zero), tr S, S:S, tr(Sd^3),
 // |Sd| and the Cs = 0.1 Smagorinsky increment, S = -3 Pi / (2 rho tau0).
 // spp (optional) receives sqrt(2 Pi:Pi), the stress norm of the relaxation formula.
-__device__ __forceinline__ void features(float rho, const float* neq, float tau0, float* x, float* spp = nullptr) {
-    using Tb = Tables<D3Q19>;
-    const float ir = 1.f / rho;
-#pragma unroll
-    for (int k = 0; k < 19; ++k) {
-        // mass and momentum of f - feq vanish (the collision conserves them): exact zero inputs,
-        // not rounding noise that an input normalisation would amplify
-        if (k == 0 || k == 3 || k == 5 || k == 7) {
-            x[k] = 0.f;
-            continue;
-        }
-        float m = 0.f;
-#pragma unroll
-        for (int q = 0; q < 19; ++q) {
-            const int c = Tb::M(k, q);
-            if (c == 1) m += neq[q];
-            else if (c == -1) m -= neq[q];
-            else if (c != 0) m = fmaf((float)c, neq[q], m);
-        }
-        x[k] = m * ir;
-    }
-    float p[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // xx yy zz xy xz yz
-#pragma unroll
-    for (int q = 1; q < 19; ++q) {
-        const int cx = Tb::cx(q), cy = Tb::cy(q), cz = Tb::cz(q);
-        if (cx) p[0] += neq[q];
-        if (cy) p[1] += neq[q];
-        if (cz) p[2] += neq[q];
-        if (cx * cy) p[3] += cx * cy > 0 ? neq[q] : -neq[q];
-        if (cx * cz) p[4] += cx * cz > 0 ? neq[q] : -neq[q];
-        if (cy * cz) p[5] += cy * cz > 0 ? neq[q] : -neq[q];
-    }
-    const float k = -1.5f * ir / tau0;
+// `unscale` multiplies neq first (the inverse storage scale for scaled deviations).
+__device__ __forceinline__ void features(float rho, const float* neq, float tau0, float* x, float* spp = nullptr,
+                                         float unscale = 1.f) {
+    // moments M neq through sums / differences of opposite pairs (rows of lbm_d3q19.h:98-167)
+    const float* n = neq;
+    const float S1 = n[1] + n[2], D1 = n[1] - n[2];
+    const float S2 = n[3] + n[4], D2 = n[3] - n[4];
+    const float S3 = n[5] + n[6], D3 = n[5] - n[6];
+    const float S4 = n[7] + n[10], D4 = n[7] - n[10];
+    const float S5 = n[8] + n[9], D5 = n[8] - n[9];
+    const float S6 = n[11] + n[14], D6 = n[11] - n[14];
+    const float S7 = n[12] + n[13], D7 = n[12] - n[13];
+    const float S8 = n[15] + n[18], D8 = n[15] - n[18];
+    const float S9 = n[16] + n[17], D9 = n[16] - n[17];
+    const float Sa = S1 + S2 + S3;
+    const float Sxy = S4 + S5, Sxz = S6 + S7, Syz = S8 + S9;
+    const float Sd = Sxy + Sxz + Syz;
+    const float X1 = D4 - D5, X2 = D6 - D7, Y1 = D4 + D5, Y2 = D8 - D9, Z1 = D6 + D7, Z2 = D8 + D9;
+    const float ir = unscale / rho;
+    // mass and momentum of f - feq vanish (the collision conserves them): exact zero inputs,
+    // not rounding noise that an input normalisation would amplify
+    x[0] = 0.f;
+    x[3] = 0.f;
+    x[5] = 0.f;
+    x[7] = 0.f;
+    x[1] = (-30.f * n[0] - 11.f * Sa + 8.f * Sd) * ir;
+    x[2] = (12.f * n[0] - 4.f * Sa + Sd) * ir;
+    x[4] = (-4.f * D1 + X1 + X2) * ir;
+    x[6] = (-4.f * D2 + Y1 + Y2) * ir;
+    x[8] = (-4.f * D3 + Z1 + Z2) * ir;
+    x[9] = (2.f * S1 - S2 - S3 + Sxy + Sxz - 2.f * Syz) * ir;
+    x[10] = (-4.f * S1 + 2.f * (S2 + S3) + Sxy + Sxz - 2.f * Syz) * ir;
+    x[11] = (S2 - S3 + Sxy - Sxz) * ir;
+    x[12] = (-2.f * S2 + 2.f * S3 + Sxy - Sxz) * ir;
+    x[13] = (S4 - S5) * ir;
+    x[14] = (S8 - S9) * ir;
+    x[15] = (S6 - S7) * ir;
+    x[16] = (X1 - X2) * ir;
+    x[17] = (-Y1 + Y2) * ir;
+    x[18] = (Z1 - Z2) * ir;
+    // non-equilibrium stress xx yy zz xy xz yz
+    const float p[6] = {unscale * (S1 + S4 + S5 + S6 + S7), unscale * (S2 + S4 + S5 + S8 + S9),
+                        unscale * (S3 + S6 + S7 + S8 + S9), unscale * (S4 - S5), unscale * (S6 - S7),
+                        unscale * (S8 - S9)};
+    const float k = -1.5f / (rho * tau0);
     float s[6];
 #pragma unroll
     for (int i = 0; i < 6; ++i) s[i] = k * p[i];

@@ -101,7 +101,8 @@ class HitConfig:
     batch: int = 128 * 148 * 2
     lr: float = 2e-3           # cosine-decayed to lr / 20
     closure_every: int = 8     # the amortised variant evaluates the network on every k-th step
-    sweep_cs: tuple = ()       # extra Smagorinsky runs with these constants (sensitivity of the error)
+    calibrate_alpha: tuple = (0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 1.0)  # network output scales tried
+    calibrate_cs: tuple = (0.06, 0.07, 0.08, 0.09, 0.1, 0.12)   # Smagorinsky constants tried
     storage: int = zl.STORAGE_F32
     fine_storage: int = zl.STORAGE_F32
     cs: float = 0.1
@@ -223,15 +224,17 @@ def _time_steps(ctx, steps: int) -> float:
     return a.elapsed_time(b)
 
 
-def closure_cost(net, n: int, tau: float, every: int, steps: int = 100, cs: float = 0.1, seed: int = 1) -> dict:
-    """MLUPS of the coarse step on an n^3 HIT box with Smagorinsky, with the network on every step,
-    and with the network on every `every`-th step (kernel time, CUDA events, after warm-up)."""
+def closure_cost(net, n: int, tau: float, intervals=(1, 8, 16), steps: int = 96, cs: float = 0.1,
+                 seed: int = 1) -> dict:
+    """MLUPS of the coarse step on an n^3 HIT box with Smagorinsky and with the network evaluated on
+    every k-th step for each k in `intervals` (kernel time, CUDA events, after warm-up)."""
     import torch
     u = hit_velocity(n, seed=seed)
     rho = torch.ones(n ** 3, dtype=torch.float32, device="cuda")
     out = {"grid": n, "steps": steps}
-    for name, les, k in (("smagorinsky", zl.LES_SMAGORINSKY, 1), ("learned", zl.LES_LEARNED, 1),
-                         (f"learned_every{every}", zl.LES_LEARNED, every)):
+    variants = [("smagorinsky", zl.LES_SMAGORINSKY, 1)]
+    variants += [("learned" if k == 1 else f"learned_every{k}", zl.LES_LEARNED, k) for k in intervals]
+    for name, les, k in variants:
         ctx = box_context(n, tau, les=les, cs=cs)
         if les == zl.LES_LEARNED:
             ctx.set_closure(net)
@@ -241,7 +244,7 @@ def closure_cost(net, n: int, tau: float, every: int, steps: int = 100, cs: floa
         ms = _time_steps(ctx, steps)
         out[name] = float(n) ** 3 * steps / (ms / 1e3) / 1e6
         ctx.close()
-    for name in ("learned", f"learned_every{every}"):
+    for name, _, _ in variants[1:]:
         out[f"{name}_cost_fraction"] = 1.0 - out[name] / out["smagorinsky"]
     return out
 
@@ -256,18 +259,22 @@ def run(cfg: HitConfig, log=print) -> HitResult:
     return res
 
 
-def _run(cfg: HitConfig, log=print) -> HitResult:
-    import torch
-    res = HitResult(config={**cfg.__dict__, "coarse": cfg.coarse, "tau_fine": cfg.tau_fine,
-                            "tau_coarse": cfg.tau_coarse})
-    nf, nc, fac = cfg.fine, cfg.coarse, cfg.factor
-    every = max(1, cfg.coarse_steps // cfg.checkpoints)
-    ck_times = [every * i for i in range(cfg.checkpoints + 1)]
-    snap_times = [int(cfg.coarse_steps / 2 * (i + 1) / cfg.train_snapshots) for i in range(cfg.train_snapshots)]
-    k_max = nc // 2 - 1
+@dataclass
+class FineReference:
+    spectra: dict            # coarse step -> filtered fine spectrum
+    rho0: object             # filtered initial density / velocity (coarse grid)
+    u0: object
+    pairs: tuple = ()        # (x, y) device tensors of the training snapshots
+    mlups: float = 0.0
+    seconds: float = 0.0
 
-    # ---- fine run: filtered spectra at the checkpoints, training pairs at the snapshots
-    u0 = hit_velocity(nf, cfg.k0, cfg.u_rms, cfg.seed)
+
+def fine_reference(cfg: HitConfig, seed: int, ck_times, snap_times=(), log=print) -> FineReference:
+    """Fine run of one realization: filtered spectra at ck_times (coarse steps) and training pairs
+    at snap_times."""
+    import torch
+    nf, nc, fac = cfg.fine, cfg.coarse, cfg.factor
+    u0 = hit_velocity(nf, cfg.k0, cfg.u_rms, seed)
     torch.cuda.empty_cache()  # the FFT work space goes back before the populations are allocated
     fine = box_context(nf, cfg.tau_fine, storage=cfg.fine_storage)
     rho0 = torch.ones(nf ** 3, dtype=torch.float32, device="cuda")
@@ -277,20 +284,18 @@ def _run(cfg: HitConfig, log=print) -> HitResult:
     torch.cuda.empty_cache()
     filt = torch.empty((nc ** 3, 29), dtype=torch.float32, device="cuda")
     u_bar0, rho_bar0 = _filtered_velocity(fine, cfg, filt)
-    u_bar0, rho_bar0 = u_bar0.clone(), rho_bar0.clone()
+    ref = FineReference(spectra={}, rho0=rho_bar0.clone(), u0=u_bar0.clone())
     xs, ys = [], []
     scratch = torch.empty((nc ** 3, 3), dtype=torch.float32, device="cuda")
-    ref_spectra = {}
-    t_fine = time.perf_counter()
-    fine_ms = 0.0
-    t = 0
+    t0 = time.perf_counter()
+    ms, t = 0.0, 0
     for target in sorted(set(ck_times) | set(snap_times)):
         if target > t:
-            fine_ms += _time_steps(fine, (target - t) * fac)
+            ms += _time_steps(fine, (target - t) * fac)
             t = target
         u_bar, _ = _filtered_velocity(fine, cfg, filt)
         if t in ck_times:
-            ref_spectra[t] = energy_spectrum(u_bar, nc)
+            ref.spectra[t] = energy_spectrum(u_bar, nc)
         if t in snap_times:
             x = torch.empty((nc ** 3, 24), dtype=torch.float32, device="cuda")
             y = torch.empty(nc ** 3, dtype=torch.float32, device="cuda")
@@ -299,71 +304,124 @@ def _run(cfg: HitConfig, log=print) -> HitResult:
             torch.cuda.synchronize()
             xs.append(x)
             ys.append(y)
-        log(f"fine step {t * fac}: filtered E(1..4) = {ref_spectra.get(t, [0] * 5)[1:5]}")
+        log(f"seed {seed}, fine step {t * fac}")
     fine.close()
     del fine
     torch.cuda.empty_cache()
-    fine_updates = float(nf) ** 3 * t * fac
-    res.mlups["fine_srt"] = fine_updates / (fine_ms / 1e3) / 1e6
-    res.training["fine_run_seconds"] = time.perf_counter() - t_fine
+    ref.mlups = float(nf) ** 3 * t * fac / (ms / 1e3) / 1e6 if ms > 0 else 0.0
+    ref.seconds = time.perf_counter() - t0
+    if xs:
+        ref.pairs = (torch.cat(xs), torch.cat(ys))
+    return ref
 
-    # ---- training
-    x = torch.cat(xs)
-    y = torch.cat(ys)
-    del xs, ys
+
+def scaled_net(net: "zl.ZlMlp", alpha: float) -> "zl.ZlMlp":
+    """The network with its output scaled by alpha (w3, b3 times alpha): c = alpha * c_network."""
+    v = net.flat().copy()
+    o_w3 = 64 * 24 + 64 + 64 * 64 + 64
+    v[o_w3:o_w3 + 65] *= alpha
+    return zl.ZlMlp.from_flat(v)
+
+
+def coarse_run(cfg: HitConfig, ref: FineReference, ck_times, les: int, cs: float, net=None, every: int = 1,
+               diagnose: bool = False):
+    """One coarse LES run from the filtered initial field; spectra and errors against `ref`."""
+    import torch
+    nc = cfg.coarse
+    ctx = box_context(nc, cfg.tau_coarse, storage=cfg.storage, les=les, cs=cs)
+    if les == zl.LES_LEARNED:
+        ctx.set_closure(net)
+        ctx.set_closure_interval(every)
+    ctx.set_equilibrium_dense(0, ref.rho0.data_ptr(), ref.u0.data_ptr())
+    rho_d = torch.empty(nc ** 3, dtype=torch.float32, device="cuda")
+    u_d = torch.empty((nc ** 3, 3), dtype=torch.float32, device="cuda")
+    spectra, errs, errs_low, pred = {}, [], [], []
+    t, ms = 0, 0.0
+    for target in ck_times:
+        if target > t:
+            ms += _time_steps(ctx, target - t)
+            t = target
+        ctx.get_macros_dense(0, rho_d.data_ptr(), u_d.data_ptr())
+        ctx.synchronize()
+        e = energy_spectrum(u_d, nc)
+        spectra[str(t)] = e.tolist()
+        if t > 0:
+            if diagnose and net is not None:
+                pred.append(predicted_y(ctx, net, nc))
+            errs.append(spectrum_error(e, ref.spectra[t], nc // 2 - 1))
+            errs_low.append(spectrum_error(e, ref.spectra[t], nc // 4))
+        if not np.all(np.isfinite(e)):
+            errs.append(float("inf"))
+            errs_low.append(float("inf"))
+            break
+    ctx.close()
+    return {"error": float(np.mean(errs)) if errs else None, "error_k_le_n/4": float(np.mean(errs_low)) if errs_low else None,
+            "per_checkpoint": errs, "spectra": spectra, "mlups": float(nc) ** 3 * t / (ms / 1e3) / 1e6 if ms else None,
+            "predicted_y": pred}
+
+
+def _run(cfg: HitConfig, log=print) -> HitResult:
+    """Training realization (seed): fine run, training pairs, network training, and a one-number
+    calibration of the network output scale (and, for a fair comparison, of the Smagorinsky
+    constant) against its filtered spectra.  Test realization (seed + 1000): a fresh fine run
+    against which Smagorinsky (configured and calibrated constant) and the learned closure
+    (raw and calibrated) are scored."""
+    import torch
+    res = HitResult(config={**cfg.__dict__, "coarse": cfg.coarse, "tau_fine": cfg.tau_fine,
+                            "tau_coarse": cfg.tau_coarse})
+    nc = cfg.coarse
+    every = max(1, cfg.coarse_steps // cfg.checkpoints)
+    ck_times = [every * i for i in range(cfg.checkpoints + 1)]
+    snap_times = [int(cfg.coarse_steps / 2 * (i + 1) / cfg.train_snapshots) for i in range(cfg.train_snapshots)]
+    res.times = ck_times
+
+    train_ref = fine_reference(cfg, cfg.seed, ck_times, snap_times, log)
+    res.mlups["fine_srt"] = train_ref.mlups
+    x, y = train_ref.pairs
+    train_ref.pairs = ()
     net, info = train(x, y, cfg, log)
     res.training.update(info)
     del x, y
     torch.cuda.empty_cache()
 
-    # ---- coarse runs from the filtered initial field
-    res.spectra["filtered_fine"] = {str(k): v.tolist() for k, v in ref_spectra.items()}
-    res.times = ck_times
-    runs = (("smagorinsky", zl.LES_SMAGORINSKY, 1), ("learned", zl.LES_LEARNED, 1),
-            (f"learned_every{cfg.closure_every}", zl.LES_LEARNED, cfg.closure_every))
-    runs = runs + tuple((f"smagorinsky_cs{c:g}", zl.LES_SMAGORINSKY, 1) for c in cfg.sweep_cs)
+    # calibration on the training realization
+    calib = {"alpha": {}, "cs": {}}
+    for a in cfg.calibrate_alpha:
+        r = coarse_run(cfg, train_ref, ck_times, zl.LES_LEARNED, cfg.cs, scaled_net(net, a), cfg.closure_every)
+        calib["alpha"][f"{a:g}"] = r["error"]
+        log(f"calibration: alpha {a:g} -> {r['error']}")
+    for c in cfg.calibrate_cs:
+        r = coarse_run(cfg, train_ref, ck_times, zl.LES_SMAGORINSKY, c)
+        calib["cs"][f"{c:g}"] = r["error"]
+        log(f"calibration: Cs {c:g} -> {r['error']}")
+    finite = lambda d: {k: v for k, v in d.items() if v is not None and np.isfinite(v)}
+    alpha = float(min(finite(calib["alpha"]).items(), key=lambda kv: kv[1])[0]) if finite(calib["alpha"]) else 1.0
+    cs_best = float(min(finite(calib["cs"]).items(), key=lambda kv: kv[1])[0]) if finite(calib["cs"]) else cfg.cs
+    res.training["calibration"] = {**calib, "alpha_best": alpha, "cs_best": cs_best}
+    del train_ref
+    torch.cuda.empty_cache()
+
+    # evaluation on an independent realization
+    test_ref = fine_reference(cfg, cfg.seed + 1000, ck_times, (), log)
+    res.spectra["filtered_fine"] = {str(k): v.tolist() for k, v in test_ref.spectra.items()}
+    net_cal = scaled_net(net, alpha)
+    runs = [("smagorinsky", zl.LES_SMAGORINSKY, cfg.cs, None, 1),
+            (f"smagorinsky_calibrated", zl.LES_SMAGORINSKY, cs_best, None, 1),
+            ("learned", zl.LES_LEARNED, cfg.cs, net, 1),
+            ("learned_calibrated", zl.LES_LEARNED, cfg.cs, net_cal, 1),
+            (f"learned_calibrated_every{cfg.closure_every}", zl.LES_LEARNED, cfg.cs, net_cal, cfg.closure_every)]
     res.training["coarse_predicted_y"] = {}
-    for name, les, every in runs:
-        cs = float(name[len("smagorinsky_cs"):]) if name.startswith("smagorinsky_cs") else cfg.cs
-        ctx = box_context(nc, cfg.tau_coarse, storage=cfg.storage, les=les, cs=cs)
-        if les == zl.LES_LEARNED:
-            ctx.set_closure(net)
-            ctx.set_closure_interval(every)
-        ctx.set_equilibrium_dense(0, rho_bar0.data_ptr(), u_bar0.data_ptr())
-        rho_d = torch.empty(nc ** 3, dtype=torch.float32, device="cuda")
-        u_d = torch.empty((nc ** 3, 3), dtype=torch.float32, device="cuda")
-        spectra, errs, errs_low = {}, [], []
-        t, ms = 0, 0.0
-        for target in ck_times:
-            if target > t:
-                ms += _time_steps(ctx, target - t)
-                t = target
-            ctx.get_macros_dense(0, rho_d.data_ptr(), u_d.data_ptr())
-            ctx.synchronize()
-            if t > 0:
-                res.training["coarse_predicted_y"].setdefault(name, []).append(predicted_y(ctx, net, nc))
-            e = energy_spectrum(u_d, nc)
-            spectra[str(t)] = e.tolist()
-            if t > 0:
-                errs.append(spectrum_error(e, ref_spectra[t], k_max))
-                errs_low.append(spectrum_error(e, ref_spectra[t], nc // 4))
-            if not np.all(np.isfinite(e)):
-                log(f"{name}: non-finite spectrum at coarse step {t}")
-                break
-        res.spectra[name] = spectra
-        res.errors[name] = {"log_spectrum_rms_k1_to_n/2-1": float(np.mean(errs)) if errs else None,
-                            "log_spectrum_rms_k1_to_n/4": float(np.mean(errs_low)) if errs_low else None,
-                            "per_checkpoint": errs}
-        res.mlups[name] = float(nc) ** 3 * t / (ms / 1e3) / 1e6 if ms > 0 else None
-        ctx.close()
-        log(f"{name}: spectrum error {res.errors[name]['log_spectrum_rms_k1_to_n/2-1']}, "
-            f"{res.mlups[name]} MLUPS")
-    for name, _, _ in runs[1:3]:
-        if res.mlups.get("smagorinsky") and res.mlups.get(name):
-            res.mlups[f"{name}_cost_fraction"] = 1.0 - res.mlups[name] / res.mlups["smagorinsky"]
-    res.mlups["cost_256"] = closure_cost(net, max(256, nc), cfg.tau_coarse, cfg.closure_every)
-    log(f"closure cost on {max(256, nc)}^3: {res.mlups['cost_256']}")
+    for name, les, cs, n_, k in runs:
+        r = coarse_run(cfg, test_ref, ck_times, les, cs, n_, k, diagnose=n_ is not None)
+        res.spectra[name] = r.pop("spectra")
+        res.training["coarse_predicted_y"][name] = r.pop("predicted_y")
+        res.mlups[name] = r.pop("mlups")
+        res.errors[name] = r
+        log(f"{name}: spectrum error {r['error']} (k <= n/4: {r['error_k_le_n/4']}), {res.mlups[name]} MLUPS")
+    res.mlups["cost"] = closure_cost(net_cal, max(256, nc), cfg.tau_coarse, (1, 8, 16, cfg.closure_every))
+    log(f"closure cost on {max(256, nc)}^3: {res.mlups['cost']}")
     res.training["net"] = net.flat().tolist()
+    res.training["alpha"] = alpha
     return res
 
 
@@ -379,7 +437,7 @@ def main(argv=None):
     ap.add_argument("--snapshots", type=int, default=4)
     ap.add_argument("--train-steps", type=int, default=2000)
     ap.add_argument("--every", type=int, default=8)
-    ap.add_argument("--sweep-cs", default="", help="comma-separated Smagorinsky constants to compare")
+
     ap.add_argument("--seed", type=int, default=20261203)
     ap.add_argument("--fine-storage", default="f32")
     ap.add_argument("--out", default=None)
@@ -387,7 +445,7 @@ def main(argv=None):
     cfg = HitConfig(fine=a.fine, factor=a.factor, nu_fine=a.nu, coarse_steps=a.coarse_steps,
                     checkpoints=a.checkpoints, train_snapshots=a.snapshots, train_steps=a.train_steps,
                     closure_every=a.every, seed=a.seed,
-                    sweep_cs=tuple(float(v) for v in a.sweep_cs.split(",") if v),
+
                     fine_storage=zl.STORAGE_NAMES[a.fine_storage])
     res = run(cfg, log=lambda m: print(m, flush=True))
     out = {"config": res.config, "times": res.times, "errors": res.errors, "mlups": res.mlups,
