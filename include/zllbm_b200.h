@@ -163,6 +163,11 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level);
    sub-step of a fine level. */
 int zl_advance(zl_ctx* ctx, int steps);
 
+/* In zl_advance, run consecutive level steps that no transfer separates (e.g. levels 0, 1, 2 at
+   the start of a sub-cycled step) as one launch of the multi-level kernel.  On by default; the
+   results are identical either way (those steps touch disjoint data). */
+int zl_set_batching(zl_ctx* ctx, int enabled);
+
 /* Replay zl_advance as a captured CUDA graph of two background steps (every launch of the
    sub-cycled order, transfers and boundary passes included).  The graph is re-captured after any
    change of levels, interfaces, vertices or tuning.  Off by default. */

@@ -119,3 +119,29 @@ def test_graph_recaptured_after_direct_step():
             ctx.advance(6)
             results.append(ctx.get_populations(0, codes))
     assert np.array_equal(results[0], results[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", AMR)
+def test_batched_levels_match_one_launch_per_level(name):
+    """Consecutive level steps with no transfer between them share one launch (default); turning
+    batching off runs one launch per level step.  FP64 results agree bit for bit."""
+    import zllbm_b200 as zl
+    meta, z = load_amr(name)
+    levels = meta["levels"]
+    out = []
+    for batched in (False, True):
+        with zl.Context(config(meta, zl.STORAGE_F64)) as ctx:
+            for lv in range(levels + 1):
+                ctx.set_level_nodes(lv, z[f"codes{lv}"])
+                ctx.set_populations(lv, z[f"codes{lv}"], z[f"f_before{lv}"])
+            for lv in range(1, levels + 1):
+                excluded = z[f"codes{lv - 1}"][(z[f"flags{lv - 1}"] & 4) != 0]
+                ctx.set_level_interface(lv, z[f"c2f_fine{lv}"], z[f"f2c_coarse{lv - 1}"], excluded)
+            if "ib" in meta:
+                v = z["vertices_before"]
+                ctx.ib_set_vertices(levels, v[:, 0:3], v[:, 3:6], v[:, 6])
+            ctx.set_batching(batched)
+            ctx.advance(meta["steps"] + 1)
+            out.append([ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)])
+    compare(out[1], out[0], "ib" in meta)

@@ -116,6 +116,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_set_level_interface": ([P, ctypes.c_int, u64p, i64, u64p, i64, u64p, i64], ctypes.c_int),
         "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_batching": ([P, ctypes.c_int], ctypes.c_int),
         "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
         "zl_conservation": ([P, ctypes.c_int, dp], ctypes.c_int),
         "zl_synchronize": ([P], ctypes.c_int),
@@ -300,6 +301,9 @@ class Context:
 
     def transfer_levels(self, fine_level: int):
         self._check(self.lib.zl_transfer_levels(self.handle, fine_level))
+
+    def set_batching(self, enabled: bool):
+        self._check(self.lib.zl_set_batching(self.handle, 1 if enabled else 0))
 
     def set_graph(self, enabled: bool):
         self._check(self.lib.zl_set_graph(self.handle, 1 if enabled else 0))

@@ -683,19 +683,15 @@ __device__ __forceinline__ T missing_value(int q, int faces, const T* pre, const
 // One thread per node of the level box.  Odd selects the layout read (see file comment).
 // Bnd: the level has at least one non-periodic axis.  Masked: the box holds absent cells.
 // Ext: extended physics compiled in, kExtForce (Guo forcing) and / or kExtLes (Smagorinsky).
-template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext = 0>
-__global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+// The update of one node c of the level box (collide, stream, stale values / fused bounce back).
+template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext>
+__device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo, const StepParams& p, const Coord& c) {
     constexpr bool Forced = (Ext & kExtForce) != 0;
     constexpr bool Les = (Ext & kExtLes) != 0;
     using Tb = Tables<L>;
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
-    Coord c;
-    c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
-    c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
-    c.x[2] = blockIdx.z;
-    if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
 
     // box coordinates of x-1, x, x+1 along each axis; cell indices fit in 32 bits (checked at set-up)
     int bx[3], row[3][3];
@@ -779,6 +775,52 @@ __global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, Leve
                 St::store_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v);
             }
         }
+    }
+}
+
+template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext = 0>
+__global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    Coord c;
+    c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
+    c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
+    c.x[2] = blockIdx.z;
+    if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
+    aa_node<L, S, Coll, Odd, Bnd, Masked, Ext>(f, geo, p, c);
+}
+
+// ---------------------------------------------------------------- several levels in one launch
+// Levels whose steps follow one another with no transfer between them are independent: one
+// persistent launch sweeps all their nodes.  Node i of the batch belongs to the level whose
+// [first[l], first[l + 1]) range holds it and is the (i - first[l])-th node of that box, x fastest.
+// Every level of a multi-level context keeps its info array, so the masked, bounded variant
+// (correct for any level) is used throughout; the layout phase is per level.
+constexpr int kBatchMax = 8;
+struct LevelBatch {
+    int count;
+    int odd[kBatchMax];
+    long long first[kBatchMax + 1];
+    void* f[kBatchMax];
+    LevelGeom geo[kBatchMax];
+    const StepParams* params[kBatchMax];  // device copies of the levels' parameters
+};
+
+template <class L, class S, int Coll, int Ext>
+__global__ void __launch_bounds__(256, 3) aa_batch_kernel(LevelBatch b) {
+    const long long total = b.first[b.count];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        int l = 0;
+        while (l + 1 < b.count && i >= b.first[l + 1]) ++l;
+        const LevelGeom& geo = b.geo[l];
+        const long long k = i - b.first[l];
+        Coord c;
+        c.x[0] = (int)(k % geo.n[0]);
+        const long long r = k / geo.n[0];
+        c.x[1] = (int)(r % geo.n[1]);
+        c.x[2] = (int)(r / geo.n[1]);
+        S* f = static_cast<S*>(b.f[l]);
+        if (b.odd[l]) aa_node<L, S, Coll, true, true, true, Ext>(f, geo, *b.params[l], c);
+        else aa_node<L, S, Coll, false, true, true, Ext>(f, geo, *b.params[l], c);
     }
 }
 

@@ -80,6 +80,8 @@ struct zl_ctx {
     DeviceBuffer closure_net;   // zl_mlp of the learned LES closure (zl_set_closure)
     DeviceBuffer closure_err;   // int: a tensor-core wait of the closure step gave up
     int closure_every = 1;      // the network runs on every closure_every-th step of a level
+    DeviceBuffer params_dev;    // StepParams of every level on the device (batched steps read them)
+    bool batched = true;        // independent consecutive level steps share one launch (zl_set_batching)
 };
 
 namespace {
@@ -252,6 +254,17 @@ int zl_destroy(zl_ctx* ctx) {
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
+    return ZL_OK;
+}
+
+// Device copy of a level's StepParams (read by the batched multi-level step).
+static int sync_params(zl_ctx* ctx, int level) {
+    if (!ctx->params_dev.ptr) {
+        int rc = alloc(ctx, ctx->params_dev, sizeof(StepParams) * ZL_MAX_LEVELS);
+        if (rc) return rc;
+    }
+    ZL_CUDA(ctx, cudaMemcpy((StepParams*)ctx->params_dev.ptr + level, &ctx->levels[level].params, sizeof(StepParams),
+                            cudaMemcpyHostToDevice));
     return ZL_OK;
 }
 
@@ -472,6 +485,7 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
         L.codes.erase(std::unique(L.codes.begin(), L.codes.end()), L.codes.end());
     }
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if ((rc = sync_params(ctx, level))) return rc;
     L.active = true;
     return ZL_OK;
 }
@@ -555,6 +569,7 @@ int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, do
 }
 
 static int ib_pass(zl_ctx* ctx, Level& L, int level);
+static int level_faces(zl_ctx* ctx, Level& L);
 
 int zl_step_level(zl_ctx* ctx, int level) {
     int rc = check_level(ctx, level, true);
@@ -589,9 +604,15 @@ int zl_step_level(zl_ctx* ctx, int level) {
                                     L.geo, L.params, ctx->stream));
     }
     L.even_layout ^= 1;
-    // domain faces in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
-    // (lbm_grid_interface.cpp:225-314); bounce back is fused into the step kernel unless
-    // the level needs every face as an ordered pass
+    if ((rc = level_faces(ctx, L))) return rc;
+    ++L.steps;
+    return ZL_OK;
+}
+
+// Domain faces after a level's step, in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
+// (lbm_grid_interface.cpp:225-314); bounce back is fused into the step kernel unless the level
+// needs every face as an ordered pass.
+static int level_faces(zl_ctx* ctx, Level& L) {
     for (int k = 0; k < 2 * ctx->dims; ++k) {
         const int face = k < ctx->dims ? 2 * k : 2 * (k - ctx->dims) + 1;
         if (!((L.geo.face_on_box >> face) & 1)) continue;
@@ -608,7 +629,6 @@ int zl_step_level(zl_ctx* ctx, int level) {
             ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
         }
     }
-    ++L.steps;
     return ZL_OK;
 }
 
@@ -639,19 +659,73 @@ static void time_stepping_order(int level, int max_level, std::vector<int>* orde
     }
 }
 
+// Steps of several levels with no transfer between them touch disjoint data: one launch of the
+// batched kernel covers them (immersed-boundary passes before it, face passes after it, each in
+// the levels' order).
+static int step_group(zl_ctx* ctx, const std::vector<int>& group) {
+    if (group.size() == 1) return zl_step_level(ctx, group[0]);
+    LevelBatch b{};
+    b.count = (int)group.size();
+    b.first[0] = 0;
+    int rc;
+    for (size_t i = 0; i < group.size(); ++i) {
+        const int l = group[i];
+        if ((rc = check_level(ctx, l, true))) return rc;
+        Level& L = ctx->levels[l];
+        if (L.n_vertices > 0 && (rc = ib_pass(ctx, L, l))) return rc;
+        b.odd[i] = L.even_layout == 1;
+        b.f[i] = L.f.ptr;
+        b.geo[i] = L.geo;
+        b.params[i] = (const StepParams*)ctx->params_dev.ptr + l;
+        b.first[i + 1] = b.first[i] + (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2];
+    }
+    const int ext = (ctx->cfg.forcing ? kExtForce : 0) | (ctx->cfg.les ? kExtLes : 0);
+    ZL_CUDA(ctx, ctx->ops->batch(ctx->dims, ctx->cfg.collision, ext, b, ctx->stream));
+    for (int l : group) {
+        Level& L = ctx->levels[l];
+        L.even_layout ^= 1;
+        if ((rc = level_faces(ctx, L))) return rc;
+        ++L.steps;
+    }
+    return ZL_OK;
+}
+
+static bool batchable(const zl_ctx* ctx) {
+    if (!ctx->batched || ctx->cfg.max_level == 0 || ctx->cfg.les == ZL_LES_LEARNED) return false;
+    for (int l = 0; l <= ctx->cfg.max_level; ++l)
+        if (!ctx->levels[l].active || !ctx->levels[l].geo.info) return false;
+    return true;
+}
+
 static int advance_direct(zl_ctx* ctx, int steps, const std::vector<int>& order) {
+    const bool batch = batchable(ctx);
+    std::vector<int> group;
+    auto flush = [&]() -> int {
+        if (group.empty()) return ZL_OK;
+        const int rc = step_group(ctx, group);
+        group.clear();
+        return rc;
+    };
     for (int s = 0; s < steps; ++s) {
         int count[ZL_MAX_LEVELS] = {0};
         for (int l : order) {
             ++count[l];
-            int rc = zl_step_level(ctx, l);
-            if (rc) return rc;
+            int rc;
+            if (!batch) {
+                if ((rc = zl_step_level(ctx, l))) return rc;
+            } else {
+                // a level already in the group depends on its own previous step: start a new group
+                if (std::find(group.begin(), group.end(), l) != group.end() && (rc = flush())) return rc;
+                group.push_back(l);
+            }
             // InformationFromGridOfDifferentLevel (lbm_solver_interface.cpp:224-238)
             if (l > 0 && count[l] % 2 == 0) {
-                rc = zl_transfer_levels(ctx, l);
-                if (rc) return rc;
+                if ((rc = flush())) return rc;
+                if ((rc = zl_transfer_levels(ctx, l))) return rc;
             }
         }
+        int rc = flush();
+        if (rc) return rc;
     }
     return ZL_OK;
 }
@@ -701,6 +775,13 @@ int zl_advance(zl_ctx* ctx, int steps) {
         for (int l : order) ctx->levels[l].steps += 2;
     }
     if (steps % 2) return advance_direct(ctx, 1, order);
+    return ZL_OK;
+}
+
+int zl_set_batching(zl_ctx* ctx, int enabled) {
+    if (!ctx) return ZL_EINVAL;
+    ctx->batched = enabled != 0;
+    ++ctx->generation;
     return ZL_OK;
 }
 
@@ -908,6 +989,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
         if ((rc = alloc(ctx, F.macro, (size_t)cells * 4 * sizeof(double)))) return rc;
         ZL_CUDA(ctx, cudaMemset(F.macro.ptr, 0, (size_t)cells * 4 * sizeof(double)));
         F.params.macro = (double*)F.macro.ptr;
+        if ((rc = sync_params(ctx, level))) return rc;
         or_bits_kernel<<<(F.n_f2c + 127) / 128, 128, 0, ctx->stream>>>((uint32_t*)F.info.ptr,
                                                                         (const int*)F.f2c_fine.ptr, F.n_f2c,
                                                                         kInfoSaveMacro);

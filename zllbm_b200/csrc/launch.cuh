@@ -33,6 +33,8 @@ struct LaunchSet {
     cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const LevelMap& m, const StepParams& p,
                             int even_layout, const IbVertices& v, double* node_force, double* node_vel, int* bad,
                             cudaStream_t s);
+    // ext: kExtForce / kExtLes bits of the levels in the batch
+    cudaError_t (*batch)(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s);
 };
 
 const LaunchSet& launch_set_f64();
@@ -202,13 +204,33 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
                                                              node_vel, bad);                                     \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
+    template <class L, int C>                                                                                    \
+    cudaError_t batch_lc(int ext, const LevelBatch& b, cudaStream_t s) {                                         \
+        const long long total = b.first[b.count];                                                                \
+        if (total <= 0) return cudaSuccess;                                                                      \
+        const long long want = (total + 255) / 256, cap = 148 * 6;                                               \
+        const unsigned blocks = (unsigned)(want < cap ? want : cap);                                             \
+        switch (ext) {                                                                                           \
+            case 0: aa_batch_kernel<L, S, C, 0><<<blocks, 256, 0, s>>>(b); break;                                \
+            case kExtForce: aa_batch_kernel<L, S, C, kExtForce><<<blocks, 256, 0, s>>>(b); break;                \
+            case kExtLes: aa_batch_kernel<L, S, C, kExtLes><<<blocks, 256, 0, s>>>(b); break;                    \
+            default: aa_batch_kernel<L, S, C, kExtForce | kExtLes><<<blocks, 256, 0, s>>>(b); break;             \
+        }                                                                                                        \
+        return cudaGetLastError();                                                                               \
+    }                                                                                                            \
+    cudaError_t batch_any(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s) {                    \
+        if (dims == 2)                                                                                           \
+            return coll == kMrt ? batch_lc<D2Q9, kMrt>(ext, b, s) : batch_lc<D2Q9, kSrt>(ext, b, s);             \
+        return coll == kMrt ? batch_lc<D3Q19, kMrt>(ext, b, s) : batch_lc<D3Q19, kSrt>(ext, b, s);               \
+    }                                                                                                            \
     }                                                                                                            \
     const LaunchSet& NAME() {                                                                                    \
         static const LaunchSet set = {(int)sizeof(S), NAME##_impl::step_any, NAME##_impl::neq_any,                \
                                       NAME##_impl::face_any,                                                     \
                                       NAME##_impl::scatter_any, NAME##_impl::gather_any,                         \
                                       NAME##_impl::conservation_any, NAME##_impl::c2f_any,                       \
-                                      NAME##_impl::f2c_any, NAME##_impl::ib_touch_any};                          \
+                                      NAME##_impl::f2c_any, NAME##_impl::ib_touch_any,                           \
+                                      NAME##_impl::batch_any};                                                   \
         return set;                                                                                              \
     }
 
