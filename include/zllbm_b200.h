@@ -61,6 +61,9 @@ extern "C" {
 #define ZL_BC_BOUNCE_BACK 1
 #define ZL_BC_PERIODIC 2
 #define ZL_BC_NONEQ_EXTRAPOLATION 3
+/* No counterpart in the reference: populations entering across the face are advected out of the
+   inner node, f(x_b) = (f_old(x_b) + U f(x_b - n)) / (1 + U), with U = |bc_velocity[face][axis]| > 0. */
+#define ZL_BC_CONVECTIVE_OUTFLOW 4
 
 /* face slots (EDomainBoundaryDirection, amr_project/grid/grid_enumerates.h) */
 #define ZL_FACE_XMIN 0
@@ -163,6 +166,15 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level);
    sub-step of a fine level. */
 int zl_advance(zl_ctx* ctx, int steps);
 
+/* Time interpolation at coarse/fine interfaces (no counterpart in the reference, whose
+   explosion is spatial only and leaves the fine ghost layers stale during odd fine sub-steps,
+   lbm_solver_interface.cpp:224-238).  zl_interpolate_interface sets the explosion targets of
+   fine_level to 0.5 (their values at the last zl_transfer_levels + the values the coarse
+   level's current state gives); with zl_set_temporal_interpolation(ctx, 1), zl_advance does
+   that before the second fine sub-step of every pair.  Off by default. */
+int zl_set_temporal_interpolation(zl_ctx* ctx, int enabled);
+int zl_interpolate_interface(zl_ctx* ctx, int fine_level);
+
 /* In zl_advance, run consecutive level steps that no transfer separates (e.g. levels 0, 1, 2 at
    the start of a sub-cycled step) as one launch of the multi-level kernel.  On by default; the
    results are identical either way (those steps touch disjoint data). */
@@ -225,6 +237,14 @@ int zl_mrt_matrix(int lattice, double tau, double* out);
    stencil half-width 2, StencilDisTwo :372-384). */
 int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordinates, const double* velocity,
                        const double* area);
+
+/* Delta kernel of a level's immersed boundary: ZL_IB_DELTA_4, the reference's four-point
+   StencilDisTwo (immersed_boundary.cpp:365-384, the default), or ZL_IB_DELTA_3, the three-point
+   kernel of Roma, Peskin and Berger (1999), which the reference does not have.  Set it before
+   zl_ib_set_vertices (the stencil check uses it). */
+#define ZL_IB_DELTA_4 4
+#define ZL_IB_DELTA_3 3
+int zl_ib_set_delta(zl_ctx* ctx, int level, int width);
 
 /* Vertex forces of the last forcing pass (n * 3, may be NULL) and their sum F area / dx^(d-1)
    in FP64 (total[3], may be NULL; WriteTimeHisLagrangianForce, :596-642). */

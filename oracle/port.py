@@ -27,6 +27,7 @@ PORT_SO = os.path.join(REF_DIR, "libzl_port.so")
 REF_RUN = os.path.join(REF_DIR, "zl_ref_run")
 
 BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ = 0, 1, 2, 3
+BC_CONVECTIVE = 4  # not in the reference; restated in zl_port.c
 SRT, MRT = 0, 1
 FACES = ("xmin", "xmax", "ymin", "ymax", "zmin", "zmax")
 

@@ -360,6 +360,17 @@ static void apply_face(const lattice* l, const zlp_level* c, double dt, int face
                     macro(l, c, dt, fi, &rho_i, u_i);
                     zlp_feq(l->dims, rho_i, u_i, feq_i);
                     for (int iq = 0; iq < q; ++iq) fn[iq] = feq_b[iq] + fi[iq] - feq_i[iq];
+                } else if (kind == ZLP_BC_CONVECTIVE) {
+                    /* convective outflow (not in the reference): the populations entering across
+                       the face, f = (f_old + U f_inner) / (1 + U), U = |velocity . n| of the face */
+                    int pi[3] = {x, y, z};
+                    pi[axis] = inner;
+                    const double* fi = f + node_index(c, pi[0], pi[1], pi[2]) * q;
+                    const double u = fabs(uw[axis]);
+                    for (int i = 0; i < l->nface_q; ++i) {
+                        const int d = in_dirs[i];
+                        fn[d] = (fn[d] + u * fi[d]) / (1. + u);
+                    }
                 }
             }
 }

@@ -20,7 +20,8 @@
 extern "C" {
 #endif
 
-enum { ZLP_BC_NONE = 0, ZLP_BC_BOUNCE_BACK = 1, ZLP_BC_PERIODIC = 2, ZLP_BC_NONEQ_EXTRAP = 3 };
+enum { ZLP_BC_NONE = 0, ZLP_BC_BOUNCE_BACK = 1, ZLP_BC_PERIODIC = 2, ZLP_BC_NONEQ_EXTRAP = 3,
+       ZLP_BC_CONVECTIVE = 4 /* no counterpart in the reference, see apply_face */ };
 enum { ZLP_SRT = 0, ZLP_MRT = 1 };
 enum { ZLP_LES_OFF = 0, ZLP_LES_SMAGORINSKY = 1 };
 

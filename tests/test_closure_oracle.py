@@ -113,3 +113,17 @@ def test_bf16_gelu_constants_and_accuracy():
     z = np.linspace(-6, 6, 1001)
     err = np.abs(C.gelu_bf16(z) - C.gelu(z))
     assert err.max() < 0.03 * max(1.0, np.abs(z).max()) and np.median(err) < 5e-3
+
+
+def test_delta_kernels_moment_conditions():
+    """Both immersed-boundary kernels are partitions of unity with zero first moment; the
+    three-point kernel also has sum phi^2 = 1/2 (Roma, Peskin and Berger 1999)."""
+    from oracle import ib
+    for x in np.linspace(0.0, 1.0, 41):
+        for width in (3, 4):
+            nodes, w = ib.stencil(10.0 + x, width)
+            assert w.sum() == pytest.approx(1.0, abs=1e-14)
+            assert ((10.0 + x - nodes) * w).sum() == pytest.approx(0.0, abs=1e-14)
+        nodes, w = ib.stencil(10.0 + x, 3)
+        assert (w ** 2).sum() == pytest.approx(0.5, abs=1e-14)
+    assert ib.delta_three(np.array([1.5, 2.0]))[0] == pytest.approx(0.0, abs=1e-15)

@@ -145,3 +145,71 @@ def test_batched_levels_match_one_launch_per_level(name):
             ctx.advance(meta["steps"] + 1)
             out.append([ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)])
     compare(out[1], out[0], "ib" in meta)
+
+
+def _amr_ctx(meta, z, storage):
+    import zllbm_b200 as zl
+    levels = meta["levels"]
+    ctx = zl.Context(config(meta, storage))
+    for lv in range(levels + 1):
+        ctx.set_level_nodes(lv, z[f"codes{lv}"])
+        ctx.set_populations(lv, z[f"codes{lv}"], z[f"f_before{lv}"])
+    for lv in range(1, levels + 1):
+        excluded = z[f"codes{lv - 1}"][(z[f"flags{lv - 1}"] & 4) != 0]
+        ctx.set_level_interface(lv, z[f"c2f_fine{lv}"], z[f"f2c_coarse{lv - 1}"], excluded)
+    return ctx
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", ["amr2d_l1", "amr3d_l1"])
+def test_interface_interpolation_is_the_mean_of_two_transfers(name):
+    """zl_interpolate_interface writes 0.5 (last transfer + transfer from the coarse state now)
+    into the explosion targets (FP64, bit for bit)."""
+    import zllbm_b200 as zl
+    meta, z = load_amr(name)
+    ghosts = z["c2f_fine1"]
+    seq = lambda ctx: (ctx.step_level(0), ctx.step_level(1), ctx.step_level(1), ctx.transfer_levels(1),
+                       ctx.step_level(0), ctx.step_level(1))
+    with _amr_ctx(meta, z, zl.STORAGE_F64) as a, _amr_ctx(meta, z, zl.STORAGE_F64) as b:
+        a.step_level(0), a.step_level(1), a.step_level(1), a.transfer_levels(1)
+        b.step_level(0), b.step_level(1), b.step_level(1), b.transfer_levels(1)
+        last = a.get_populations(1, ghosts)
+        for ctx in (a, b):
+            ctx.step_level(0)
+            ctx.step_level(1)
+        a.interpolate_interface(1)
+        b.transfer_levels(1)
+        mean = a.get_populations(1, ghosts)
+        now = b.get_populations(1, ghosts)
+    assert np.array_equal(mean, 0.5 * (last + now))
+    assert not np.array_equal(mean, now)
+
+
+@pytest.mark.gpu
+def test_temporal_interpolation_keeps_a_uniform_flow():
+    """With every level at feq(rho0, u0) the explosion values do not change in time, so the
+    interpolated run equals the plain one bit for bit; on the fixture's flow it differs."""
+    import zllbm_b200 as zl
+    meta, z = load_amr("amr2d_l2")
+    levels = meta["levels"]
+    uni = {}
+    for lv in range(levels + 1):
+        f = z[f"f_before{lv}"]
+        uni[lv] = np.tile(f.mean(axis=0), (f.shape[0], 1))
+    res = []
+    for temporal in (False, True):
+        with _amr_ctx(meta, z, zl.STORAGE_F64) as ctx:
+            for lv in range(levels + 1):
+                ctx.set_populations(lv, z[f"codes{lv}"], uni[lv])
+            ctx.set_temporal_interpolation(temporal)
+            ctx.advance(3)
+            res.append([ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)])
+    for a, b in zip(*res):
+        assert np.array_equal(a, b)
+    out = []
+    for temporal in (False, True):
+        with _amr_ctx(meta, z, zl.STORAGE_F64) as ctx:
+            ctx.set_temporal_interpolation(temporal)
+            ctx.advance(2)
+            out.append(ctx.get_populations(levels, z[f"codes{levels}"]))
+    assert not np.array_equal(out[0], out[1])

@@ -19,7 +19,7 @@ HEADER = os.path.join(os.path.dirname(PKG), "include", "zllbm_b200.h")
 
 D2Q9, D3Q19 = 2, 3
 SRT, MRT = 0, 1
-BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION = 0, 1, 2, 3
+BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION, BC_CONVECTIVE_OUTFLOW = 0, 1, 2, 3, 4
 STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORAGE_F64, "f32": STORAGE_F32, "f16": STORAGE_F16, "bf16": STORAGE_BF16}
 ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE",
@@ -117,6 +117,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_batching": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_temporal_interpolation": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_interpolate_interface": ([P, ctypes.c_int], ctypes.c_int),
         "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
         "zl_conservation": ([P, ctypes.c_int, dp], ctypes.c_int),
         "zl_synchronize": ([P], ctypes.c_int),
@@ -131,6 +133,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_moments_noalloc": ([ctypes.c_int, P, i64, P, P], ctypes.c_int),
         "zl_ib_set_vertices": ([P, ctypes.c_int, i64, dp, dp, dp], ctypes.c_int),
         "zl_ib_get_forces": ([P, ctypes.c_int, dp, dp], ctypes.c_int),
+        "zl_ib_set_delta": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "zl_set_level_box": ([P, ctypes.c_int, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)],
                              ctypes.c_int),
         "zl_set_equilibrium_dense": ([P, ctypes.c_int, P, P], ctypes.c_int),
@@ -302,6 +305,12 @@ class Context:
     def transfer_levels(self, fine_level: int):
         self._check(self.lib.zl_transfer_levels(self.handle, fine_level))
 
+    def set_temporal_interpolation(self, enabled: bool):
+        self._check(self.lib.zl_set_temporal_interpolation(self.handle, 1 if enabled else 0))
+
+    def interpolate_interface(self, fine_level: int):
+        self._check(self.lib.zl_interpolate_interface(self.handle, fine_level))
+
     def set_batching(self, enabled: bool):
         self._check(self.lib.zl_set_batching(self.handle, 1 if enabled else 0))
 
@@ -333,6 +342,10 @@ class Context:
         self._check(self.lib.zl_ib_set_vertices(self.handle, level, a.size, _p(c, ctypes.c_double),
                                                 _p(v, ctypes.c_double), _p(a, ctypes.c_double)))
         self._nv = {**getattr(self, "_nv", {}), level: a.size}
+
+    def ib_set_delta(self, level: int, width: int):
+        """Stencil width of the delta kernel: 4 (reference) or 3 (Roma, Peskin and Berger)."""
+        self._check(self.lib.zl_ib_set_delta(self.handle, level, width))
 
     def ib_get_forces(self, level: int):
         n = self._nv[level]

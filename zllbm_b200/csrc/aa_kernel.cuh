@@ -26,7 +26,7 @@
 
 namespace zl {
 
-enum BcKind : int { kBcNone = 0, kBcBounceBack = 1, kBcPeriodic = 2, kBcNeq = 3 };
+enum BcKind : int { kBcNone = 0, kBcBounceBack = 1, kBcPeriodic = 2, kBcNeq = 3, kBcConvective = 4 };
 enum Collision : int { kSrt = 0, kMrt = 1 };
 
 // Per-cell information for levels whose node set does not fill its box.
@@ -73,6 +73,7 @@ struct StepParams {
     int les;
     double les_c;           // 18 Cs^2
     const float* c_node;    // learned closure: per-cell constant c (C = 18 c), or nullptr
+    double conv_u[6];       // convective outflow: convection speed per face
 };
 
 // Per-node extras handed to the collision.

@@ -56,6 +56,9 @@ struct Level {
     DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
     DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
     int n_vertices = 0;
+    int ib_width = 4;        // immersed-boundary stencil: 4 (reference) or 3 (Roma et al.)
+    DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q doubles)
+    bool c2f_last_valid = false;
     DeviceBuffer c_node;     // learned closure: c of the last network evaluation per cell
 };
 
@@ -82,6 +85,7 @@ struct zl_ctx {
     int closure_every = 1;      // the network runs on every closure_every-th step of a level
     DeviceBuffer params_dev;    // StepParams of every level on the device (batched steps read them)
     bool batched = true;        // independent consecutive level steps share one launch (zl_set_batching)
+    bool temporal = false;      // time interpolation at the coarse/fine interfaces (zl_set_temporal_interpolation)
 };
 
 namespace {
@@ -207,12 +211,15 @@ int zl_create(const zl_config* config, zl_ctx** out) {
     if (!(config->viscosity > 0.)) return ZL_EINVAL;
     if (config->les < ZL_LES_OFF || config->les > ZL_LES_LEARNED) return ZL_EINVAL;
     for (int f = 0; f < 6; ++f)
-        if (config->bc_kind[f] < ZL_BC_NONE || config->bc_kind[f] > ZL_BC_NONEQ_EXTRAPOLATION) return ZL_EINVAL;
+        if (config->bc_kind[f] < ZL_BC_NONE || config->bc_kind[f] > ZL_BC_CONVECTIVE_OUTFLOW) return ZL_EINVAL;
     const int dims = config->lattice == ZL_D2Q9 ? 2 : 3;
     for (int a = 0; a < dims; ++a) {
         if (config->domain_max[a] <= config->domain_min[a]) return ZL_EINVAL;
         const bool pmin = config->bc_kind[2 * a] == ZL_BC_PERIODIC, pmax = config->bc_kind[2 * a + 1] == ZL_BC_PERIODIC;
         if (pmin != pmax) return ZL_EINVAL;  // periodic faces come in pairs
+        for (int f = 2 * a; f < 2 * a + 2; ++f)
+            if (config->bc_kind[f] == ZL_BC_CONVECTIVE_OUTFLOW && !(std::fabs(config->bc_velocity[f][a]) > 0.))
+                return ZL_EINVAL;  // a convective outflow needs its convection speed
     }
     if (cudaSetDevice(config->device) != cudaSuccess) return ZL_EDEVICE;
     zl_ctx* ctx = new zl_ctx();
@@ -339,12 +346,15 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
         }
     };
     make_geo(true);
-    bool has_neq = false, wraps = false;
-    for (int f = 0; f < 2 * dims; ++f)
+    bool has_neq = false, has_conv = false, wraps = false;
+    for (int f = 0; f < 2 * dims; ++f) {
         if (ctx->cfg.bc_kind[f] == ZL_BC_NONEQ_EXTRAPOLATION && ((geo.face_on_box >> f) & 1)) has_neq = true;
+        if (ctx->cfg.bc_kind[f] == ZL_BC_CONVECTIVE_OUTFLOW && ((geo.face_on_box >> f) & 1)) has_conv = true;
+    }
     for (int a = 0; a < dims; ++a) wraps = wraps || geo.periodic[a];
     if (has_neq && wraps) make_geo(false);
-    L.ordered = has_neq;
+    // faces that read their inner neighbour run as passes in the face order, after the step
+    L.ordered = has_neq || has_conv;
     const long long cells = (long long)geo.a[0] * geo.a[1] * geo.a[2];
     if (cells >= (1ll << 31) - 64)
         return fail(ctx, ZL_EINVAL, "level %d box of %lld cells exceeds 2^31 (split the level)", level, cells);
@@ -404,7 +414,10 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
         const double cs = ctx->cfg.les_cs > 0. ? ctx->cfg.les_cs : 0.16;
         p.les_c = 18. * cs * cs;
     }
-    for (int f = 0; f < 6; ++f) p.face_kind[f] = ctx->cfg.bc_kind[f];
+    for (int f = 0; f < 6; ++f) {
+        p.face_kind[f] = ctx->cfg.bc_kind[f];
+        p.conv_u[f] = std::fabs(ctx->cfg.bc_velocity[f][f >> 1]);
+    }
     for (int f = 0; f < 2 * dims; ++f) {
         const double* U = ctx->cfg.bc_velocity[f];
         for (int o = 0; o < q; ++o) {
@@ -627,8 +640,31 @@ static int level_faces(zl_ctx* ctx, Level& L) {
             ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
         } else if (L.ordered && kind == ZL_BC_BOUNCE_BACK) {
             ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
+        } else if (kind == ZL_BC_CONVECTIVE_OUTFLOW) {
+            ZL_CUDA(ctx, ctx->ops->face(ctx->dims, kind, L.f.ptr, L.geo, L.params, face, L.even_layout, ctx->stream));
         }
     }
+    return ZL_OK;
+}
+
+static C2FStencil c2f_stencil(const Level& F) {
+    return C2FStencil{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
+                      (const uint8_t*)F.c2f_fine.ptr, (const double*)F.c2f_w.ptr, F.n_c2f};
+}
+
+// Explosion targets of fine_level <- 0.5 (values at the last transfer + values from the coarse
+// level's current state); with save_only, only record the current values as "last".
+static int interpolate_interface(zl_ctx* ctx, int fine_level, bool save_only) {
+    Level& F = ctx->levels[fine_level];
+    Level& C = ctx->levels[fine_level - 1];
+    if (!F.has_transfer) return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface first", fine_level);
+    if (!save_only && !F.c2f_last_valid)
+        return fail(ctx, ZL_ESTATE, "level %d: no transfer yet to interpolate from", fine_level);
+    const C2FStencil st = c2f_stencil(F);
+    ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
+                               C.params, st, F.tau_c2f, save_only ? (double*)F.c2f_last.ptr : nullptr,
+                               save_only ? nullptr : (const double*)F.c2f_last.ptr, save_only ? 0 : 1, ctx->stream));
+    if (save_only) F.c2f_last_valid = true;
     return ZL_OK;
 }
 
@@ -642,7 +678,8 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level) {
     C2FStencil st{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
                   (const uint8_t*)F.c2f_fine.ptr, (const double*)F.c2f_w.ptr, F.n_c2f};
     ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
-                               C.params, st, F.tau_c2f, ctx->stream));
+                               C.params, st, F.tau_c2f, (double*)F.c2f_last.ptr, nullptr, 1, ctx->stream));
+    F.c2f_last_valid = F.c2f_last.ptr != nullptr;
     ZL_CUDA(ctx, ctx->ops->f2c(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
                                C.params, (const int*)F.f2c_coarse.ptr, (const int*)F.f2c_fine.ptr, F.n_f2c,
                                (const double*)F.macro.ptr, F.tau_f2c, ctx->stream));
@@ -711,6 +748,11 @@ static int advance_direct(zl_ctx* ctx, int steps, const std::vector<int>& order)
         for (int l : order) {
             ++count[l];
             int rc;
+            // the second sub-step of a pair starts half a coarse step after the last transfer:
+            // its explosion targets take the average of that transfer and the coarse state now
+            if (ctx->temporal && l > 0 && count[l] % 2 == 0) {
+                if ((rc = flush()) || (rc = interpolate_interface(ctx, l, false))) return rc;
+            }
             if (!batch) {
                 if ((rc = zl_step_level(ctx, l))) return rc;
             } else {
@@ -737,6 +779,14 @@ int zl_advance(zl_ctx* ctx, int steps) {
     for (int l = 1; l <= ctx->cfg.max_level; ++l)
         if (!ctx->levels[l].has_transfer)
             return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface before zl_advance", l);
+    // time interpolation needs the explosion values of a "last transfer": before the first one,
+    // those of the current state (recorded outside any graph capture)
+    if (ctx->temporal)
+        for (int l = 1; l <= ctx->cfg.max_level; ++l)
+            if (!ctx->levels[l].c2f_last_valid) {
+                const int rc = interpolate_interface(ctx, l, true);
+                if (rc) return rc;
+            }
     // a closure evaluated every k-th step repeats with period k, not with the graph's two steps
     const bool periodic_closure = ctx->cfg.les == ZL_LES_LEARNED && ctx->closure_net.ptr && ctx->closure_every > 1;
     if (!ctx->use_graph || steps < 2 || periodic_closure) return advance_direct(ctx, steps, order);
@@ -776,6 +826,20 @@ int zl_advance(zl_ctx* ctx, int steps) {
     }
     if (steps % 2) return advance_direct(ctx, 1, order);
     return ZL_OK;
+}
+
+int zl_set_temporal_interpolation(zl_ctx* ctx, int enabled) {
+    if (!ctx) return ZL_EINVAL;
+    ctx->temporal = enabled != 0;
+    ++ctx->generation;
+    return ZL_OK;
+}
+
+int zl_interpolate_interface(zl_ctx* ctx, int fine_level) {
+    int rc = check_level(ctx, fine_level, true);
+    if (rc) return rc;
+    if (fine_level < 1) return fail(ctx, ZL_EINVAL, "level %d has no coarser level", fine_level);
+    return interpolate_interface(ctx, fine_level, false);
 }
 
 int zl_set_batching(zl_ctx* ctx, int enabled) {
@@ -983,6 +1047,8 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
         return rc;
     F.n_c2f = (int)tgt.size();
     F.n_f2c = (int)f2c_c.size();
+    if ((rc = alloc(ctx, F.c2f_last, (size_t)std::max(F.n_c2f, 1) * ctx->q * sizeof(double)))) return rc;
+    F.c2f_last_valid = false;
     // coalescence sources keep rho, u of their last collision
     if (F.n_f2c > 0) {
         const long long cells = (long long)F.geo.a[0] * F.geo.a[1] * F.geo.a[2];
@@ -1037,6 +1103,7 @@ static IbVertices ib_view(zl_ctx* ctx, Level& L, int level) {
     v.area = (const double*)L.ib_area.ptr;
     v.force = (double*)L.ib_force.ptr;
     v.n = L.n_vertices;
+    v.width = L.ib_width;
     const double dx0 = ctx->cfg.dx > 0. ? ctx->cfg.dx : 1.;
     v.dx = dx0 / (double)(1u << level);
     return v;
@@ -1049,13 +1116,14 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.map, L.params, L.even_layout, v,
                                     (double*)L.force.ptr, (double*)L.ib_vel.ptr, (int*)ctx->scratch_flag.ptr,
                                     ctx->stream));
-    const unsigned blocks = (unsigned)((v.n + 127) / 128);
+    // one warp per vertex, kIbWarps vertices per block
+    const unsigned blocks = (unsigned)((v.n + kIbWarps - 1) / kIbWarps), threads = 32 * kIbWarps;
     if (ctx->dims == 2) {
-        ib_force_kernel<2><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<2><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+        ib_force_kernel<2><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<2><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
     } else {
-        ib_force_kernel<3><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<3><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+        ib_force_kernel<3><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<3><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
     }
     ZL_CUDA(ctx, cudaGetLastError());
     return ZL_OK;
@@ -1099,6 +1167,15 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
             return fail(ctx, ZL_ETOPOLOGY, "level %d: an immersed-boundary stencil node is not on the level", level);
         }
     }
+    return ZL_OK;
+}
+
+int zl_ib_set_delta(zl_ctx* ctx, int level, int width) {
+    int rc = check_level(ctx, level, false);
+    if (rc) return rc;
+    if (width != ZL_IB_DELTA_4 && width != ZL_IB_DELTA_3) return fail(ctx, ZL_EINVAL, "stencil width %d", width);
+    ctx->levels[level].ib_width = width;
+    ++ctx->generation;
     return ZL_OK;
 }
 

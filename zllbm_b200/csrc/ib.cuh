@@ -6,8 +6,14 @@
 //   2. every vertex interpolates the node velocities with the delta kernel and sets its force
 //      F = 2 (U_b - u) (:183-184, :318-320);
 //   3. every vertex spreads F delta area / (dt dx^(d-1)) into the node forces (:187-199, :322-339).
-// Launch 3 accumulates with FP64 atomics, so the order in which vertices add into a node is not
-// fixed; the reference's order is that of an unordered_map.  Sums agree to rounding.
+// Launches 2 and 3 give each vertex a warp: the block's vertex records are staged in shared
+// memory, lanes take the stencil nodes, and the interpolation sums are warp-shuffle reductions;
+// the spread adds into the nodes with FP64 atomics.  Summation orders differ from the reference's
+// (an unordered_map walk and a sequential stencil loop); sums agree to rounding.
+//
+// Stencils: width 4 is the reference's StencilDisTwo (immersed_boundary.cpp:365-384); width 3 is
+// the three-point kernel of Roma, Peskin and Berger (J. Comput. Phys. 153, 1999), which the
+// reference does not have.
 #pragma once
 #include "level_ops.cuh"
 
@@ -20,6 +26,7 @@ struct IbVertices {
     double* force;        // n * 3, vertex force_ (written by launch 2)
     int n;
     double dx;            // grid spacing of the level
+    int width;            // stencil nodes per axis: 4 (reference) or 3 (Roma et al.)
 };
 
 // Stencil of the delta kernel (StencilDisOne / StencilDisTwo, immersed_boundary.cpp:365-384)
@@ -33,13 +40,44 @@ __device__ __forceinline__ double ib_delta_two(double dist) {
     return 0.;
 }
 
-// Reference point of a vertex: level indices and the fractional distances.
-__device__ __forceinline__ void ib_reference(const IbVertices& v, int i, int dims, long long* idx, double* dis) {
-    for (int a = 0; a < dims; ++a) {
-        const double r = v.coord[i * 3 + a] / v.dx;
-        idx[a] = (long long)(uint32_t)(r + 1e-6);
-        dis[a] = r - (double)(uint32_t)(r + 1e-6);
+// Three-point kernel (Roma, Peskin and Berger 1999): (1 + sqrt(1 - 3 r^2)) / 3 for |r| <= 1/2,
+// (5 - 3 |r| - sqrt(1 - 3 (1 - |r|)^2)) / 6 for 1/2 <= |r| <= 3/2, zero beyond.
+__device__ __forceinline__ double ib_delta_three(double dist) {
+    const double a = fabs(dist);
+    if (a <= 0.5) return (1. + sqrt(1. - 3. * a * a)) / 3.;
+    if (a <= 1.5) {
+        const double b = 1. - a;
+        return (5. - 3. * a - sqrt(1. - 3. * b * b)) / 6.;
     }
+    return 0.;
+}
+
+// Reference point of a vertex on axis a: the first stencil node `first` and the value whose
+// distance to stencil node o is computed by ib_dist.  Width 4 keeps the reference's arithmetic
+// (index (uint32)(r + 1e-6), distance |dis - ix - 1| with ix = o - 2); width 3 centres the stencil
+// on the nearest node.
+__device__ __forceinline__ void ib_reference(const IbVertices& v, const double* coord, int dims, long long* first,
+                                             double* dis) {
+    for (int a = 0; a < dims; ++a) {
+        const double r = coord[a] / v.dx;
+        if (v.width == 4) {
+            const long long idx = (long long)(uint32_t)(r + 1e-6);
+            first[a] = idx - 1;
+            dis[a] = r - (double)(uint32_t)(r + 1e-6);
+        } else {
+            const long long j0 = (long long)floor(r + 0.5);
+            first[a] = j0 - 1;
+            dis[a] = r - (double)j0;
+        }
+    }
+}
+
+__device__ __forceinline__ double ib_weight(const IbVertices& v, double dis, int o) {
+    if (v.width == 4) {
+        const int ix = o - 2;
+        return ib_delta_two(fabs(dis - ix - 1));
+    }
+    return ib_delta_three(dis - (double)(o - 1));
 }
 
 // Node cell of level indices, -1 when the node is not on the level.
@@ -56,6 +94,23 @@ __device__ __forceinline__ long long ib_cell(const LevelGeom& geo, const LevelMa
     return cell;
 }
 
+// Stencil node k of a vertex (k over width^dims nodes, x fastest): level indices and weight.
+__device__ __forceinline__ double ib_stencil_node(const IbVertices& v, int dims, const long long* first,
+                                                  const double* dis, int k, long long* nid) {
+    const int w = v.width;
+    const int o[3] = {k % w, (k / w) % w, k / (w * w)};
+    double weight = 1.;
+    for (int a = 0; a < 3; ++a) {
+        if (a < dims) {
+            nid[a] = first[a] + o[a];
+            weight *= ib_weight(v, dis[a], o[a]);
+        } else {
+            nid[a] = 0;
+        }
+    }
+    return weight;
+}
+
 template <class L, class S>
 __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, LevelMap m, StepParams p, int even_layout,
                                 IbVertices v, double* __restrict__ node_force, double* __restrict__ node_vel,
@@ -63,16 +118,14 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, LevelMap
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ, D = L::kDims;
-    constexpr int K = D == 3 ? 64 : 16;
+    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= v.n * K) return;
     const int i = t / K, k = t % K;
-    long long idx[3], nid[3];
+    long long first[3], nid[3];
     double dis[3];
-    ib_reference(v, i, D, idx, dis);
-    nid[0] = idx[0] + (k & 3) - 1;
-    nid[1] = idx[1] + ((k >> 2) & 3) - 1;
-    nid[2] = D == 3 ? idx[2] + ((k >> 4) & 3) - 1 : 0;
+    ib_reference(v, v.coord + i * 3, D, first, dis);
+    ib_stencil_node(v, D, first, dis, k, nid);
     const long long cell = ib_cell(geo, m, nid, D);
     if (cell < 0) {
         atomicExch(bad, 1);
@@ -119,57 +172,82 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, LevelMap
     }
 }
 
-template <int D>
-__global__ void ib_force_kernel(LevelGeom geo, LevelMap m, IbVertices v, const double* __restrict__ node_vel) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= v.n) return;
-    long long idx[3];
-    double dis[3];
-    ib_reference(v, i, D, idx, dis);
-    double ur = 0., vr = 0., wr = 0.;
-    const int nz = D == 3 ? 4 : 1;
-    for (int iz = -2; iz < -2 + nz; ++iz) {
-        const double dz = D == 3 ? ib_delta_two(fabs(dis[2] - iz - 1)) : 1.;
-        for (int iy = -2; iy < 2; ++iy) {
-            const double dy = ib_delta_two(fabs(dis[1] - iy - 1));
-            for (int ix = -2; ix < 2; ++ix) {
-                const double dx = ib_delta_two(fabs(dis[0] - ix - 1));
-                const long long nid[3] = {idx[0] + ix + 1, idx[1] + iy + 1, D == 3 ? idx[2] + iz + 1 : 0};
-                const long long cell = ib_cell(geo, m, nid, D);
-                const double delta = D == 3 ? dx * dy * dz : dx * dy;
-                ur += node_vel[cell * 3] * delta;
-                vr += node_vel[cell * 3 + 1] * delta;
-                if (D == 3) wr += node_vel[cell * 3 + 2] * delta;
-            }
-        }
+constexpr int kIbWarps = 4;  // vertices (warps) per block of the interpolation and spread kernels
+
+// This block's vertex records (coordinate, velocity, area) in shared memory.
+struct IbStage {
+    double coord[kIbWarps][3];
+    double vel[kIbWarps][3];
+    double area[kIbWarps];
+};
+
+__device__ __forceinline__ void ib_stage(const IbVertices& v, IbStage& s) {
+    const int base = blockIdx.x * kIbWarps;
+    for (int e = threadIdx.x; e < kIbWarps * 7; e += blockDim.x) {
+        const int w = e / 7, f = e % 7, i = base + w;
+        if (i >= v.n) continue;
+        if (f < 3) s.coord[w][f] = v.coord[i * 3 + f];
+        else if (f < 6) s.vel[w][f - 3] = v.vel[i * 3 + f - 3];
+        else s.area[w] = v.area[i];
     }
-    v.force[i * 3] = 2. * (v.vel[i * 3] - ur);
-    v.force[i * 3 + 1] = 2. * (v.vel[i * 3 + 1] - vr);
-    v.force[i * 3 + 2] = D == 3 ? 2. * (v.vel[i * 3 + 2] - wr) : 0.;
+    __syncthreads();
+}
+
+__device__ __forceinline__ double warp_sum_d(double x) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+    return x;
 }
 
 template <int D>
-__global__ void ib_spread_kernel(LevelGeom geo, LevelMap m, StepParams p, IbVertices v,
-                                 double* __restrict__ node_force) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(LevelGeom geo, LevelMap m, IbVertices v,
+                                                                 const double* __restrict__ node_vel) {
+    __shared__ IbStage s;
+    ib_stage(v, s);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kIbWarps + w;
     if (i >= v.n) return;
-    long long idx[3];
+    long long first[3], nid[3];
     double dis[3];
-    ib_reference(v, i, D, idx, dis);
-    const double area = D == 3 ? v.area[i] / p.dt / v.dx / v.dx : v.area[i] / p.dt / v.dx;
-    const int nz = D == 3 ? 4 : 1;
-    for (int iz = -2; iz < -2 + nz; ++iz) {
-        const double dz = D == 3 ? ib_delta_two(fabs(dis[2] - iz - 1)) : 1.;
-        for (int iy = -2; iy < 2; ++iy) {
-            const double dy = ib_delta_two(fabs(dis[1] - iy - 1));
-            for (int ix = -2; ix < 2; ++ix) {
-                const double dx = ib_delta_two(fabs(dis[0] - ix - 1));
-                const long long nid[3] = {idx[0] + ix + 1, idx[1] + iy + 1, D == 3 ? idx[2] + iz + 1 : 0};
-                const long long cell = ib_cell(geo, m, nid, D);
-                const double dt = (D == 3 ? dx * dy * dz : dx * dy) * area;
-                for (int a = 0; a < D; ++a) atomicAdd(node_force + cell * 3 + a, v.force[i * 3 + a] * dt);
-            }
-        }
+    ib_reference(v, s.coord[w], D, first, dis);
+    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    double ur = 0., vr = 0., wr = 0.;
+    for (int k = lane; k < K; k += 32) {
+        const double delta = ib_stencil_node(v, D, first, dis, k, nid);
+        const long long cell = ib_cell(geo, m, nid, D);
+        ur += node_vel[cell * 3] * delta;
+        vr += node_vel[cell * 3 + 1] * delta;
+        if (D == 3) wr += node_vel[cell * 3 + 2] * delta;
+    }
+    ur = warp_sum_d(ur);
+    vr = warp_sum_d(vr);
+    if (D == 3) wr = warp_sum_d(wr);
+    if (lane == 0) {
+        v.force[i * 3] = 2. * (s.vel[w][0] - ur);
+        v.force[i * 3 + 1] = 2. * (s.vel[w][1] - vr);
+        v.force[i * 3 + 2] = D == 3 ? 2. * (s.vel[w][2] - wr) : 0.;
+    }
+}
+
+template <int D>
+__global__ void __launch_bounds__(32 * kIbWarps) ib_spread_kernel(LevelGeom geo, LevelMap m, StepParams p,
+                                                                  IbVertices v, double* __restrict__ node_force) {
+    __shared__ IbStage s;
+    ib_stage(v, s);
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kIbWarps + w;
+    if (i >= v.n) return;
+    long long first[3], nid[3];
+    double dis[3];
+    ib_reference(v, s.coord[w], D, first, dis);
+    const double area = D == 3 ? s.area[w] / p.dt / v.dx / v.dx : s.area[w] / p.dt / v.dx;
+    const double F[3] = {v.force[i * 3], v.force[i * 3 + 1], v.force[i * 3 + 2]};
+    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    for (int k = lane; k < K; k += 32) {
+        const double delta = ib_stencil_node(v, D, first, dis, k, nid);
+        const long long cell = ib_cell(geo, m, nid, D);
+        const double dt = delta * area;
+        for (int a = 0; a < D; ++a) atomicAdd(node_force + cell * 3 + a, F[a] * dt);
     }
 }
 

@@ -13,7 +13,7 @@ struct LaunchSet {
                         const StepParams& p, cudaStream_t s);
     cudaError_t (*neq)(int dims, void* f, const LevelGeom& geo, const StepParams& p, int face, int even_layout,
                        const double* feq_b, cudaStream_t s);
-    // kind: ZL_BC_BOUNCE_BACK or ZL_BC_PERIODIC face pass
+    // kind: ZL_BC_BOUNCE_BACK, ZL_BC_PERIODIC or ZL_BC_CONVECTIVE_OUTFLOW face pass
     cudaError_t (*face)(int dims, int kind, void* f, const LevelGeom& geo, const StepParams& p, int face,
                         int even_layout, cudaStream_t s);
     cudaError_t (*scatter)(int dims, void* f, const LevelGeom& geo, const StepParams& p, const LevelMap& m,
@@ -26,7 +26,7 @@ struct LaunchSet {
                                 int even_layout, double* partial, int nblocks, double* out, cudaStream_t s);
     cudaError_t (*c2f)(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const C2FStencil& st, double tau_ratio,
-                       cudaStream_t s);
+                       double* save, const double* prev, int store, cudaStream_t s);
     cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const int* coarse_cell,
                        const int* fine_cell, int n, const double* fine_macro, double tau_ratio, cudaStream_t s);
@@ -120,9 +120,11 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
         dim3 b(128), g((n0 + 127) / 128, n1);                                                                    \
         if (dims == 2) {                                                                                         \
             if (kind == kBcBounceBack) bb_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);           \
+            else if (kind == kBcConvective) conv_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);    \
             else periodic_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);                           \
         } else {                                                                                                 \
             if (kind == kBcBounceBack) bb_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);          \
+            else if (kind == kBcConvective) conv_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);   \
             else periodic_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);                          \
         }                                                                                                        \
         return cudaGetLastError();                                                                               \
@@ -165,15 +167,16 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
     }                                                                                                            \
     cudaError_t c2f_any(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc,                   \
                         const LevelGeom& cgeo, int c_even, const StepParams& fp, const StepParams& cp,           \
-                        const C2FStencil& st, double tau_ratio, cudaStream_t s) {                                \
+                        const C2FStencil& st, double tau_ratio, double* save, const double* prev, int store,     \
+                        cudaStream_t s) {                                                                        \
         if (st.n_targets <= 0) return cudaSuccess;                                                               \
         const unsigned blocks = (unsigned)((st.n_targets + 127) / 128);                                          \
         if (dims == 2)                                                                                           \
             c2f_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp, cp, \
-                                                       st, tau_ratio);                                           \
+                                                       st, tau_ratio, save, prev, store);                        \
         else                                                                                                     \
             c2f_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp,    \
-                                                        cp, st, tau_ratio);                                      \
+                                                        cp, st, tau_ratio, save, prev, store);                   \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t f2c_any(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc,                   \
@@ -194,7 +197,7 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
                              const StepParams& p, int even, const IbVertices& v, double* node_force,             \
                              double* node_vel, int* bad, cudaStream_t s) {                                       \
         if (v.n <= 0) return cudaSuccess;                                                                        \
-        const int k = dims == 3 ? 64 : 16;                                                                       \
+        const int k = dims == 3 ? v.width * v.width * v.width : v.width * v.width;                               \
         const unsigned blocks = (unsigned)(((long long)v.n * k + 127) / 128);                                    \
         if (dims == 2)                                                                                           \
             ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, m, p, even, v, node_force,         \

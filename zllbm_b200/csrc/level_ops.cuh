@@ -205,6 +205,41 @@ __device__ __forceinline__ FaceNode face_node(const LevelGeom& geo, int face) {
     return r;
 }
 
+// Convective outflow (no counterpart in the reference, which only has bounce back, periodic and
+// non-equilibrium extrapolation faces): every population entering the domain across the face is
+// advected out of the inner node with speed U (a first-order upwind step of df/dt + U df/dn = 0),
+//     f(x_b, q) = (f_old(x_b, q) + U f(x_b - n, q)) / (1 + U),
+// where f_old is the stale value the stream left at x_b and f(x_b - n, q) the inner node's new
+// post-stream value.  The formula is linear, so deviation and scaled storage use it unchanged.
+template <class L, class S>
+__global__ void conv_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    using St = Storage<S>;
+    using Tb = Tables<L>;
+    using T = typename St::T;
+    const FaceNode r = face_node<L>(geo, face);
+    if (!r.ok) return;
+    const int axis = face >> 1;
+    const int out = (face & 1) ? 1 : -1;  // outward normal along the axis
+    Coord ci = r.c;
+    ci.x[axis] -= out;
+    if (geo.info) {
+        const long long inner = (long long)(ci.x[0] + geo.g[0]) +
+                                (long long)geo.a[0] * ((ci.x[1] + geo.g[1]) + (long long)geo.a[1] * (ci.x[2] + geo.g[2]));
+        if (!(__ldg(geo.info + inner) & kInfoPresent)) return;
+    }
+    const T u = (T)p.conv_u[face];
+    const T one = (T)1;
+#pragma unroll
+    for (int q = 1; q < L::kQ; ++q) {
+        const int ca = axis == 0 ? Tb::cx(q) : (axis == 1 ? Tb::cy(q) : Tb::cz(q));
+        if (ca * out >= 0) continue;  // enters across this face iff c . n_out < 0
+        const long long sb = post_stream_slot<L>(geo, r.c, q, even_layout);
+        const T fb = St::load_raw(f + sb);
+        const T fi = St::load_raw(f + post_stream_slot<L>(geo, ci, q, even_layout));
+        St::store_raw(f + sb, (fb + u * fi) / (one + u));
+    }
+}
+
 // Bounce back as its own pass (lbm_bounce_back.cpp:28-91): f(x, q_in) = f*(x, o) - 6 rho0 w_o (c_o.U),
 // o = bb_source(q_in, face).
 // Used when the level's faces must be applied one after another in the reference's order.
@@ -264,8 +299,13 @@ struct C2FStencil {
 // collision_model/lbm_collision_models.cpp:244-251) or the post-stream populations of the
 // coincident fine node when the coarse node is absent or flagged.
 template <class L, class S>
+// save (optional) receives the targets' values (n_targets x Q, FP64); with prev (optional) the
+// targets get 0.5 (prev + value) instead, the time interpolation between the last transfer and
+// the coarse level's current state (no counterpart in the reference, whose explosion is spatial
+// only); store = 0 only saves.
 __global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, const S* __restrict__ fc, LevelGeom cgeo,
-                           int c_even, StepParams fp, StepParams cp, C2FStencil st, double tau_ratio) {
+                           int c_even, StepParams fp, StepParams cp, C2FStencil st, double tau_ratio,
+                           double* __restrict__ save, const double* __restrict__ prev, int store) {
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
@@ -302,6 +342,15 @@ __global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, const
         }
 #pragma unroll
         for (int q = 0; q < Q; ++q) acc[q] = acc[q] + w * g[q];
+    }
+    if (save) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) save[(long long)t * Q + q] = (double)acc[q];
+    }
+    if (!store) return;
+    if (prev) {
+#pragma unroll
+        for (int q = 0; q < Q; ++q) acc[q] = (T)0.5 * ((T)prev[(long long)t * Q + q] + acc[q]);
     }
     const Coord c = cell_coord(fgeo, st.target[t]);
 #pragma unroll
