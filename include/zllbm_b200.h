@@ -185,6 +185,11 @@ int zl_set_batching(zl_ctx* ctx, int enabled);
    change of levels, interfaces, vertices or tuning.  Off by default. */
 int zl_set_graph(zl_ctx* ctx, int enabled);
 
+/* Thread-block shape of a level's step kernel: x (a multiple of 32) by y threads, at most 256;
+   a negative x selects the kernel that updates two nodes per thread with packed FP32 pairs
+   (full periodic D3Q19 boxes in FP32/FP16/BF16 storage, no forcing or LES). */
+int zl_set_block(zl_ctx* ctx, int level, int x, int y);
+
 /* Choose the thread-block shape of a level's step kernel by timing candidate shapes (on a saved
    copy of the populations, which are restored).  chosen[2] (may be NULL) receives {x, y}. */
 int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen);

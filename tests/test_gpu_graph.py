@@ -213,3 +213,31 @@ def test_temporal_interpolation_keeps_a_uniform_flow():
             ctx.advance(2)
             out.append(ctx.get_populations(levels, z[f"codes{levels}"]))
     assert not np.array_equal(out[0], out[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3), (3, 5e-2)])
+@pytest.mark.parametrize("coll", ["tgv3d_mrt", "tgv3d_srt"])
+def test_two_nodes_per_thread_kernel(coll, storage, tol):
+    """The packed-pair kernel against the reference dump (same tolerances as the scalar kernel)
+    and against the scalar kernel (FP32: 1e-6)."""
+    import zllbm_b200 as zl
+    from fixtures import load_lbm, solver_config
+    meta, codes, f0, f1 = load_lbm(coll)
+    out = []
+    for shape in ((128, 1), (-64, 1), (-32, 2)):
+        with zl.Context(solver_config(meta, storage)) as ctx:
+            ctx.set_level_nodes(0, codes)
+            ctx.set_populations(0, codes, f0)
+            ctx.set_block(0, *shape)
+            ctx.advance(meta["steps"])
+            out.append(ctx.get_populations(0, codes))
+    w = np.abs(f1).max()
+    for got in out[1:]:
+        if storage == 1:
+            assert np.abs(got - f1).max() <= tol * w
+            assert np.abs(got - out[0]).max() <= 1e-6 * w
+        else:
+            from test_gpu_parity import velocity
+            ue, ug = velocity(meta, f1), velocity(meta, got)
+            assert np.linalg.norm(ug - ue) / np.linalg.norm(ue) <= tol

@@ -117,6 +117,7 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_batching": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_block": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "zl_set_temporal_interpolation": ([P, ctypes.c_int], ctypes.c_int),
         "zl_interpolate_interface": ([P, ctypes.c_int], ctypes.c_int),
         "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -310,6 +311,10 @@ class Context:
 
     def interpolate_interface(self, fine_level: int):
         self._check(self.lib.zl_interpolate_interface(self.handle, fine_level))
+
+    def set_block(self, level: int, x: int, y: int = 1):
+        """Step-kernel block shape; negative x: two nodes per thread (packed FP32 pairs)."""
+        self._check(self.lib.zl_set_block(self.handle, level, x, y))
 
     def set_batching(self, enabled: bool):
         self._check(self.lib.zl_set_batching(self.handle, 1 if enabled else 0))

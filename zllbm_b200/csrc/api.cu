@@ -855,6 +855,20 @@ int zl_set_graph(zl_ctx* ctx, int enabled) {
     return ZL_OK;
 }
 
+int zl_set_block(zl_ctx* ctx, int level, int x, int y) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    const int ax = std::abs(x);
+    if (ax < 32 || ax % 32 || y < 1 || ax * y > 256) return fail(ctx, ZL_EINVAL, "block shape %d x %d", x, y);
+    if (x < 0 && !pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes))
+        return fail(ctx, ZL_EINVAL, "two nodes per thread needs a full periodic D3Q19 box in reduced storage");
+    L.geo.block[0] = x;
+    L.geo.block[1] = y;
+    ++ctx->generation;
+    return ZL_OK;
+}
+
 int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
@@ -864,7 +878,10 @@ int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
     DeviceBuffer saved;
     if ((rc = alloc(ctx, saved, L.f.bytes))) return rc;
     ZL_CUDA(ctx, cudaMemcpyAsync(saved.ptr, L.f.ptr, L.f.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    const int shapes[][2] = {{256, 1}, {128, 2}, {128, 1}, {64, 4}, {64, 2}, {32, 8}, {32, 4}};
+    // negative x: two nodes per thread (full periodic D3Q19 boxes in reduced storage only)
+    const int shapes[][2] = {{256, 1}, {128, 2}, {128, 1}, {64, 4}, {64, 2}, {32, 8}, {32, 4},
+                             {-128, 1}, {-64, 2}, {-256, 1}, {-64, 1}};
+    const bool pairs = pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes);
     cudaEvent_t t0, t1;
     ZL_CUDA(ctx, cudaEventCreate(&t0));
     ZL_CUDA(ctx, cudaEventCreate(&t1));
@@ -875,7 +892,8 @@ int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
         LevelGeom g = L.geo;
         g.block[0] = shapes[i][0];
         g.block[1] = shapes[i][1];
-        if (g.block[0] > 2 * std::max(32, g.n[0])) continue;
+        if (g.block[0] < 0 && !pairs) continue;
+        if (std::abs(g.block[0]) > 2 * std::max(32, g.n[0])) continue;
         const bool odd0 = L.even_layout == 1;
         for (int warm = 0; warm < 2; ++warm)
             ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd0 != (warm & 1), L.bnd,

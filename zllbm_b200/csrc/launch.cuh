@@ -4,6 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "ib.cuh"
+#include "pair_kernel.cuh"
 
 namespace zl {
 
@@ -44,15 +45,27 @@ const LaunchSet& launch_set_bf16();
 
 // Block shape and grid of the fused step: one thread per node, x fastest.  The shape is the
 // level's autotuned choice (zl_autotune) or a default of up to 256 threads along x.
+// A negative block x selects the two-nodes-per-thread kernel with |x| threads along x.
 inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) {
     int bx = geo.block[0], by = geo.block[1];
+    int nx = geo.n[0];
+    if (bx < 0) {
+        bx = -bx;
+        nx = (nx + 1) / 2;
+    }
     if (bx <= 0 || by <= 0) {
         bx = 256;
-        while (bx > 32 && bx / 2 >= geo.n[0]) bx /= 2;
+        while (bx > 32 && bx / 2 >= nx) bx /= 2;
         by = 1;
     }
     block = dim3(bx, by, 1);
-    grid = dim3((geo.n[0] + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? geo.n[2] : 1);
+    grid = dim3((nx + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? geo.n[2] : 1);
+}
+
+// The two-nodes-per-thread kernel applies to full periodic D3Q19 boxes in deviation storage
+// without forcing or LES.
+inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, int elem_bytes) {
+    return dims == 3 && !bnd && !masked && !p.forced && !p.les && elem_bytes < 8;
 }
 
 #define ZL_DEFINE_LAUNCH_SET(NAME, S)                                                                            \
@@ -69,9 +82,22 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
         return odd ? step_one<L, C, true, true, true, X>(f, geo, p, s)                                           \
                    : step_one<L, C, false, true, true, X>(f, geo, p, s);                                         \
     }                                                                                                            \
+    template <int C>                                                                                             \
+    cudaError_t step_pair(bool odd, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {           \
+        if constexpr (Storage<S>::kDeviation) {                                                                  \
+            dim3 g, b;                                                                                           \
+            step_shape(geo, 3, g, b);                                                                            \
+            if (odd) aa_pair_kernel<S, C, true><<<g, b, 0, s>>>(f, geo, p);                                      \
+            else aa_pair_kernel<S, C, false><<<g, b, 0, s>>>(f, geo, p);                                         \
+            return cudaGetLastError();                                                                           \
+        }                                                                                                        \
+        return cudaErrorInvalidValue;                                                                            \
+    }                                                                                                            \
     template <class L, int C>                                                                                    \
     cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,        \
                         cudaStream_t s) {                                                                        \
+        if (L::kDims == 3 && geo.block[0] < 0 && pair_eligible(3, bnd, masked, p, (int)sizeof(S)))               \
+            return step_pair<C>(odd, f, geo, p, s);                                                              \
         if (p.forced || p.les) {                                                                                 \
             if (!masked) return cudaErrorInvalidValue;                                                           \
             if (p.forced && p.les) return step_ext<L, C, kExtForce | kExtLes>(odd, f, geo, p, s);                \
