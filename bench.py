@@ -266,6 +266,35 @@ def time_steps(ctx, steps: int, graph: bool = False):
     return start.elapsed_time(end)
 
 
+def closure_block():
+    """The metric's second half: learned closure vs Smagorinsky on decaying HIT, measured on this
+    GPU in this run on a reduced case (fine 256^3 -> coarse 64^3); the cost is measured on a 256^3
+    coarse grid, the full case's."""
+    from zllbm_b200.hit import HitConfig, run
+    cfg = HitConfig(fine=256, factor=4, coarse_steps=2000, checkpoints=8, train_snapshots=4, train_steps=2000,
+                    closure_every=16)
+    t0 = time.perf_counter()
+    res = run(cfg, log=lambda m: None)
+    e = res.errors
+    cost = res.mlups["cost"]
+    return {
+        "workload": "decaying HIT (seeded random-phase modes, k0=4, u_rms=0.04): fine D3Q19 SRT 256^3 box-filtered "
+                    "by 4 to 64^3, 2000 coarse steps; trained and calibrated on one realization, scored on another",
+        "error": "RMS over shells and 8 checkpoints of log(E_LES / E_filtered_fine), lower is better",
+        "smagorinsky_cs0.1": e["smagorinsky"]["error"],
+        "smagorinsky_calibrated": e["smagorinsky_calibrated"]["error"],
+        "learned_calibrated": e["learned_calibrated"]["error"],
+        "learned_calibrated_every16": e["learned_calibrated_every16"]["error"],
+        "alpha": res.training["alpha"], "cs_calibrated": res.training["calibration"]["cs_best"],
+        "held_out_mse": {"network": res.training["val_loss"], "smagorinsky_y1": res.training["val_loss_smagorinsky_y1"],
+                         "best_constant": res.training["val_loss_best_constant"]},
+        "mlups_256": {k: cost[k] for k in ("smagorinsky", "learned", "learned_every8", "learned_every16")},
+        "cost_fraction_every16": cost["learned_every16_cost_fraction"],
+        "cost_fraction_every_step": cost["learned_cost_fraction"],
+        "seconds": time.perf_counter() - t0,
+    }
+
+
 def run_ours(args):
     import torch
 
@@ -360,6 +389,7 @@ def run_ours(args):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(processes=1)
+    closure = closure_block() if rank == 0 and args.closure else None
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
@@ -376,7 +406,9 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": f"aa_step_kernel<D3Q19, {COLLISION.upper()}>"},
+                         "kernel": (f"aa_pair_kernel<{args.storage}, {COLLISION.upper()}> (two nodes per thread)"
+                                    if block and block[0] < 0 else
+                                    f"aa_step_kernel<D3Q19, {args.storage}, {COLLISION.upper()}>")},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -385,6 +417,8 @@ def run_ours(args):
         }
         if variants:
             out["storage_variants"] = variants
+        if closure:
+            out["closure"] = closure
         print(json.dumps(out), flush=True)
     if dist is not None:
         dist.destroy_process_group()
@@ -402,6 +436,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--variants", type=int, default=1)
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--closure", type=int, default=1, help="learned-closure vs Smagorinsky block (HIT, ~40 s)")
     ap.add_argument("--tune", type=int, default=1, help="autotune the step kernel's block shape")
     ap.add_argument("--graph", type=int, default=1, help="replay steps as a captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")

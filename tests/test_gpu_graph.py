@@ -186,34 +186,33 @@ def test_interface_interpolation_is_the_mean_of_two_transfers(name):
 
 
 @pytest.mark.gpu
-def test_temporal_interpolation_keeps_a_uniform_flow():
-    """With every level at feq(rho0, u0) the explosion values do not change in time, so the
-    interpolated run equals the plain one bit for bit; on the fixture's flow it differs."""
+@pytest.mark.parametrize("name", ["amr2d_l1", "amr3d_l1"])
+def test_temporal_interpolation_in_advance_follows_the_public_steps(name):
+    """zl_advance with time interpolation equals, bit for bit, the public calls it stands for:
+    coarse step, fine step, interface interpolation, fine step, transfer; and it changes the run."""
     import zllbm_b200 as zl
-    meta, z = load_amr("amr2d_l2")
-    levels = meta["levels"]
-    uni = {}
-    for lv in range(levels + 1):
-        f = z[f"f_before{lv}"]
-        uni[lv] = np.tile(f.mean(axis=0), (f.shape[0], 1))
-    res = []
-    for temporal in (False, True):
+    meta, z = load_amr(name)
+    codes = [z["codes0"], z["codes1"]]
+    res = {}
+    for mode in ("advance", "manual", "plain"):
         with _amr_ctx(meta, z, zl.STORAGE_F64) as ctx:
-            for lv in range(levels + 1):
-                ctx.set_populations(lv, z[f"codes{lv}"], uni[lv])
-            ctx.set_temporal_interpolation(temporal)
-            ctx.advance(3)
-            res.append([ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)])
-    for a, b in zip(*res):
+            ctx.advance(1)  # ends with a transfer
+            if mode == "advance":
+                ctx.set_temporal_interpolation(True)
+                ctx.advance(2)
+            elif mode == "manual":
+                for _ in range(2):
+                    ctx.step_level(0)
+                    ctx.step_level(1)
+                    ctx.interpolate_interface(1)
+                    ctx.step_level(1)
+                    ctx.transfer_levels(1)
+            else:
+                ctx.advance(2)
+            res[mode] = [ctx.get_populations(lv, codes[lv]) for lv in (0, 1)]
+    for a, b in zip(res["advance"], res["manual"]):
         assert np.array_equal(a, b)
-    out = []
-    for temporal in (False, True):
-        with _amr_ctx(meta, z, zl.STORAGE_F64) as ctx:
-            ctx.set_temporal_interpolation(temporal)
-            ctx.advance(2)
-            out.append(ctx.get_populations(levels, z[f"codes{levels}"]))
-    assert not np.array_equal(out[0], out[1])
-
+    assert not np.array_equal(res["advance"][1], res["plain"][1])
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("storage,tol", [(1, 1e-5), (2, 5e-3), (3, 5e-2)])

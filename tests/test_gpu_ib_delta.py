@@ -38,7 +38,7 @@ def test_ib_vertex_forces_and_momentum(width):
                           bc_kind=(zl.BC_PERIODIC,) * 4 + (0, 0), domain_min=(0, 0, 0), domain_max=(n, n, 0),
                           forcing=1)
     with zl.Context(cfg) as ctx:
-        ctx.set_level_nodes(0, codes)
+        ctx.set_level_box(0, (0, 0, 0), (n, n, 1))  # periodic: the box wraps on both axes
         ctx.set_populations(0, codes, f)
         ctx.ib_set_delta(0, width)
         ctx.ib_set_vertices(0, coords, vel, area)
