@@ -276,6 +276,24 @@ int zl_abi_version(void);
    synchronizing. */
 int zl_moments_noalloc(int lattice, const double* f_device, int64_t n, double* out_device, void* stream);
 
+/* ---------------------------------------------------------------- checkpoint node records
+   The file grid_nodes of the reference's checkpoint folder (MpiManager::WriteCheckPointGridNodes,
+   mpi_checkpoint.cpp:272-380; node data GridNodeLbm::CopyANodeToBufferForCheckpoint,
+   lbm_interface.h:57-78), from and into the device state, so that runs restart across the
+   reference and this library.  Layout: uint32 node count, int32 node data size, then per node
+   uint64 code, int32 level, int32 flag, double f[q], double force[dims] (forcing contexts: the
+   node forces of the last forcing pass), ordered by background cell (ascending code >> dims *
+   level), then level, then x-y-z order inside the cell.  The other files of the folder
+   (loadings, interface_nodes) describe the host's grid and stay with the host. */
+
+/* codes[l], flags[l] (the reference's flag_status_, kept by the host) and n[l] list level l's
+   nodes, for every level 0 .. max_level. */
+int zl_write_checkpoint_nodes(zl_ctx* ctx, const char* path, const uint64_t* const* codes,
+                              const int32_t* const* flags, const int64_t* n);
+/* Populations of every record into its level (each level's node set must contain the codes);
+   flags and forces are left to the host (forces are recomputed by the next forcing pass). */
+int zl_read_checkpoint_nodes(zl_ctx* ctx, const char* path);
+
 /* ---------------------------------------------------------------- full-box levels, device I/O
    No counterpart in the reference, whose levels are always hash maps of nodes; these let a
    periodic box of 10^9 nodes be set up and read without host node lists. */

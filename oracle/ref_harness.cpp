@@ -9,6 +9,7 @@
 //   bc=<face>:<bb|per|neq>[:ux,uy[,uz]]  (repeatable; faces xmin xmax ymin ymax zmin zmax)
 //   init=eq|tgv  u0=<TGV amplitude>  rho0=<default density>  vel=ux,uy[,uz] (initial uniform)
 //   out0=<file>  out=<file>  (binary dumps before and after stepping; optional)
+//   ckpt=<prefix>  (after stepping, the reference's checkpoint folder <prefix>_checkpoint<step>)
 //   timing=1 (print wall-clock seconds of the TimeMarching loop)  warmup=W (untimed steps first)
 //
 // Dump format (little endian): int32 dims, int32 q, int64 n, then n records of
@@ -449,6 +450,21 @@ int main(int argc, char* argv[]) {
     if (kv.count("out")) dump(kv["out"], dims, q, grid0);
     if (kv.count("lout")) dump_levels(kv["lout"], dims, q, *amr->ptr_grid_manager_);
     if (ib_geo && kv.count("vout")) dump_vertices(kv["vout"]);
+    if (kv.count("ckpt")) {
+        // the reference's own checkpoint writer (IoManager::WriteCheckPointData,
+        // io_checkpoint.cpp:27-51): folder <ckpt>_checkpoint<steps> with loadings, grid_nodes,
+        // interface_nodes
+        const auto t = static_cast<DefAmrLUint>(warmup + steps);
+        if (dims == 2) {
+            auto& gm = dynamic_cast<amrproject::GridManager2D&>(*amr->ptr_grid_manager_);
+            amr->ptr_io_manager_->WriteCheckPointData(t, kv["ckpt"], gm, gm, *amr->ptr_criterion_manager_,
+                                                      *amr->ptr_mpi_manager_);
+        } else {
+            auto& gm = dynamic_cast<amrproject::GridManager3D&>(*amr->ptr_grid_manager_);
+            amr->ptr_io_manager_->WriteCheckPointData(t, kv["ckpt"], gm, gm, *amr->ptr_criterion_manager_,
+                                                      *amr->ptr_mpi_manager_);
+        }
+    }
     if (kv.count("timing")) {
         const double sec = std::chrono::duration<double>(t1 - t0).count();
         std::printf("{\"nodes\": %zu, \"steps\": %d, \"seconds\": %.6f}\n", grid0.map_grid_node_.size(), steps, sec);

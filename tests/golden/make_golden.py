@@ -130,6 +130,35 @@ def run_amr(name, case, tmp):
     print(name, [len(l["nodes"]) for l in before], "nodes per level")
 
 
+# checkpoints written by the reference's own writer (IoManager::WriteCheckPointData) after a run
+CKPT_CASES = ("amr2d_l1", "amr3d_l1", "force2d_mrt", "force3d_srt")
+
+
+def run_checkpoint(name, case, tmp):
+    """grid_nodes of the reference's checkpoint folder and every level's state at that time."""
+    from oracle.port import load_levels
+    wd = os.path.join(tmp, "ckpt_" + name)
+    os.makedirs(wd, exist_ok=True)
+    args = [REF_RUN, f"dims={case['dims']}", "n=" + ",".join(str(v) for v in case["n"]), f"levels={case['levels']}",
+            f"coll={case['coll']}", f"nu={case['nu']!r}", f"steps={case['steps']}",
+            "lout=" + os.path.join(wd, "l1.bin"), "ckpt=" + os.path.join(wd, "run")] + [f"bc={b}" for b in case["bc"]]
+    for key in ("geo", "ib", "ext", "inner", "cforce"):
+        if key in case:
+            args.append(f"{key}={case[key]}")
+    if "cforce" in case:
+        args.append("forces=1")
+    subprocess.run(args, check=True, cwd=wd, stdout=subprocess.DEVNULL)
+    _, _, after = load_levels(os.path.join(wd, "l1.bin"))
+    raw = np.fromfile(os.path.join(wd, f"run_checkpoint{case['steps']}", "grid_nodes"), np.uint8)
+    out = {"meta": json.dumps(case), "grid_nodes": raw}
+    for lv, a in enumerate(after):
+        out[f"codes{lv}"] = a["nodes"]["code"]
+        out[f"flags{lv}"] = a["nodes"]["flag"]
+        out[f"f{lv}"] = a["nodes"]["f"]
+    np.savez_compressed(os.path.join(HERE, f"ckpt_{name}.npz"), **out)
+    print("checkpoint", name, raw.size, "bytes")
+
+
 def morton_cases(dims: int, rng: np.random.Generator) -> np.ndarray:
     nb = 64 // dims
     edge = []
@@ -163,6 +192,8 @@ def main():
             print(name, before.size, "nodes")
         for name, case in AMR_CASES.items():
             run_amr(name, case, tmp)
+        for name in CKPT_CASES:
+            run_checkpoint(name, AMR_CASES[name], tmp)
         for dims in (2, 3):
             fout = os.path.join(tmp, f"les{dims}.bin")
             subprocess.run([REF_RUN, "mode=les", f"dims={dims}", f"out={fout}"], check=True, cwd=tmp,
@@ -185,4 +216,11 @@ def main():
 
 
 if __name__ == "__main__":
-    main()
+    if sys.argv[1:] == ["checkpoints"]:
+        if not os.path.exists(REF_RUN):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            for name in CKPT_CASES:
+                run_checkpoint(name, AMR_CASES[name], tmp)
+    else:
+        main()

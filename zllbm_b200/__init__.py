@@ -118,6 +118,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_batching": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_block": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "zl_write_checkpoint_nodes": ([P, ctypes.c_char_p, ctypes.POINTER(u64p),
+                                       ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(i64)],
+                                      ctypes.c_int),
+        "zl_read_checkpoint_nodes": ([P, ctypes.c_char_p], ctypes.c_int),
         "zl_set_temporal_interpolation": ([P, ctypes.c_int], ctypes.c_int),
         "zl_interpolate_interface": ([P, ctypes.c_int], ctypes.c_int),
         "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -315,6 +319,20 @@ class Context:
     def set_block(self, level: int, x: int, y: int = 1):
         """Step-kernel block shape; negative x: two nodes per thread (packed FP32 pairs)."""
         self._check(self.lib.zl_set_block(self.handle, level, x, y))
+
+    def write_checkpoint_nodes(self, path: str, codes: list, flags: list):
+        """The reference's grid_nodes checkpoint file from the device state; codes[l], flags[l]
+        per level 0 .. max_level."""
+        levels = len(codes)
+        cs = [_u64(c) for c in codes]
+        fs = [np.ascontiguousarray(np.asarray(f, dtype=np.int32)) for f in flags]
+        cp = (ctypes.POINTER(ctypes.c_uint64) * levels)(*[_p(c, ctypes.c_uint64) for c in cs])
+        fp = (ctypes.POINTER(ctypes.c_int32) * levels)(*[_p(f, ctypes.c_int32) for f in fs])
+        n = (ctypes.c_int64 * levels)(*[c.size for c in cs])
+        self._check(self.lib.zl_write_checkpoint_nodes(self.handle, path.encode(), cp, fp, n))
+
+    def read_checkpoint_nodes(self, path: str):
+        self._check(self.lib.zl_read_checkpoint_nodes(self.handle, path.encode()))
 
     def set_batching(self, enabled: bool):
         self._check(self.lib.zl_set_batching(self.handle, 1 if enabled else 0))

@@ -1402,3 +1402,137 @@ int zl_set_closure(zl_ctx* ctx, const zl_mlp* net) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- checkpoint node records
+// Cell of a code on a level (the code must belong to the level; periodic duplicates wrap).
+static long long cell_of_level_code(const Level& L, int dims, uint64_t code) {
+    uint32_t idx[3];
+    zl::morton_decode(code, dims, idx);
+    long long b[3] = {0, 0, 0};
+    for (int a = 0; a < dims; ++a) {
+        long long v = (long long)idx[a] - L.map.lo[a];
+        if (L.map.periodic[a] && v == L.map.n[a]) v = 0;
+        if (v < 0 || v >= L.map.n[a]) return -1;
+        b[a] = v + L.geo.g[a];
+    }
+    return b[0] + (long long)L.geo.a[0] * (b[1] + (long long)L.geo.a[1] * b[2]);
+}
+
+extern "C" {
+
+int zl_write_checkpoint_nodes(zl_ctx* ctx, const char* path, const uint64_t* const* codes,
+                              const int32_t* const* flags, const int64_t* n) {
+    if (!ctx || !path || !codes || !flags || !n) return ZL_EINVAL;
+    const int dims = ctx->dims, q = ctx->q, levels = ctx->cfg.max_level + 1;
+    const int n_forces = ctx->cfg.forcing ? dims : 0;
+    struct Key {
+        uint64_t cell;
+        int level;
+        long long local, index;
+    };
+    std::vector<Key> keys;
+    std::vector<std::vector<double>> f(levels), force(levels);
+    for (int l = 0; l < levels; ++l) {
+        int rc = check_level(ctx, l, true);
+        if (rc) return rc;
+        if (n[l] < 0 || (n[l] > 0 && (!codes[l] || !flags[l]))) return fail(ctx, ZL_EINVAL, "level %d: bad node list", l);
+        f[l].resize((size_t)n[l] * q);
+        if (n[l] > 0 && (rc = zl_get_populations(ctx, l, codes[l], f[l].data(), n[l]))) return rc;
+        const Level& L = ctx->levels[l];
+        if (n_forces) {
+            // the node forces of the last forcing pass (GridNodeLbm::force_)
+            const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
+            std::vector<double> all((size_t)cells * 3);
+            ZL_CUDA(ctx, cudaMemcpy(all.data(), L.force.ptr, all.size() * sizeof(double), cudaMemcpyDeviceToHost));
+            force[l].resize((size_t)n[l] * n_forces);
+            for (int64_t i = 0; i < n[l]; ++i) {
+                const long long c = cell_of_level_code(L, dims, codes[l][i]);
+                if (c < 0) return fail(ctx, ZL_ETOPOLOGY, "level %d: code not on the level", l);
+                for (int a = 0; a < n_forces; ++a) force[l][(size_t)i * n_forces + a] = all[(size_t)c * 3 + a];
+            }
+        }
+        // background cell (SFBitsetToNLowerLevel), then x-y-z order inside the cell
+        // (SFBitsetHigherLevelInACell, sfbitset_aux.cpp:140-156, :1958-1985)
+        const uint64_t side = 1ull << l;
+        for (int64_t i = 0; i < n[l]; ++i) {
+            uint32_t idx[3];
+            zl::morton_decode(codes[l][i], dims, idx);
+            long long local = 0;
+            for (int a = dims - 1; a >= 0; --a) local = local * (long long)side + (long long)(idx[a] & (side - 1));
+            keys.push_back({codes[l][i] >> (dims * l), l, local, i});
+        }
+    }
+    std::sort(keys.begin(), keys.end(), [](const Key& a, const Key& b) {
+        if (a.cell != b.cell) return a.cell < b.cell;
+        if (a.level != b.level) return a.level < b.level;
+        return a.local < b.local;
+    });
+    const int32_t data_size = 4 + 8 * q + 8 * n_forces;
+    const size_t node_size = 8 + 4 + (size_t)data_size;
+    if (keys.size() > 0xffffffffull) return fail(ctx, ZL_ETOOLARGE, "more than 2^32 nodes");
+    std::vector<char> buf(8 + keys.size() * node_size);
+    const uint32_t total = (uint32_t)keys.size();
+    std::memcpy(buf.data(), &total, 4);
+    std::memcpy(buf.data() + 4, &data_size, 4);
+    char* p = buf.data() + 8;
+    for (const Key& k : keys) {
+        const int32_t lv = k.level;
+        std::memcpy(p, &codes[lv][k.index], 8);
+        std::memcpy(p + 8, &lv, 4);
+        std::memcpy(p + 12, &flags[lv][k.index], 4);
+        std::memcpy(p + 16, &f[lv][(size_t)k.index * q], (size_t)q * 8);
+        if (n_forces) std::memcpy(p + 16 + q * 8, &force[lv][(size_t)k.index * n_forces], (size_t)n_forces * 8);
+        p += node_size;
+    }
+    FILE* fh = std::fopen(path, "wb");
+    if (!fh) return fail(ctx, ZL_EINVAL, "cannot open %s", path);
+    const size_t w = std::fwrite(buf.data(), 1, buf.size(), fh);
+    std::fclose(fh);
+    if (w != buf.size()) return fail(ctx, ZL_EINVAL, "short write to %s", path);
+    return ZL_OK;
+}
+
+int zl_read_checkpoint_nodes(zl_ctx* ctx, const char* path) {
+    if (!ctx || !path) return ZL_EINVAL;
+    const int q = ctx->q, levels = ctx->cfg.max_level + 1;
+    FILE* fh = std::fopen(path, "rb");
+    if (!fh) return fail(ctx, ZL_EINVAL, "cannot open %s", path);
+    uint32_t total = 0;
+    int32_t data_size = 0;
+    if (std::fread(&total, 4, 1, fh) != 1 || std::fread(&data_size, 4, 1, fh) != 1) {
+        std::fclose(fh);
+        return fail(ctx, ZL_EINVAL, "%s: no checkpoint header", path);
+    }
+    const int extra = data_size - 4 - 8 * q;
+    if (extra < 0 || extra % 8) {
+        std::fclose(fh);
+        return fail(ctx, ZL_EINVAL, "%s: node data of %d bytes does not hold %d populations", path, data_size, q);
+    }
+    const size_t node_size = 12 + (size_t)data_size;
+    std::vector<char> buf((size_t)total * node_size);
+    const size_t got = buf.empty() ? 0 : std::fread(buf.data(), node_size, total, fh);
+    std::fclose(fh);
+    if (got != total) return fail(ctx, ZL_EINVAL, "%s: %zu of %u node records", path, got, total);
+    std::vector<std::vector<uint64_t>> codes(levels);
+    std::vector<std::vector<double>> f(levels);
+    for (uint32_t i = 0; i < total; ++i) {
+        const char* p = buf.data() + (size_t)i * node_size;
+        uint64_t code;
+        int32_t lv;
+        std::memcpy(&code, p, 8);
+        std::memcpy(&lv, p + 8, 4);
+        if (lv < 0 || lv >= levels) return fail(ctx, ZL_ETOPOLOGY, "%s: record of level %d", path, lv);
+        codes[lv].push_back(code);
+        const size_t o = f[lv].size();
+        f[lv].resize(o + q);
+        std::memcpy(&f[lv][o], p + 16, (size_t)q * 8);
+    }
+    for (int l = 0; l < levels; ++l) {
+        if (codes[l].empty()) continue;
+        const int rc = zl_set_populations(ctx, l, codes[l].data(), f[l].data(), (int64_t)codes[l].size());
+        if (rc) return rc;
+    }
+    return ZL_OK;
+}
+
+}  // extern "C"
