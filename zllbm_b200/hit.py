@@ -101,8 +101,8 @@ class HitConfig:
     batch: int = 128 * 148 * 2
     lr: float = 2e-3           # cosine-decayed to lr / 20
     closure_every: int = 8     # the amortised variant evaluates the network on every k-th step
-    calibrate_alpha: tuple = (0.3, 0.4, 0.5, 0.6, 0.7, 0.8, 1.0)  # network output scales tried
-    calibrate_cs: tuple = (0.06, 0.07, 0.08, 0.09, 0.1, 0.12)   # Smagorinsky constants tried
+    calibrate_alpha: tuple = (0.2, 0.3, 0.4, 0.5, 0.6, 0.8, 1.0)      # network output scales tried
+    calibrate_cs: tuple = (0.05, 0.06, 0.07, 0.08, 0.09, 0.1, 0.12)   # Smagorinsky constants tried
     storage: int = zl.STORAGE_F32
     fine_storage: int = zl.STORAGE_F32
     cs: float = 0.1
