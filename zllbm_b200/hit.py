@@ -137,6 +137,19 @@ def _filtered_velocity(ctx, cfg: HitConfig, buf):
     return buf[:, 1:4].contiguous(), buf[:, 0].contiguous()
 
 
+def initial_net(seed: int, in_mean=None, in_inv_std=None) -> "zl.ZlMlp":
+    """He-initialised closure network (zero hidden biases, output bias 1 = the Smagorinsky value)
+    with the given input normalisation (identity when omitted)."""
+    rng = np.random.default_rng(seed)
+    w1 = rng.normal(0, math.sqrt(2.0 / 24), (64, 24))
+    w2 = rng.normal(0, math.sqrt(2.0 / 64), (64, 64))
+    w3 = rng.normal(0, 0.1 * math.sqrt(1.0 / 64), 64)
+    mean = np.zeros(24) if in_mean is None else np.asarray(in_mean)
+    inv = np.ones(24) if in_inv_std is None else np.asarray(in_inv_std)
+    flat = np.concatenate([w1.ravel(), np.zeros(64), w2.ravel(), np.zeros(64), w3, [1.0], mean, inv])
+    return zl.ZlMlp.from_flat(flat.astype(np.float32))
+
+
 def train(x, y, cfg: HitConfig, log=print):
     """Train the closure network on device tensors x [n, 24], y [n] with the library's trainer.
     Returns the ZlMlp and a dict of losses (train, held-out, constant Smagorinsky y = 1)."""
@@ -150,13 +163,7 @@ def train(x, y, cfg: HitConfig, log=print):
     mean = x[tr_idx].mean(dim=0)
     std = x[tr_idx].std(dim=0)
     inv = torch.where(std > 0, 1.0 / std.clamp(min=1e-30), torch.ones_like(std))
-    rng = np.random.default_rng(cfg.seed + 2)
-    w1 = rng.normal(0, math.sqrt(2.0 / 24), (64, 24))
-    w2 = rng.normal(0, math.sqrt(2.0 / 64), (64, 64))
-    w3 = rng.normal(0, 0.1 * math.sqrt(1.0 / 64), 64)
-    flat = np.concatenate([w1.ravel(), np.zeros(64), w2.ravel(), np.zeros(64), w3, [1.0],
-                           mean.cpu().numpy(), inv.cpu().numpy()]).astype(np.float32)
-    net = zl.ZlMlp.from_flat(flat)
+    net = initial_net(cfg.seed + 2, mean.cpu().numpy(), inv.cpu().numpy())
     xv, yv = x[val].contiguous(), y[val].contiguous()
     yp = torch.empty_like(yv)
 
