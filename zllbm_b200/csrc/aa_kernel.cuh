@@ -137,7 +137,8 @@ template <> struct Storage<__nv_bfloat16> {
 // reference multiplies by a zero lattice component add +-0 and are skipped: that
 // leaves every sum bit-identical.
 template <class L>
-__device__ __forceinline__ void macro_exact(const double* f, double& rho, double& ux, double& uy, double& uz) {
+__device__ __forceinline__ void macro_exact(const double* f, double& rho, double& ux, double& uy, double& uz,
+                                            const double* F = nullptr, double dt = 0.) {
     using Tb = Tables<L>;
     rho = f[0];
     ux = 0.;
@@ -154,6 +155,12 @@ __device__ __forceinline__ void macro_exact(const double* f, double& rho, double
             if (Tb::cz(q) == 1) uz = uz + f[q];
             if (Tb::cz(q) == -1) uz = uz - f[q];
         }
+    }
+    if (F) {
+        // CalMacroForce{2D,3D}Incompressible (lbm_solver_interface.cpp:556-561, :586-592)
+        ux = ux + 0.5 * F[0] * dt;
+        uy = uy + 0.5 * F[1] * dt;
+        if (L::kDims == 3) uz = uz + 0.5 * F[2] * dt;
     }
     ux = ux / rho;
     uy = uy / rho;
@@ -488,6 +495,111 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
     for (int q = 0; q < 19; ++q) out[q] = fmaf(-omega, n[q], d[q]) - c[q];
 }
 
+// D3Q19 MRT without forcing or LES, in one pass over the deviations d (scaled units).
+//
+// The same update as feq_neq_dev + mrt_d3q19_dev, f* = f - omega neq - sum_k lambda_k m_k M_k,
+// rearranged so that no per-direction neq is formed:
+//   * the relaxed moments of neq are the moments of d minus their equilibrium values, which are
+//     closed forms in (rho, j) for the second-order equilibrium of the reference
+//     (lbm_solver_interface.cpp:374-435): with drho = scale (rho - 1), G = scale rho,
+//     m1 = 19 (Sd - d0 - G u^2), m2 = 9 d0 - 7 Sa - 2 Sd + 5.5 G u^2,
+//     m4 = -(10/3) D1 + (5/3)(X1 + X2) (likewise m6, m8: -2/3 j folded in),
+//     m10 = M10.d + G (3 ux^2 - u^2) / 2, m12 = M12.d + G (uy^2 - uz^2) / 2, m16..18 = M.d;
+//   * f*_q = (1 - omega) d_q + omega feq_q - c_q, with d_q, feq_q and c_q split into the parts
+//     even and odd under q -> opp(q), so each opposite pair is formed from its sum and difference
+//     (the populations themselves are not needed past the pair sums).
+// The odd part of feq uses the momentum sums j directly (3 w G (c.u) = 3 w (c.j)).
+__device__ __forceinline__ void mrt_d3q19_fused(const float* d, float* out, const StepParams& p, float* mac) {
+    const float omega = p.omega32;
+    const float* lam = p.mrt_coef;
+    const float S1 = d[1] + d[2], D1 = d[1] - d[2];
+    const float S2 = d[3] + d[4], D2 = d[3] - d[4];
+    const float S3 = d[5] + d[6], D3 = d[5] - d[6];
+    const float S4 = d[7] + d[10], D4 = d[7] - d[10];
+    const float S5 = d[8] + d[9], D5 = d[8] - d[9];
+    const float S6 = d[11] + d[14], D6 = d[11] - d[14];
+    const float S7 = d[12] + d[13], D7 = d[12] - d[13];
+    const float S8 = d[15] + d[18], D8 = d[15] - d[18];
+    const float S9 = d[16] + d[17], D9 = d[16] - d[17];
+    const float S23 = S2 + S3;
+    const float Sa = S1 + S23;
+    const float Sxy = S4 + S5, Sxz = S6 + S7, Syz = S8 + S9;
+    const float Sd = (Sxy + Sxz) + Syz;
+    const float drho = (d[0] + Sa) + Sd;
+    const float X1 = D4 - D5, X2 = D6 - D7;
+    const float Y1 = D4 + D5, Y2 = D8 - D9;
+    const float Z1 = D6 + D7, Z2 = D8 + D9;
+    const float X12 = X1 + X2, Y12 = Y1 + Y2, Z12 = Z1 + Z2;
+    const float jx = D1 + X12, jy = D2 + Y12, jz = D3 + Z12;
+    const float rho = fmaf(drho, p.inv_scale, 1.f);
+    const float k = p.inv_scale / rho;
+    const float ux = jx * k, uy = jy * k, uz = jz * k;
+    mac[0] = rho;
+    mac[1] = ux;
+    mac[2] = uy;
+    mac[3] = uz;
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    const float usq = ux2 + uy2 + uz2;
+    const float G = p.scale * rho;
+    const float Gu = G * usq;
+    // relaxed moments of neq, times lambda_k = (s_k - omega) / |M_k|^2
+    const float a1 = (19.f * lam[1]) * ((Sd - d[0]) - Gu);
+    const float a2 = lam[2] * fmaf(5.5f, Gu, fmaf(9.f, d[0], fmaf(-7.f, Sa, -2.f * Sd)));
+    const float a4 = lam[4] * fmaf(-10.f / 3.f, D1, (5.f / 3.f) * X12);
+    const float a6 = lam[6] * fmaf(-10.f / 3.f, D2, (5.f / 3.f) * Y12);
+    const float a8 = lam[8] * fmaf(-10.f / 3.f, D3, (5.f / 3.f) * Z12);
+    const float hG = 0.5f * G;
+    const float a10 = lam[10] * fmaf(hG, fmaf(3.f, ux2, -usq), fmaf(-4.f, S1, fmaf(2.f, S23, (Sxy + Sxz) - 2.f * Syz)));
+    const float a12 = lam[12] * fmaf(hG, uy2 - uz2, fmaf(2.f, S3 - S2, Sxy - Sxz));
+    const float a16 = lam[16] * (X1 - X2), a17 = lam[17] * (Y2 - Y1), a18 = lam[18] * (Z1 - Z2);
+    // even parts of the correction per direction class, odd parts per pair
+    const float e_ax = fmaf(-11.f, a1, -4.f * a2);
+    const float e_dg = fmaf(8.f, a1, a2);
+    const float c0 = fmaf(-30.f, a1, 12.f * a2);
+    const float cx = fmaf(-4.f, a10, e_ax);
+    const float cy = e_ax + 2.f * (a10 - a12);
+    const float cz = e_ax + 2.f * (a10 + a12);
+    const float c_xy = e_dg + (a10 + a12), c_xz = e_dg + (a10 - a12), c_yz = fmaf(-2.f, a10, e_dg);
+    const float u1 = a4 + a16, u2 = a6 - a17;   // q7: u1 + u2, q8: u2 - u1
+    const float v1 = a4 - a16, v2 = a8 + a18;   // q11: v1 + v2, q12: v2 - v1
+    const float t1 = a6 + a17, t2 = a8 - a18;   // q15: t1 + t2, q16: t2 - t1
+    // omega feq: w (B + 4.5 G (c.u)^2) even, 3 w (c.j) odd, B = drho - 1.5 G u^2
+    const float B = fmaf(-1.5f, Gu, drho);
+    const float ow0 = omega * (1.f / 3.f), ow1 = omega * (1.f / 18.f), ow2 = omega * (1.f / 36.f);
+    const float K1 = ow1 * (4.5f * G), L1 = ow1 * B;
+    const float K2 = ow2 * (4.5f * G), L2 = ow2 * B, K2x2 = K2 + K2;
+    const float o1 = ow1 * 3.f, o2 = ow2 * 3.f;
+    // (1 - omega) d_q of a pair from its sum and difference: d_q = (S + D) / 2, d_opp = (S - D) / 2
+    const float h = 0.5f * (1.f - omega);
+    out[0] = fmaf(1.f - omega, d[0], fmaf(ow0, B, -c0));
+    auto pair = [&](int q, int o, float S, float D, float A, float Bo) {
+        const float e = fmaf(h, S, A), od = fmaf(h, D, Bo);
+        out[q] = e + od;
+        out[o] = e - od;
+    };
+    pair(1, 2, S1, D1, fmaf(K1, ux2, L1) - cx, fmaf(o1, jx, 4.f * a4));
+    pair(3, 4, S2, D2, fmaf(K1, uy2, L1) - cy, fmaf(o1, jy, 4.f * a6));
+    pair(5, 6, S3, D3, fmaf(K1, uz2, L1) - cz, fmaf(o1, jz, 4.f * a8));
+    {
+        // xy plane: q7 (+1,+1,0) / q10, q8 (-1,+1,0) / q9
+        const float P = fmaf(K2, ux2 + uy2, L2) - c_xy, Q = K2x2 * (ux * uy);
+        pair(7, 10, S4, D4, P + Q, fmaf(o2, jx + jy, -(u1 + u2)));
+        pair(8, 9, S5, D5, P - Q, fmaf(o2, jy - jx, -(u2 - u1)));
+    }
+    {
+        // xz plane: q11 (+1,0,+1) / q14, q12 (-1,0,+1) / q13
+        const float P = fmaf(K2, ux2 + uz2, L2) - c_xz, Q = K2x2 * (ux * uz);
+        pair(11, 14, S6, D6, P + Q, fmaf(o2, jx + jz, -(v1 + v2)));
+        pair(12, 13, S7, D7, P - Q, fmaf(o2, jz - jx, -(v2 - v1)));
+    }
+    {
+        // yz plane: q15 (0,+1,+1) / q18, q16 (0,-1,+1) / q17
+        const float P = fmaf(K2, uy2 + uz2, L2) - c_yz, Q = K2x2 * (uy * uz);
+        pair(15, 18, S8, D8, P + Q, fmaf(o2, jy + jz, -(t1 + t2)));
+        pair(16, 17, S9, D9, P - Q, fmaf(o2, jz - jy, -(t2 - t1)));
+    }
+}
+
 // out_q = sum_k coef_k (M_k . x) M_kq over the moments flagged in `use` (compile-time folded basis).
 template <class L, class Use>
 __device__ __forceinline__ void moment_apply(const float* x, const float* coef, float* out, Use use) {
@@ -528,6 +640,12 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
                                             const NodeForce* nf, float les_c = 0.f) {
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
+    if constexpr (L::kQ == 19 && !Les) {
+        if (coll == kMrt && !nf) {
+            mrt_d3q19_fused(d, out, p, mac);
+            return;
+        }
+    }
     float neq[Q];
     float F[3] = {0.f, 0.f, 0.f};
     if (nf) {
@@ -694,23 +812,18 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
     using T = typename St::T;
     constexpr int Q = L::kQ;
 
-    // box coordinates of x-1, x, x+1 along each axis; cell indices fit in 32 bits (checked at set-up)
-    int bx[3], row[3][3];
-    {
-        int by[3], bz[3];
+    // box coordinates of x-1, x, x+1 along x and of the node's own row; the rows above and below
+    // are formed on the general route only.  Cell indices fit in 32 bits (checked at set-up).
+    int bx[3];
 #pragma unroll
-        for (int d = -1; d <= 1; ++d) {
-            bx[d + 1] = wrap_or_ghost(c.x[0] + d, geo.n[0], geo.g[0], geo.periodic[0]);
-            by[d + 1] = wrap_or_ghost(c.x[1] + d, geo.n[1], geo.g[1], geo.periodic[1]);
-            bz[d + 1] = L::kDims == 3 ? wrap_or_ghost(c.x[2] + d, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
-        }
-#pragma unroll
-        for (int dy = 0; dy < 3; ++dy)
-#pragma unroll
-            for (int dz = 0; dz < 3; ++dz) row[dy][dz] = geo.a[0] * (by[dy] + geo.a[1] * bz[dz]);
-    }
-    auto cell = [&](int dx, int dy, int dz) -> int { return bx[dx + 1] + row[dy + 1][dz + 1]; };
-    const int self = cell(0, 0, 0);
+    for (int d = -1; d <= 1; ++d) bx[d + 1] = wrap_or_ghost(c.x[0] + d, geo.n[0], geo.g[0], geo.periodic[0]);
+    const int row_self = geo.a[0] * ((c.x[1] + geo.g[1]) + geo.a[1] * (L::kDims == 3 ? c.x[2] + geo.g[2] : 0));
+    const int self = bx[1] + row_self;
+    auto cell = [&](int dx, int dy, int dz) -> int {
+        const int by = wrap_or_ghost(c.x[1] + dy, geo.n[1], geo.g[1], geo.periodic[1]);
+        const int bz = L::kDims == 3 ? wrap_or_ghost(c.x[2] + dz, geo.n[2], geo.g[2], geo.periodic[2]) : 0;
+        return bx[dx + 1] + geo.a[0] * (by + geo.a[1] * bz);
+    };
     // population planes: uniform 64-bit bases, per-thread 32-bit cell offsets
     const long long st = geo.stride;
     auto plane = [&](int q) -> S* { return f + q * st; };
@@ -721,71 +834,153 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
         if (!(info & kInfoPresent)) return;
     }
 
+    // The node update, given where population q is read from and where its post-collision value goes.
+    auto body = [&](auto read_slot, auto write_slot) {
+        T pre[Q], post[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) pre[q] = St::load_raw(read_slot(q));
+
+        T mac[4];
+        NodeForce nf;
+        if (Forced) {
+            // GetAllForcesForANode (lbm_solver_interface.cpp:132-144): constant force plus node forces
+#pragma unroll
+            for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
+        }
+        if constexpr (St::kDeviation) {
+            // Smagorinsky constant C: the level's, or 18 c of the learned closure's last evaluation
+            const float les_c = Les ? (p.c_node ? 18.f * __ldg(p.c_node + self) : (float)p.les_c) : 0.f;
+            collide_dev<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr, les_c);
+        } else {
+            collide_exact<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
+        }
+        if (Masked && (info & kInfoSaveMacro)) {
+            double* m = p.macro + (long long)self * 4;
+            m[0] = (double)mac[0];
+            m[1] = (double)mac[1];
+            m[2] = (double)mac[2];
+            m[3] = (double)mac[3];
+        }
+
+#pragma unroll
+        for (int q = 0; q < Q; ++q) St::store_raw(write_slot(q), post[q]);
+        if (Bnd || Masked) {
+            const int faces = Bnd ? (Masked ? (int)((info >> kInfoFaceShift) & 63u) : on_faces(geo, c, L::kDims)) : 0;
+#pragma unroll
+            for (int q = 1; q < Q; ++q) {
+                const bool miss = Masked ? ((info >> q) & 1u) : upstream_missing<L>(geo, c, q);
+                if (!miss) continue;
+                const T v = missing_value<L, T>(q, faces, pre, post, p);
+                if (Odd) {
+                    St::store_raw(plane(q) + self, v);
+                } else {
+                    St::store_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v);
+                }
+            }
+        }
+    };
+
+    // Full boxes with a ghost frame address neighbours through three per-thread pointers (cells
+    // x-1, x, x+1 of the node's row) plus offsets that are uniform across the launch (plane q and
+    // the row step dy a0 + dz a0 a1), unless a periodic y / z row wraps at this node.  Both routes
+    // reach the same slots; the uniform one needs no per-access index arithmetic.  The two routes
+    // are separate copies of the node update so that each is scheduled on its own.  (Fully
+    // periodic boxes take aa_node_periodic for such rows instead.)
+    const bool uniform_rows =
+        Bnd && !Masked && (!geo.periodic[1] || (c.x[1] > 0 && c.x[1] < geo.n[1] - 1)) &&
+        (L::kDims == 2 || !geo.periodic[2] || (c.x[2] > 0 && c.x[2] < geo.n[2] - 1));
+    if (uniform_rows) {
+        S* const px[3] = {f + (bx[0] + row_self), f + (bx[1] + row_self), f + (bx[2] + row_self)};
+        const long long row_y = geo.a[0], row_z = (long long)geo.a[0] * geo.a[1];
+        auto uoff = [&](int q, int dy, int dz) -> long long { return q * st + dy * row_y + dz * row_z; };
+        body(
+            [&](int q) -> S* {
+                if (Odd && q != 0) return px[1 - Tb::cx(q)] + uoff(Tb::opp(q), -Tb::cy(q), -Tb::cz(q));
+                return px[1] + uoff(q, 0, 0);
+            },
+            [&](int q) -> S* {
+                if (Odd && q != 0) return px[1 + Tb::cx(q)] + uoff(q, Tb::cy(q), Tb::cz(q));
+                return px[1] + uoff(Tb::opp(q), 0, 0);
+            });
+    } else {
+        body(
+            [&](int q) -> S* {
+                if (Odd && q != 0) return plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q));
+                return plane(q) + self;
+            },
+            [&](int q) -> S* {
+                if (Odd && q != 0) return plane(q) + cell(Tb::cx(q), Tb::cy(q), Tb::cz(q));
+                return plane(Tb::opp(q)) + self;
+            });
+    }
+}
+
+// The node update on a fully periodic box (no ghost frame) for a node whose rows y +- 1 and
+// z +- 1 need no wrap-around: three per-thread pointers (x - 1, x, x + 1 of the node's row, x
+// wrapped) plus launch-uniform offsets q * stride + dy a0 + dz a0 a1 reach every slot.
+template <class L, class S, int Coll, bool Odd, int Ext>
+__device__ __forceinline__ void aa_node_periodic(S* __restrict__ f, const LevelGeom& geo, const StepParams& p,
+                                                 const Coord& c) {
+    constexpr bool Forced = (Ext & kExtForce) != 0;
+    constexpr bool Les = (Ext & kExtLes) != 0;
+    using Tb = Tables<L>;
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    const int x = c.x[0], n0 = geo.n[0];
+    const int xm = x == 0 ? n0 - 1 : x - 1, xp = x == n0 - 1 ? 0 : x + 1;
+    const int row = geo.a[0] * (c.x[1] + (L::kDims == 3 ? geo.a[1] * c.x[2] : 0));
+    S* const px[3] = {f + (row + xm), f + (row + x), f + (row + xp)};
+    const long long st = geo.stride;
+    const int a0 = geo.a[0], a01 = geo.a[0] * geo.a[1];
+    auto off = [&](int q, int dy, int dz) -> long long { return q * st + (long long)(dy * a0 + dz * a01); };
     T pre[Q], post[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        if (Odd && q != 0) {
-            pre[q] = St::load_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)));
-        } else {
-            pre[q] = St::load_raw(plane(q) + self);
-        }
+        if (Odd && q != 0) pre[q] = St::load_raw(px[1 - Tb::cx(q)] + off(Tb::opp(q), -Tb::cy(q), -Tb::cz(q)));
+        else pre[q] = St::load_raw(px[1] + off(q, 0, 0));
     }
-
     T mac[4];
     NodeForce nf;
     if (Forced) {
-        // GetAllForcesForANode (lbm_solver_interface.cpp:132-144): constant force plus node forces
 #pragma unroll
-        for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
+        for (int a = 0; a < 3; ++a)
+            nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)(row + x) * 3 + a] : 0.);
     }
     if constexpr (St::kDeviation) {
-        // Smagorinsky constant C: the level's, or 18 c of the learned closure's last evaluation
-        const float les_c = Les ? (p.c_node ? 18.f * __ldg(p.c_node + self) : (float)p.les_c) : 0.f;
+        const float les_c = Les ? (p.c_node ? 18.f * __ldg(p.c_node + row + x) : (float)p.les_c) : 0.f;
         collide_dev<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr, les_c);
     } else {
         collide_exact<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     }
-    if (Masked && (info & kInfoSaveMacro)) {
-        double* m = p.macro + (long long)self * 4;
-        m[0] = (double)mac[0];
-        m[1] = (double)mac[1];
-        m[2] = (double)mac[2];
-        m[3] = (double)mac[3];
-    }
-
-    int faces = 0;
-    if (Bnd) faces = Masked ? (int)((info >> kInfoFaceShift) & 63u) : on_faces(geo, c, L::kDims);
-
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
-        if (Odd && q != 0) {
-            St::store_raw(plane(q) + cell(Tb::cx(q), Tb::cy(q), Tb::cz(q)), post[q]);
-        } else {
-            St::store_raw(plane(Tb::opp(q)) + self, post[q]);
-        }
-    }
-    if (Bnd || Masked) {
-#pragma unroll
-        for (int q = 1; q < Q; ++q) {
-            const bool miss = Masked ? ((info >> q) & 1u) : upstream_missing<L>(geo, c, q);
-            if (!miss) continue;
-            const T v = missing_value<L, T>(q, faces, pre, post, p);
-            if (Odd) {
-                St::store_raw(plane(q) + self, v);
-            } else {
-                St::store_raw(plane(Tb::opp(q)) + cell(-Tb::cx(q), -Tb::cy(q), -Tb::cz(q)), v);
-            }
-        }
+        if (Odd && q != 0) St::store_raw(px[1 + Tb::cx(q)] + off(q, Tb::cy(q), Tb::cz(q)), post[q]);
+        else St::store_raw(px[1] + off(Tb::opp(q), 0, 0), post[q]);
     }
 }
 
+// Resident CTAs per SM the register budget is cut for: the plain reduced-precision even step
+// (own slots only) fits 64 registers; the odd step and the variants with more state keep 80.
+template <class S, bool Odd, bool Bnd, bool Masked, int Ext>
+struct StepOccupancy {
+    static constexpr int kMinBlocks = (sizeof(S) < 8 && !Odd && !Bnd && !Masked && Ext == 0) ? 4 : 3;
+};
+
 template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext = 0>
-__global__ void __launch_bounds__(256, 3) aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+__global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>::kMinBlocks))
+    aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
     Coord c;
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
     c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
     c.x[2] = blockIdx.z;
     if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
+    if constexpr (!Bnd && !Masked) {
+        if (c.x[1] > 0 && c.x[1] < geo.n[1] - 1 && (L::kDims == 2 || (c.x[2] > 0 && c.x[2] < geo.n[2] - 1))) {
+            aa_node_periodic<L, S, Coll, Odd, Ext>(f, geo, p, c);
+            return;
+        }
+    }
     aa_node<L, S, Coll, Odd, Bnd, Masked, Ext>(f, geo, p, c);
 }
 

@@ -144,33 +144,7 @@ __global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, 
         }
     } else {
         double rho, ux, uy, uz, feq[Q];
-        if (p.forced) {
-            using Tb = Tables<L>;
-            rho = fi[0];
-            ux = 0.;
-            uy = 0.;
-            uz = 0.;
-#pragma unroll
-            for (int q = 1; q < Q; ++q) {
-                rho = rho + fi[q];
-                if (Tb::cx(q) == 1) ux = ux + fi[q];
-                if (Tb::cx(q) == -1) ux = ux - fi[q];
-                if (Tb::cy(q) == 1) uy = uy + fi[q];
-                if (Tb::cy(q) == -1) uy = uy - fi[q];
-                if (L::kDims == 3) {
-                    if (Tb::cz(q) == 1) uz = uz + fi[q];
-                    if (Tb::cz(q) == -1) uz = uz - fi[q];
-                }
-            }
-            ux = ux + 0.5 * F[0] * p.dt;
-            uy = uy + 0.5 * F[1] * p.dt;
-            if (L::kDims == 3) uz = uz + 0.5 * F[2] * p.dt;
-            ux = ux / rho;
-            uy = uy / rho;
-            if (L::kDims == 3) uz = uz / rho;
-        } else {
-            macro_exact<L>(fi, rho, ux, uy, uz);
-        }
+        macro_exact<L>(fi, rho, ux, uy, uz, p.forced ? F : nullptr, p.dt);
         feq_exact<L>(rho, ux, uy, uz, feq);
 #pragma unroll
         for (int q = 0; q < Q; ++q)
@@ -439,17 +413,29 @@ __global__ void gather_kernel(const S* __restrict__ f, LevelGeom geo, StepParams
     }
     if (rho_out) {
         // velocity recomputed from post-boundary f, as the reference's output does
-        // (lbm_grid_interface.cpp:614-657)
+        // (lbm_grid_interface.cpp:614-657), with the node's forces when the level is forced
+        double F[3] = {0., 0., 0.};
+        if (p.forced) {
+            const long long self = (long long)(c.x[0] + geo.g[0]) +
+                                   (long long)geo.a[0] * ((c.x[1] + geo.g[1]) + (long long)geo.a[1] * (c.x[2] + geo.g[2]));
+            for (int a = 0; a < 3; ++a) F[a] = p.const_force[a] + (p.force ? p.force[self * 3 + a] : 0.);
+        }
         if constexpr (St::kDeviation) {
             float rho, ux, uy, uz;
             macro_dev<L>(v, rho, ux, uy, uz);
+            if (p.forced) {
+                const float h = 0.5f * (float)p.dt / rho;
+                ux += h * (float)F[0];
+                uy += h * (float)F[1];
+                uz += h * (float)F[2];
+            }
             rho_out[i] = rho;
             u_out[i * D] = ux;
             u_out[i * D + 1] = uy;
             if (D == 3) u_out[i * D + 2] = uz;
         } else {
             double rho, ux, uy, uz;
-            macro_exact<L>(v, rho, ux, uy, uz);
+            macro_exact<L>(v, rho, ux, uy, uz, p.forced ? F : nullptr, p.dt);
             rho_out[i] = rho;
             u_out[i * D] = ux;
             u_out[i * D + 1] = uy;
@@ -470,31 +456,34 @@ __global__ void __launch_bounds__(256) conservation_partial_kernel(const S* __re
     constexpr int Q = L::kQ;
     __shared__ double red[4][256 / 32];
     double acc[4] = {0., 0., 0., 0.};
-    const long long total = (long long)geo.n[0] * geo.n[1] * (L::kDims == 3 ? geo.n[2] : 1);
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
+    // blocks stride over the (y, z) rows of the box, threads over x: no per-node division
+    const int rows = geo.n[1] * (L::kDims == 3 ? geo.n[2] : 1);
+    for (int r = blockIdx.x; r < rows; r += gridDim.x) {
         Coord c;
-        c.x[0] = (int)(i % geo.n[0]);
-        c.x[1] = (int)((i / geo.n[0]) % geo.n[1]);
-        c.x[2] = L::kDims == 3 ? (int)(i / ((long long)geo.n[0] * geo.n[1])) : 0;
-        if (geo.info) {
-            const long long self = (long long)(c.x[0] + geo.g[0]) +
-                                   (long long)geo.a[0] * ((c.x[1] + geo.g[1]) + (long long)geo.a[1] * (c.x[2] + geo.g[2]));
-            if (!(__ldg(geo.info + self) & kInfoPresent)) continue;
+        c.x[1] = r % geo.n[1];
+        c.x[2] = L::kDims == 3 ? r / geo.n[1] : 0;
+        for (int x = threadIdx.x; x < geo.n[0]; x += blockDim.x) {
+            c.x[0] = x;
+            if (geo.info) {
+                const long long self = (long long)(c.x[0] + geo.g[0]) +
+                                       (long long)geo.a[0] * ((c.x[1] + geo.g[1]) + (long long)geo.a[1] * (c.x[2] + geo.g[2]));
+                if (!(__ldg(geo.info + self) & kInfoPresent)) continue;
+            }
+            double rho = 0., jx = 0., jy = 0., jz = 0.;
+#pragma unroll
+            for (int q = 0; q < Q; ++q) {
+                double v = (double)St::load(f + post_stream_slot<L>(geo, c, q, even_layout), p);
+                if constexpr (St::kDeviation) v += Tables<L>::w(q);
+                rho += v;
+                if (Tables<L>::cx(q)) jx += Tables<L>::cx(q) > 0 ? v : -v;
+                if (Tables<L>::cy(q)) jy += Tables<L>::cy(q) > 0 ? v : -v;
+                if (L::kDims == 3 && Tables<L>::cz(q)) jz += Tables<L>::cz(q) > 0 ? v : -v;
+            }
+            acc[0] += rho;
+            acc[1] += jx;
+            acc[2] += jy;
+            acc[3] += jz;
         }
-        double rho = 0., jx = 0., jy = 0., jz = 0.;
-        for (int q = 0; q < Q; ++q) {
-            double v = (double)St::load(f + post_stream_slot<L>(geo, c, q, even_layout), p);
-            if constexpr (St::kDeviation) v += Tables<L>::w(q);
-            rho += v;
-            jx += Tables<L>::cx(q) * v;
-            jy += Tables<L>::cy(q) * v;
-            jz += Tables<L>::cz(q) * v;
-        }
-        acc[0] += rho;
-        acc[1] += jx;
-        acc[2] += jy;
-        acc[3] += jz;
     }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
