@@ -294,6 +294,27 @@ int zl_write_checkpoint_nodes(zl_ctx* ctx, const char* path, const uint64_t* con
    flags and forces are left to the host (forces are recomputed by the next forcing pass). */
 int zl_read_checkpoint_nodes(zl_ctx* ctx, const char* path);
 
+/* ---------------------------------------------------------------- field output (VTK XML)
+   Replaces VtkWriterManager::WriteVtuAll with its default kPartitionMultiBlock option
+   (amr_project/io/vtk_writer_manager.cpp:103-190, reached through IoManager::OutputMeshData,
+   io/io_manager.cpp:100-112): <prefix>_data/rank_0_grid_level_<l>.vtu for every level and
+   <prefix>_data/rank_0_.pvtu listing them, in the reference's layout and number formats
+   (binary: base64 of a UInt32 byte count and the data; ascii: the printf formats of
+   IoManager::SetupOutputFormat).  Point arrays flag_status (UInt16), vtkGhostType (UInt8: 1 where
+   flag & ghost_mask), rho and velocity (Float32, recomputed from the current populations, with
+   the node forces on forced levels), coordinates (Float32: origin + spacing / 2^l per set
+   Morton bit, SFBitsetComputeCoordinate); VTK_PIXEL / VTK_VOXEL cells for every point whose
+   +x/+y/+z corners are all points of the level (SFBitsetBelongToOneCell).  The per-point arrays,
+   the cell connectivity and the base64 text are built on the device.
+   codes[l], flags[l], n[l]: level l's points in output order (the reference writes its hash-map
+   order) with their flag_status; space / origin: the background grid spacing and the coordinate
+   of index 0 per axis (-spacing * k0MinIndexOfBackgroundNode_ for the reference's grids).
+   The reference writes "rho" before "velocity" recomputes the node macros, so its rho is the node
+   member left by the last collision; here rho is the density of the current populations. */
+#define ZL_VTU_GHOST_DEFAULT 0x3Eu /* C2F0 | C2F ghost | F2C0 | F2C ghost | MPI outer (NodeBitStatus) */
+int zl_write_vtu(zl_ctx* ctx, const char* prefix, int binary, const double* space, const double* origin,
+                 uint32_t ghost_mask, const uint64_t* const* codes, const int32_t* const* flags, const int64_t* n);
+
 /* ---------------------------------------------------------------- full-box levels, device I/O
    No counterpart in the reference, whose levels are always hash maps of nodes; these let a
    periodic box of 10^9 nodes be set up and read without host node lists. */

@@ -10,6 +10,10 @@
 //   init=eq|tgv  u0=<TGV amplitude>  rho0=<default density>  vel=ux,uy[,uz] (initial uniform)
 //   out0=<file>  out=<file>  (binary dumps before and after stepping; optional)
 //   ckpt=<prefix>  (after stepping, the reference's checkpoint folder <prefix>_checkpoint<step>)
+//   rout=<file>  (after stepping: int32 levels, then per level int64 n and n records of uint64 code,
+//                 double rho_, sorted by code)
+//   vtu=<prefix> vtu_binary=0|1  (after stepping and rout, the reference's own field output
+//                 IoManager::OutputMeshData: folder <prefix>_data with per-level .vtu and a .pvtu)
 //   timing=1 (print wall-clock seconds of the TimeMarching loop)  warmup=W (untimed steps first)
 //
 // Dump format (little endian): int32 dims, int32 q, int64 n, then n records of
@@ -464,6 +468,34 @@ int main(int argc, char* argv[]) {
             amr->ptr_io_manager_->WriteCheckPointData(t, kv["ckpt"], gm, gm, *amr->ptr_criterion_manager_,
                                                       *amr->ptr_mpi_manager_);
         }
+    }
+    if (kv.count("rout")) {
+        // the node member rho_ the reference's "rho" output variable writes (set by the last collision)
+        FILE* fp = std::fopen(kv["rout"].c_str(), "wb");
+        if (!fp) { std::perror(kv["rout"].c_str()); return 3; }
+        auto& infos = amr->ptr_grid_manager_->vec_ptr_grid_info_;
+        int32_t nl = static_cast<int32_t>(infos.size());
+        std::fwrite(&nl, sizeof(nl), 1, fp);
+        for (auto& info : infos) {
+            auto& nodes = *dynamic_cast<lbmproject::GridInfoLbmInteface&>(*info).GetPtrToLbmGrid();
+            std::vector<std::pair<uint64_t, double>> rr;
+            for (auto& it : nodes) rr.emplace_back(it.first.to_ullong(), it.second->rho_);
+            std::sort(rr.begin(), rr.end());
+            int64_t nr = static_cast<int64_t>(rr.size());
+            std::fwrite(&nr, sizeof(nr), 1, fp);
+            for (auto& [code, rho] : rr) {
+                std::fwrite(&code, sizeof(code), 1, fp);
+                std::fwrite(&rho, sizeof(rho), 1, fp);
+            }
+        }
+        std::fclose(fp);
+    }
+    if (kv.count("vtu")) {
+        auto& io = *amr->ptr_io_manager_;
+        io.bool_binary_ = !kv.count("vtu_binary") || std::atoi(kv["vtu_binary"].c_str()) != 0;
+        io.SetupOutputFormat();
+        io.SetupDependentIOParameters();
+        io.OutputMeshData(kv["vtu"], amr->ptr_grid_manager_.get(), amr->ptr_criterion_manager_.get());
     }
     if (kv.count("timing")) {
         const double sec = std::chrono::duration<double>(t1 - t0).count();

@@ -8,7 +8,10 @@ Run in a container that has the reference sources (the oracle harness
 Each ``lbm_<name>.npz`` holds the configuration, the Morton codes of every stored
 node (reference order: sorted codes) and the populations before and after
 ``steps`` time steps of the reference's own TimeMarching.  ``morton_<d>d.npz``
-holds codes and the reference's FindXNeg/FindXPos/... results for them.
+holds codes and the reference's FindXNeg/FindXPos/... results for them.  ``vtu_<name>.npz``
+holds the .vtu/.pvtu files the reference's own VTK writer produced after a run (binary and
+ASCII), with each level's codes, flags, populations and node member rho_ at that time
+(``python tests/golden/make_golden.py vtu`` regenerates only those).
 """
 from __future__ import annotations
 
@@ -159,6 +162,55 @@ def run_checkpoint(name, case, tmp):
     print("checkpoint", name, raw.size, "bytes")
 
 
+# field output written by the reference's own VTK writer (IoManager::OutputMeshData) after a run
+VTU_CASES = {
+    "tgv3d": dict(dims=3, n=(4, 4, 4), levels=0, coll="mrt", nu=0.02, init="tgv", u0=0.05,
+                  bc=["xmin:per", "xmax:per", "ymin:per", "ymax:per", "zmin:per", "zmax:per"], steps=3),
+    "amr2d_l1": dict(AMR_CASES["amr2d_l1"], steps=2),
+    "force2d_mrt": dict(AMR_CASES["force2d_mrt"], steps=5),
+}
+
+
+def run_vtu(name, case, tmp):
+    """The reference's .vtu/.pvtu text (binary and ASCII) with every level's state at that time."""
+    from oracle.port import load_levels
+    out = {"meta": json.dumps(case)}
+    for binary in (1, 0):
+        wd = os.path.join(tmp, f"vtu_{name}_{binary}")
+        os.makedirs(wd, exist_ok=True)
+        args = [REF_RUN, f"dims={case['dims']}", "n=" + ",".join(str(v) for v in case["n"]),
+                f"levels={case['levels']}", f"coll={case['coll']}", f"nu={case['nu']!r}", f"steps={case['steps']}",
+                "lout=" + os.path.join(wd, "l1.bin"), "rout=" + os.path.join(wd, "rho.bin"),
+                "vtu=" + os.path.join(wd, "run"), f"vtu_binary={binary}"] + [f"bc={b}" for b in case["bc"]]
+        for key in ("geo", "ib", "ext", "inner", "cforce", "init", "u0"):
+            if key in case:
+                args.append(f"{key}={case[key]}")
+        if "cforce" in case:
+            args.append("forces=1")
+        subprocess.run(args, check=True, cwd=wd, stdout=subprocess.DEVNULL)
+        tag = "bin" if binary else "asc"
+        folder = os.path.join(wd, "run_data")
+        levels = case["levels"] + 1
+        for lv in range(levels):
+            out[f"vtu_{tag}{lv}"] = np.fromfile(os.path.join(folder, f"rank_0_grid_level_{lv}.vtu"), np.uint8)
+        out[f"pvtu_{tag}"] = np.fromfile(os.path.join(folder, "rank_0_.pvtu"), np.uint8)
+        if binary:
+            _, _, after = load_levels(os.path.join(wd, "l1.bin"))
+            raw = open(os.path.join(wd, "rho.bin"), "rb").read()
+            pos = 4
+            for lv, a in enumerate(after):
+                out[f"codes{lv}"] = a["nodes"]["code"]
+                out[f"flags{lv}"] = a["nodes"]["flag"]
+                out[f"f{lv}"] = a["nodes"]["f"]
+                nr = int(np.frombuffer(raw[pos:pos + 8], np.int64)[0])
+                rec = np.frombuffer(raw[pos + 8:pos + 8 + nr * 16], dtype=[("code", "<u8"), ("rho", "<f8")])
+                assert np.array_equal(rec["code"], a["nodes"]["code"])
+                out[f"rho_member{lv}"] = rec["rho"].copy()
+                pos += 8 + nr * 16
+    np.savez_compressed(os.path.join(HERE, f"vtu_{name}.npz"), **out)
+    print("vtu", name, [out[f"vtu_bin{lv}"].size for lv in range(case["levels"] + 1)], "bytes (binary)")
+
+
 def morton_cases(dims: int, rng: np.random.Generator) -> np.ndarray:
     nb = 64 // dims
     edge = []
@@ -194,6 +246,8 @@ def main():
             run_amr(name, case, tmp)
         for name in CKPT_CASES:
             run_checkpoint(name, AMR_CASES[name], tmp)
+        for name, case in VTU_CASES.items():
+            run_vtu(name, case, tmp)
         for dims in (2, 3):
             fout = os.path.join(tmp, f"les{dims}.bin")
             subprocess.run([REF_RUN, "mode=les", f"dims={dims}", f"out={fout}"], check=True, cwd=tmp,
@@ -216,7 +270,13 @@ def main():
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["checkpoints"]:
+    if sys.argv[1:] == ["vtu"]:
+        if not os.path.exists(REF_RUN):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            for name, case in VTU_CASES.items():
+                run_vtu(name, case, tmp)
+    elif sys.argv[1:] == ["checkpoints"]:
         if not os.path.exists(REF_RUN):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
         with tempfile.TemporaryDirectory() as tmp:

@@ -122,6 +122,8 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
                                        ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(i64)],
                                       ctypes.c_int),
         "zl_read_checkpoint_nodes": ([P, ctypes.c_char_p], ctypes.c_int),
+        "zl_write_vtu": ([P, ctypes.c_char_p, ctypes.c_int, dp, dp, ctypes.c_uint32, ctypes.POINTER(u64p),
+                          ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(i64)], ctypes.c_int),
         "zl_set_temporal_interpolation": ([P, ctypes.c_int], ctypes.c_int),
         "zl_interpolate_interface": ([P, ctypes.c_int], ctypes.c_int),
         "zl_autotune": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
@@ -330,6 +332,22 @@ class Context:
         fp = (ctypes.POINTER(ctypes.c_int32) * levels)(*[_p(f, ctypes.c_int32) for f in fs])
         n = (ctypes.c_int64 * levels)(*[c.size for c in cs])
         self._check(self.lib.zl_write_checkpoint_nodes(self.handle, path.encode(), cp, fp, n))
+
+    def write_vtu(self, prefix: str, codes: list, flags: list, binary: bool = True, space=(1.0, 1.0, 1.0),
+                  origin=(-1.0, -1.0, -1.0), ghost_mask: int = 0x3E):
+        """The reference's VTK XML field output (<prefix>_data/rank_0_grid_level_<l>.vtu and
+        rank_0_.pvtu); codes[l], flags[l]: level l's points in output order with their flag_status.
+        origin defaults to -spacing * 1, the reference's minimum background node index."""
+        levels = len(codes)
+        cs = [_u64(c) for c in codes]
+        fs = [np.ascontiguousarray(np.asarray(f, dtype=np.int32)) for f in flags]
+        cp = (ctypes.POINTER(ctypes.c_uint64) * levels)(*[_p(c, ctypes.c_uint64) for c in cs])
+        fp = (ctypes.POINTER(ctypes.c_int32) * levels)(*[_p(f, ctypes.c_int32) for f in fs])
+        n = (ctypes.c_int64 * levels)(*[c.size for c in cs])
+        sp = (ctypes.c_double * 3)(*space)
+        og = (ctypes.c_double * 3)(*origin)
+        self._check(self.lib.zl_write_vtu(self.handle, prefix.encode(), 1 if binary else 0, sp, og,
+                                          ctypes.c_uint32(ghost_mask), cp, fp, n))
 
     def read_checkpoint_nodes(self, path: str):
         self._check(self.lib.zl_read_checkpoint_nodes(self.handle, path.encode()))

@@ -32,6 +32,7 @@ SOURCES = {
     "kernels_f16.cu": [],
     "static_scratch.cu": [],
     "closure.cu": [],
+    "vtu.cu": [],
 }
 
 

@@ -3,12 +3,14 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <filesystem>
 #include <string>
 #include <algorithm>
 #include <vector>
 #include "zllbm_b200.h"
 #include "closure_launch.cuh"
 #include "topology.cuh"
+#include "vtu.cuh"
 
 using namespace zl;
 
@@ -1536,3 +1538,285 @@ int zl_read_checkpoint_nodes(zl_ctx* ctx, const char* path) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- VTK XML field output
+namespace {
+
+// One binary DataArray body: base64 text of the device payload, built on the device.
+int vtu_binary_array(zl_ctx* ctx, FILE* fp, const void* dpayload, size_t nbytes) {
+    if (nbytes > 0xffffffffull) return fail(ctx, ZL_ETOOLARGE, "a VTK array above 4 GiB (UInt32 header)");
+    const unsigned long long nchars = base64_chars(nbytes);
+    DeviceBuffer dtext;
+    int rc = alloc(ctx, dtext, (size_t)nchars);
+    if (rc) return rc;
+    ZL_CUDA(ctx, base64_encode(dpayload, nbytes, (char*)dtext.ptr, ctx->stream));
+    std::vector<char> text(nchars);
+    ZL_CUDA(ctx, cudaMemcpyAsync(text.data(), dtext.ptr, nchars, cudaMemcpyDeviceToHost, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (std::fwrite(text.data(), 1, nchars, fp) != nchars || std::fputc('\n', fp) == EOF)
+        return fail(ctx, ZL_EINVAL, "short write of a VTK file");
+    return ZL_OK;
+}
+
+template <class T>
+int vtu_fetch(zl_ctx* ctx, std::vector<T>& host, const void* dptr, size_t count) {
+    host.resize(count);
+    if (count) ZL_CUDA(ctx, cudaMemcpyAsync(host.data(), dptr, count * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return ZL_OK;
+}
+
+// SFBitsetComputeCoordinate (morton_aux.cpp:86-101, :310-333), for the ASCII form
+double vtu_coordinate(uint64_t code, int dims, int axis, int level, double space, double origin) {
+    const double gs = space / (double)(1ull << level);
+    double c = origin;
+    for (int b = 0; b < 64 / dims; ++b)
+        if ((code >> (dims * b + axis)) & 1ull) c += gs * (double)(1ull << b);
+    return c;
+}
+
+int vtu_level(zl_ctx* ctx, const std::string& path, int level, bool binary, const double* space, const double* origin,
+              uint32_t ghost_mask, const uint64_t* codes, const int32_t* flags, int64_t n) {
+    const int dims = ctx->dims;
+    const int corners = dims == 2 ? 4 : 8;
+    Level& L = ctx->levels[level];
+    if (n < 0 || n > 0x7fffffffll || (n > 0 && (!codes || !flags)))
+        return fail(ctx, ZL_EINVAL, "level %d: bad point list", level);
+    DeviceBuffer dcodes, dflags, dmac, dflag16, dghost, drho32, du32, dxyz, dtable, dcell, dfirst, dscan, dconn,
+        doffs, dtypes;
+    int rc;
+    if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
+    if ((rc = alloc(ctx, dflags, (size_t)std::max<int64_t>(n, 1) * 4))) return rc;
+    if (n) ZL_CUDA(ctx, cudaMemcpyAsync(dflags.ptr, flags, (size_t)n * 4, cudaMemcpyHostToDevice, ctx->stream));
+    // density and velocity recomputed from the current populations (the values the reference's
+    // "velocity" output variable computes, lbm_grid_interface.cpp:645-652)
+    if ((rc = alloc(ctx, dmac, (size_t)std::max<int64_t>(n, 1) * (dims + 1) * sizeof(double)))) return rc;
+    double* drho = (double*)dmac.ptr;
+    double* du = drho + n;
+    if (n) {
+        if ((rc = reset_flag(ctx))) return rc;
+        ZL_CUDA(ctx, ctx->ops->gather(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
+                                      (const uint64_t*)dcodes.ptr, nullptr, drho, du, n, (int*)ctx->scratch_flag.ptr,
+                                      ctx->stream));
+        int bad = 0;
+        if ((rc = read_flag(ctx, &bad))) return rc;
+        if (bad) return fail(ctx, ZL_ETOPOLOGY, "level %d: a point code is not part of the level", level);
+    }
+    // index box of the points -> point table
+    VtuLevel a{};
+    a.codes = (const uint64_t*)dcodes.ptr;
+    a.flags = (const int32_t*)dflags.ptr;
+    a.n = n;
+    a.dims = dims;
+    a.level = level;
+    for (int d = 0; d < 3; ++d) {
+        a.space[d] = space[d];
+        a.origin[d] = origin[d];
+        a.lo[d] = 0;
+        a.ext[d] = 1;
+    }
+    a.ghost_mask = ghost_mask;
+    long long table_cells = 1;
+    if (n) {
+        DeviceBuffer dmm;
+        if ((rc = alloc(ctx, dmm, 6 * sizeof(int)))) return rc;
+        int mm[6] = {INT32_MAX, INT32_MAX, INT32_MAX, 0, 0, 0};
+        ZL_CUDA(ctx, cudaMemcpyAsync(dmm.ptr, mm, sizeof(mm), cudaMemcpyHostToDevice, ctx->stream));
+        ZL_CUDA(ctx, launch_decode_minmax(a.codes, n, dims, (int*)dmm.ptr, ctx->stream));
+        ZL_CUDA(ctx, cudaMemcpyAsync(mm, dmm.ptr, sizeof(mm), cudaMemcpyDeviceToHost, ctx->stream));
+        ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        for (int d = 0; d < dims; ++d) {
+            a.lo[d] = mm[d];
+            a.ext[d] = (long long)mm[3 + d] - mm[d] + 1;
+            table_cells *= a.ext[d];
+        }
+    }
+    const size_t nn = (size_t)std::max<int64_t>(n, 1);
+    if ((rc = alloc(ctx, dtable, (size_t)table_cells * 4))) return rc;
+    ZL_CUDA(ctx, cudaMemsetAsync(dtable.ptr, 0xff, (size_t)table_cells * 4, ctx->stream));
+    if ((rc = alloc(ctx, dflag16, nn * 2)) || (rc = alloc(ctx, dghost, nn)) || (rc = alloc(ctx, drho32, nn * 4)) ||
+        (rc = alloc(ctx, du32, nn * dims * 4)) || (rc = alloc(ctx, dxyz, nn * 12)) || (rc = alloc(ctx, dcell, nn * 4)) ||
+        (rc = alloc(ctx, dfirst, nn * 4)))
+        return rc;
+    ZL_CUDA(ctx, vtu_points(a, drho, du, (uint16_t*)dflag16.ptr, (uint8_t*)dghost.ptr, (float*)drho32.ptr,
+                            (float*)du32.ptr, (float*)dxyz.ptr, (int32_t*)dtable.ptr, ctx->stream));
+    const size_t scan_bytes = std::max<size_t>(vtu_scan_bytes(n), 1);
+    if ((rc = alloc(ctx, dscan, scan_bytes))) return rc;
+    ZL_CUDA(ctx, vtu_cells(a, (const int32_t*)dtable.ptr, (uint32_t*)dcell.ptr, (uint32_t*)dfirst.ptr, dscan.ptr,
+                           scan_bytes, ctx->stream));
+    long long cells = 0;
+    if (n) {
+        uint32_t last[2];
+        ZL_CUDA(ctx, cudaMemcpyAsync(&last[0], (uint32_t*)dfirst.ptr + (n - 1), 4, cudaMemcpyDeviceToHost, ctx->stream));
+        ZL_CUDA(ctx, cudaMemcpyAsync(&last[1], (uint32_t*)dcell.ptr + (n - 1), 4, cudaMemcpyDeviceToHost, ctx->stream));
+        ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        cells = (long long)last[0] + last[1];
+    }
+    const size_t nc = (size_t)std::max<long long>(cells, 1);
+    if ((rc = alloc(ctx, dconn, nc * corners * 8)) || (rc = alloc(ctx, doffs, nc * 8)) || (rc = alloc(ctx, dtypes, nc)))
+        return rc;
+    ZL_CUDA(ctx, vtu_connect(a, (const int32_t*)dtable.ptr, (const uint32_t*)dcell.ptr, (const uint32_t*)dfirst.ptr,
+                             (uint64_t*)dconn.ptr, ctx->stream));
+    ZL_CUDA(ctx, vtu_offsets(cells, dims, (uint64_t*)doffs.ptr, (uint8_t*)dtypes.ptr, ctx->stream));
+
+    FILE* fp = std::fopen(path.c_str(), "w");
+    if (!fp) return fail(ctx, ZL_EINVAL, "cannot open %s", path.c_str());
+    struct Closer {
+        FILE* f;
+        ~Closer() { std::fclose(f); }
+    } closer{fp};
+    const char* fmt = binary ? "binary" : "ascii";
+    std::fprintf(fp, "<?xml version=\"1.0\"?>\n");
+    std::fprintf(fp, "<VTKFile type=\"UnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n");
+    std::fprintf(fp, " <UnstructuredGrid>\n");
+    std::fprintf(fp, "  <Piece NumberOfPoints=\"%lld\" NumberOfCells=\"%lld\">\n", (long long)n, cells);
+    std::fprintf(fp, "    <PointData>\n");
+    // host copies for the ASCII form (the reference prints the FP64 values with %f)
+    std::vector<double> hmac;
+    std::vector<uint64_t> hconn;
+    if (!binary) {
+        if ((rc = vtu_fetch(ctx, hmac, dmac.ptr, (size_t)n * (dims + 1)))) return rc;
+        if ((rc = vtu_fetch(ctx, hconn, dconn.ptr, (size_t)cells * corners))) return rc;
+    }
+    std::fprintf(fp, "      <DataArray NumberOfComponents=\"1\" type=\"UInt16\" Name=\"flag_status\" format=\"%s\">\n",
+                 fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, dflag16.ptr, (size_t)n * 2))) return rc;
+    } else {
+        for (int64_t i = 0; i < n; ++i) std::fprintf(fp, "       %hu\n", (unsigned short)flags[i]);
+    }
+    std::fprintf(fp, "      </DataArray>\n");
+    std::fprintf(fp, "      <DataArray type=\"UInt8\" Name=\"vtkGhostType\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, dghost.ptr, (size_t)n))) return rc;
+    } else {
+        for (int64_t i = 0; i < n; ++i) std::fprintf(fp, "   %u\n", (flags[i] & (int32_t)ghost_mask) != 0 ? 1u : 0u);
+    }
+    std::fprintf(fp, "      </DataArray>\n");
+    // output variables in std::set order: "rho", "velocity"
+    std::fprintf(fp, "      <DataArray NumberOfComponents=\"1\" type=\"Float32\" Name=\"rho\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, drho32.ptr, (size_t)n * 4))) return rc;
+    } else {
+        for (int64_t i = 0; i < n; ++i) std::fprintf(fp, "       %f\n", hmac[i]);
+    }
+    std::fprintf(fp, "      </DataArray>\n");
+    std::fprintf(fp, "      <DataArray NumberOfComponents=\"%d\" type=\"Float32\" Name=\"velocity\" format=\"%s\">\n",
+                 dims, fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, du32.ptr, (size_t)n * dims * 4))) return rc;
+    } else {
+        for (int64_t i = 0; i < n; ++i) {
+            for (int d = 0; d < dims; ++d) std::fprintf(fp, "       %f", hmac[n + i * dims + d]);
+            std::fprintf(fp, "\n");
+        }
+    }
+    std::fprintf(fp, "      </DataArray>\n");
+    std::fprintf(fp, "    </PointData>\n");
+    std::fprintf(fp, "   <Points>\n");
+    std::fprintf(fp, "    <DataArray type=\"Float32\" NumberOfComponents=\"3\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, dxyz.ptr, (size_t)n * 12))) return rc;
+    } else {
+        for (int64_t i = 0; i < n; ++i) {
+            double c[3] = {0., 0., 0.};
+            for (int d = 0; d < dims; ++d) c[d] = vtu_coordinate(codes[i], dims, d, level, space[d], origin[d]);
+            std::fprintf(fp, "   %f %f %f\n", c[0], c[1], c[2]);
+        }
+    }
+    std::fprintf(fp, "    </DataArray>\n");
+    std::fprintf(fp, "   </Points>\n");
+    std::fprintf(fp, "   <Cells>\n");
+    std::fprintf(fp, "    <DataArray type=\"UInt64\" Name=\"connectivity\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, dconn.ptr, (size_t)cells * corners * 8))) return rc;
+    } else {
+        for (long long c = 0; c < cells; ++c) {
+            std::fprintf(fp, "  ");
+            for (int k = 0; k < corners; ++k) std::fprintf(fp, " %llu", (unsigned long long)hconn[c * corners + k]);
+            std::fprintf(fp, "\n");
+        }
+    }
+    std::fprintf(fp, "    </DataArray>\n");
+    std::fprintf(fp, "    <DataArray type=\"UInt64\" Name=\"offsets\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, doffs.ptr, (size_t)cells * 8))) return rc;
+    } else {
+        for (long long c = 1; c <= cells; ++c) std::fprintf(fp, "   %llu\n", (unsigned long long)(c * corners));
+    }
+    std::fprintf(fp, "    </DataArray>\n");
+    std::fprintf(fp, "    <DataArray type=\"UInt8\" Name=\"types\" format=\"%s\">\n", fmt);
+    if (binary) {
+        if ((rc = vtu_binary_array(ctx, fp, dtypes.ptr, (size_t)cells))) return rc;
+    } else {
+        for (long long c = 0; c < cells; ++c) std::fprintf(fp, "   %u\n", dims == 2 ? 8u : 11u);
+    }
+    std::fprintf(fp, "    </DataArray>\n");
+    std::fprintf(fp, "   </Cells>\n");
+    std::fprintf(fp, "  </Piece>\n");
+    std::fprintf(fp, " </UnstructuredGrid>\n");
+    std::fprintf(fp, "</VTKFile>");
+    if (std::ferror(fp)) return fail(ctx, ZL_EINVAL, "write error on %s", path.c_str());
+    return ZL_OK;
+}
+
+}  // namespace
+
+int zl_write_vtu(zl_ctx* ctx, const char* prefix, int binary, const double* space, const double* origin,
+                 uint32_t ghost_mask, const uint64_t* const* codes, const int32_t* const* flags, const int64_t* n) {
+    if (!ctx || !prefix || !space || !origin || !codes || !flags || !n) return ZL_EINVAL;
+    const int levels = ctx->cfg.max_level + 1;
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    for (int l = 0; l < levels; ++l) {
+        const int rc = check_level(ctx, l, true);
+        if (rc) return rc;
+    }
+    const std::string folder = std::string(prefix) + "_data";
+    std::error_code ec;
+    std::filesystem::create_directories(folder, ec);
+    if (ec) return fail(ctx, ZL_EINVAL, "cannot create %s", folder.c_str());
+    for (int l = 0; l < levels; ++l) {
+        const int rc = vtu_level(ctx, folder + "/rank_0_grid_level_" + std::to_string(l) + ".vtu", l, binary != 0,
+                                 space, origin, ghost_mask, codes[l], flags[l], n[l]);
+        if (rc) return rc;
+    }
+    // WritePvtu (vtk_writer_manager.cpp:296-372)
+    const std::string pv = folder + "/rank_0_.pvtu";
+    FILE* fp = std::fopen(pv.c_str(), "w");
+    if (!fp) return fail(ctx, ZL_EINVAL, "cannot open %s", pv.c_str());
+    const char* fmt = binary ? "binary" : "ascii";
+    std::fprintf(fp, "<?xml version=\"1.0\"?>\n");
+    std::fprintf(fp, "<VTKFile type=\"PUnstructuredGrid\" version=\"0.1\" byte_order=\"LittleEndian\">\n");
+    std::fprintf(fp, " <PUnstructuredGrid>\n");
+    std::fprintf(fp, "    <PPointData>\n");
+    std::fprintf(fp, "      <PDataArray NumberOfComponents=\"1\" type=\"UInt16\" Name=\"flag_status\" format=\"%s\">\n",
+                 fmt);
+    std::fprintf(fp, "      </PDataArray>\n");
+    std::fprintf(fp, "      <PDataArray NumberOfComponents=\"1\" type=\"Float32\" Name=\"rho\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "      </PDataArray>\n");
+    std::fprintf(fp, "      <PDataArray NumberOfComponents=\"%d\" type=\"Float32\" Name=\"velocity\" format=\"%s\">\n",
+                 ctx->dims, fmt);
+    std::fprintf(fp, "      </PDataArray>\n");
+    std::fprintf(fp, "      <PDataArray type=\"UInt8\" Name=\"vtkGhostType\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "      </PDataArray>\n");
+    std::fprintf(fp, "    </PPointData>\n");
+    std::fprintf(fp, "   <PPoints>\n");
+    std::fprintf(fp, "    <PDataArray type=\"Float32\" NumberOfComponents=\"3\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "    </PDataArray>\n");
+    std::fprintf(fp, "   </PPoints>\n");
+    std::fprintf(fp, "   <PCells>\n");
+    std::fprintf(fp, "    <PDataArray type=\"UInt64\" Name=\"connectivity\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "    </PDataArray>\n");
+    std::fprintf(fp, "    <PDataArray type=\"UInt64\" Name=\"offsets\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "    </PDataArray>\n");
+    std::fprintf(fp, "    <PDataArray type=\"UInt8\" Name=\"types\" format=\"%s\">\n", fmt);
+    std::fprintf(fp, "    </PDataArray>\n");
+    std::fprintf(fp, "   </PCells>\n");
+    for (int l = 0; l < levels; ++l) std::fprintf(fp, "    <Piece Source=\"rank_0_grid_level_%d.vtu\"/>\n", l);
+    std::fprintf(fp, " </PUnstructuredGrid>\n");
+    std::fprintf(fp, " </VTKFile>\n");
+    const bool err = std::ferror(fp) != 0;
+    std::fclose(fp);
+    if (err) return fail(ctx, ZL_EINVAL, "write error on %s", pv.c_str());
+    return ZL_OK;
+}
