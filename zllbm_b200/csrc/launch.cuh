@@ -85,6 +85,13 @@ inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, 
     template <int C>                                                                                             \
     cudaError_t step_pair(bool odd, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {           \
         if constexpr (Storage<S>::kDeviation) {                                                                  \
+            if ((geo.n[0] & 1) || (geo.stride & 1)) {                                                            \
+                /* pair accesses need an even row length and plane stride: scalar kernel instead */             \
+                LevelGeom g1 = geo;                                                                              \
+                g1.block[0] = g1.block[1] = 0;                                                                   \
+                return odd ? step_one<D3Q19, C, true, false, false>(f, g1, p, s)                                 \
+                           : step_one<D3Q19, C, false, false, false>(f, g1, p, s);                               \
+            }                                                                                                    \
             dim3 g, b;                                                                                           \
             step_shape(geo, 3, g, b);                                                                            \
             if (odd) aa_pair_kernel<S, C, true><<<g, b, 0, s>>>(f, geo, p);                                      \
