@@ -532,7 +532,7 @@ __device__ __forceinline__ void mrt_d3q19_fused(const float* d, float* out, cons
     const float X12 = X1 + X2, Y12 = Y1 + Y2, Z12 = Z1 + Z2;
     const float jx = D1 + X12, jy = D2 + Y12, jz = D3 + Z12;
     const float rho = fmaf(drho, p.inv_scale, 1.f);
-    const float k = p.inv_scale / rho;
+    const float k = __fdividef(p.inv_scale, rho);  // fast reciprocal, two ulps (rho is close to 1)
     const float ux = jx * k, uy = jy * k, uz = jz * k;
     mac[0] = rho;
     mac[1] = ux;

@@ -68,7 +68,8 @@ __device__ __forceinline__ void fused_pair(const F2* d, F2* out, const StepParam
     const F2 X12 = X1 + X2, Y12 = Y1 + Y2, Z12 = Z1 + Z2;
     const F2 jx = D1 + X12, jy = D2 + Y12, jz = D3 + Z12;
     const F2 rho = vfma(drho, splat(p.inv_scale), splat(1.f));
-    const F2 k = splat(p.inv_scale) / rho;
+    // inv_scale / rho through the fast reciprocal (two ulps; rho is close to 1)
+    const F2 k = {make_float2(__fdividef(p.inv_scale, rho.v.x), __fdividef(p.inv_scale, rho.v.y))};
     const F2 ux = jx * k, uy = jy * k, uz = jz * k;
     const F2 ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
     const F2 usq = (ux2 + uy2) + uz2;
