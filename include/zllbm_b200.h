@@ -325,10 +325,11 @@ int zl_write_vtu(zl_ctx* ctx, const char* prefix, int binary, const double* spac
 int zl_set_level_box(zl_ctx* ctx, int level, const int32_t lo[3], const int32_t n[3]);
 
 /* Set every node of a full-box level to feq(rho, u), from device arrays in box order (x fastest):
-   rho_device[n], u_device[n * 3] (FP32). */
+   rho_device[n], u_device[n * 3] (FP32); any storage (FP64: feq in the reference's arithmetic). */
 int zl_set_equilibrium_dense(zl_ctx* ctx, int level, const float* rho_device, const float* u_device);
 
-/* Density and velocity of every node of a full-box level into device arrays (box order, FP32). */
+/* Density and velocity of every node of a full-box level into device arrays (box order, FP32);
+   any storage. */
 int zl_get_macros_dense(zl_ctx* ctx, int level, float* rho_device, float* u_device);
 
 /* ---------------------------------------------------------------- learned LES closure

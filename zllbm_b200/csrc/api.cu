@@ -1318,13 +1318,15 @@ int zl_mrt_matrix(int lattice, double tau, double* out) {
 
 }  // extern "C"
 
-// A full-box D3Q19 level in FP32 / FP16 / BF16 storage (the dense device I/O and closure kernels)
-static int check_box_level(zl_ctx* ctx, int level) {
+// A full-box D3Q19 level (the dense device I/O and closure kernels); the closure kernels need
+// FP32 / FP16 / BF16 storage, the dense equilibrium and macro I/O take FP64 as well.
+static int check_box_level(zl_ctx* ctx, int level, bool any_storage = false) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
     const Level& L = ctx->levels[level];
     if (ctx->dims != 3) return fail(ctx, ZL_EINVAL, "dense level I/O and the closure need D3Q19");
-    if (ctx->cfg.storage == ZL_STORAGE_F64) return fail(ctx, ZL_EINVAL, "dense level I/O needs FP32/FP16/BF16 storage");
+    if (!any_storage && ctx->cfg.storage == ZL_STORAGE_F64)
+        return fail(ctx, ZL_EINVAL, "the closure kernels need FP32/FP16/BF16 storage");
     if (L.nodes != (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2])
         return fail(ctx, ZL_EINVAL, "level %d is not a full box", level);
     return ZL_OK;
@@ -1333,7 +1335,7 @@ static int check_box_level(zl_ctx* ctx, int level) {
 extern "C" {
 
 int zl_set_equilibrium_dense(zl_ctx* ctx, int level, const float* rho_device, const float* u_device) {
-    int rc = check_box_level(ctx, level);
+    int rc = check_box_level(ctx, level, true);
     if (rc) return rc;
     if (!rho_device || !u_device) return fail(ctx, ZL_EINVAL, "null field");
     Level& L = ctx->levels[level];
@@ -1343,7 +1345,7 @@ int zl_set_equilibrium_dense(zl_ctx* ctx, int level, const float* rho_device, co
 }
 
 int zl_get_macros_dense(zl_ctx* ctx, int level, float* rho_device, float* u_device) {
-    int rc = check_box_level(ctx, level);
+    int rc = check_box_level(ctx, level, true);
     if (rc) return rc;
     if (!rho_device || !u_device) return fail(ctx, ZL_EINVAL, "null field");
     Level& L = ctx->levels[level];

@@ -399,6 +399,34 @@ __global__ void get_macros_kernel(const S* __restrict__ f, LevelGeom geo, StepPa
     u[i * 3 + 2] = mac[3];
 }
 
+// FP64 storage (absolute populations): feq in the reference's arithmetic order from the FP32
+// fields, and rho / u by the reference's macro rule, rounded to FP32 on output.
+__global__ void set_equilibrium_f64_kernel(double* __restrict__ f, LevelGeom geo, int even,
+                                           const float* __restrict__ rho, const float* __restrict__ u, long long nn) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const Coord c = box_coord(geo, i);
+    double feq[19];
+    feq_exact<D3Q19>((double)rho[i], (double)u[i * 3], (double)u[i * 3 + 1], (double)u[i * 3 + 2], feq);
+#pragma unroll
+    for (int q = 0; q < 19; ++q) f[post_stream_slot<D3Q19>(geo, c, q, even)] = feq[q];
+}
+
+__global__ void get_macros_f64_kernel(const double* __restrict__ f, LevelGeom geo, int even,
+                                      float* __restrict__ rho, float* __restrict__ u, long long nn) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const Coord c = box_coord(geo, i);
+    double v[19], r, ux, uy, uz;
+#pragma unroll
+    for (int q = 0; q < 19; ++q) v[q] = f[post_stream_slot<D3Q19>(geo, c, q, even)];
+    macro_exact<D3Q19>(v, r, ux, uy, uz);
+    rho[i] = (float)r;
+    u[i * 3] = (float)ux;
+    u[i * 3 + 1] = (float)uy;
+    u[i * 3 + 2] = (float)uz;
+}
+
 template <class S>
 __global__ void features_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, int even,
                                 float* __restrict__ x, long long nn) {
@@ -725,6 +753,17 @@ cudaError_t closure_box_op(int op, int storage, void* f, const LevelGeom& geo, c
         case ZL_STORAGE_F32: return dispatch_box<float>(op, f, geo, p, even, a, b, c, factor, nc, s);
         case ZL_STORAGE_F16: return dispatch_box<__half>(op, f, geo, p, even, a, b, c, factor, nc, s);
         case ZL_STORAGE_BF16: return dispatch_box<__nv_bfloat16>(op, f, geo, p, even, a, b, c, factor, nc, s);
+        case ZL_STORAGE_F64: {
+            const long long nn = (long long)geo.n[0] * geo.n[1] * geo.n[2];
+            const unsigned blocks = (unsigned)((nn + 255) / 256);
+            if (op == kBoxSetEq)
+                set_equilibrium_f64_kernel<<<blocks, 256, 0, s>>>((double*)f, geo, even, a, b, nn);
+            else if (op == kBoxGetMacros)
+                get_macros_f64_kernel<<<blocks, 256, 0, s>>>((const double*)f, geo, even, b, c, nn);
+            else
+                return cudaErrorInvalidValue;
+            return cudaGetLastError();
+        }
         default: return cudaErrorInvalidValue;
     }
 }
