@@ -88,6 +88,9 @@ struct zl_ctx {
     DeviceBuffer params_dev;    // StepParams of every level on the device (batched steps read them)
     bool batched = true;        // independent consecutive level steps share one launch (zl_set_batching)
     bool temporal = false;      // time interpolation at the coarse/fine interfaces (zl_set_temporal_interpolation)
+    // staging of the node I/O calls (codes, populations, macros): grown on demand and kept until
+    // the context is destroyed, so repeated exchanges allocate nothing
+    DeviceBuffer stage_codes, stage_data, stage_mac;
 };
 
 namespace {
@@ -120,6 +123,12 @@ int alloc(zl_ctx* ctx, DeviceBuffer& b, size_t bytes) {
     }
     b.bytes = bytes;
     return ZL_OK;
+}
+
+// Keep b at least `bytes` large (contents are not preserved when it grows).
+int reserve(zl_ctx* ctx, DeviceBuffer& b, size_t bytes) {
+    if (b.ptr && b.bytes >= bytes) return ZL_OK;
+    return alloc(ctx, b, bytes);
 }
 
 double lattice_w(int dims, int q) { return dims == 2 ? Tables<D2Q9>::w(q) : Tables<D3Q19>::w(q); }
@@ -180,7 +189,7 @@ int check_level(zl_ctx* ctx, int level, bool need_active) {
 
 // Copy host codes to a temporary device array.
 int upload_codes(zl_ctx* ctx, const uint64_t* codes, int64_t n, DeviceBuffer& d) {
-    int rc = alloc(ctx, d, (size_t)n * sizeof(uint64_t));
+    int rc = reserve(ctx, d, (size_t)n * sizeof(uint64_t));
     if (rc) return rc;
     if (n > 0) ZL_CUDA(ctx, cudaMemcpyAsync(d.ptr, codes, (size_t)n * 8, cudaMemcpyHostToDevice, ctx->stream));
     return ZL_OK;
@@ -538,22 +547,24 @@ static int exchange(zl_ctx* ctx, int level, const uint64_t* codes, double* f_hos
     ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
     Level& L = ctx->levels[level];
     const int q = ctx->q, dims = ctx->dims;
-    DeviceBuffer dcodes, dbuf, dmac;
+    DeviceBuffer& dcodes = ctx->stage_codes;
+    DeviceBuffer& dbuf = ctx->stage_data;
+    DeviceBuffer& dmac = ctx->stage_mac;
     if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
     if ((rc = reset_flag(ctx))) return rc;
     if (write) {
-        if ((rc = alloc(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
+        if ((rc = reserve(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
         ZL_CUDA(ctx, cudaMemcpyAsync(dbuf.ptr, f_host, (size_t)n * q * 8, cudaMemcpyHostToDevice, ctx->stream));
         ZL_CUDA(ctx, ctx->ops->scatter(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
                                        (const uint64_t*)dcodes.ptr, (const double*)dbuf.ptr, n,
                                        (int*)ctx->scratch_flag.ptr, ctx->stream));
     } else {
-        if (f_host && (rc = alloc(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
-        if (rho && (rc = alloc(ctx, dmac, (size_t)n * (dims + 1) * sizeof(double)))) return rc;
+        if (f_host && (rc = reserve(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
+        if (rho && (rc = reserve(ctx, dmac, (size_t)n * (dims + 1) * sizeof(double)))) return rc;
         double* drho = rho ? (double*)dmac.ptr : nullptr;
         double* du = rho ? drho + n : nullptr;
         ZL_CUDA(ctx, ctx->ops->gather(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
-                                      (const uint64_t*)dcodes.ptr, (double*)dbuf.ptr, drho, du, n,
+                                      (const uint64_t*)dcodes.ptr, f_host ? (double*)dbuf.ptr : nullptr, drho, du, n,
                                       (int*)ctx->scratch_flag.ptr, ctx->stream));
         if (f_host)
             ZL_CUDA(ctx, cudaMemcpyAsync(f_host, dbuf.ptr, (size_t)n * q * 8, cudaMemcpyDeviceToHost, ctx->stream));
