@@ -128,7 +128,9 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
 /* Write / read the post-stream populations f_ (GridNodeLbm::f_, lbm_interface.h:37) of the
    nodes with the given codes; f holds n * q doubles, node-major.  On periodic axes the
    reference stores the maximum plane as a duplicate of the minimum plane
-   (grid/grid_manager3d.cpp:106-112); both codes address the same device node. */
+   (grid/grid_manager3d.cpp:106-112); both codes address the same device node.  The device
+   staging of these calls (and of zl_get_macros) grows to the largest exchange and stays with the
+   context until zl_destroy, so repeated exchanges allocate nothing. */
 int zl_set_populations(zl_ctx* ctx, int level, const uint64_t* codes, const double* f, int64_t n);
 int zl_get_populations(zl_ctx* ctx, int level, const uint64_t* codes, double* f, int64_t n);
 
