@@ -5,6 +5,7 @@
 #include <cstring>
 #include <filesystem>
 #include <string>
+#include <unordered_map>
 #include <algorithm>
 #include <vector>
 #include "zllbm_b200.h"
@@ -46,8 +47,9 @@ struct Level {
     std::vector<uint64_t> codes;  // sorted node codes (kept for multi-level set-ups)
     // coarse/fine transfer with the next coarser level (this level is the fine side)
     DeviceBuffer macro;                                   // rho, u of transfer sources
-    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_fine, c2f_w;
-    int n_c2f = 0;
+    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w;
+    DeviceBuffer c2f_ucell, c2f_ufine, c2f_g;  // distinct sources: cell, kind, values of a transfer
+    int n_c2f = 0, n_c2f_src = 0;
     DeviceBuffer f2c_coarse, f2c_fine;
     int n_f2c = 0;
     bool has_transfer = false;
@@ -662,7 +664,9 @@ static int level_faces(zl_ctx* ctx, Level& L) {
 
 static C2FStencil c2f_stencil(const Level& F) {
     return C2FStencil{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
-                      (const uint8_t*)F.c2f_fine.ptr, (const double*)F.c2f_w.ptr, F.n_c2f};
+                      (const double*)F.c2f_w.ptr,      F.n_c2f,
+                      (const int*)F.c2f_ucell.ptr,     (const uint8_t*)F.c2f_ufine.ptr,
+                      F.n_c2f_src,                     F.c2f_g.ptr};
 }
 
 // Explosion targets of fine_level <- 0.5 (values at the last transfer + values from the coarse
@@ -688,8 +692,7 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level) {
     Level& F = ctx->levels[fine_level];
     Level& C = ctx->levels[fine_level - 1];
     if (!F.has_transfer) return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface first", fine_level);
-    C2FStencil st{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
-                  (const uint8_t*)F.c2f_fine.ptr, (const double*)F.c2f_w.ptr, F.n_c2f};
+    const C2FStencil st = c2f_stencil(F);
     ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
                                C.params, st, F.tau_c2f, (double*)F.c2f_last.ptr, nullptr, 1, ctx->stream));
     F.c2f_last_valid = F.c2f_last.ptr != nullptr;
@@ -1014,9 +1017,19 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
     const long long chi[3] = {(long long)ctx->cfg.domain_max[0] << (level - 1),
                               (long long)ctx->cfg.domain_max[1] << (level - 1),
                               (long long)ctx->cfg.domain_max[2] << (level - 1)};
-    std::vector<int> tgt, off(1, 0), src;
-    std::vector<uint8_t> src_fine;
+    std::vector<int> tgt, off(1, 0), src, ucell;
+    std::vector<uint8_t> ufine;
     std::vector<double> wts;
+    // distinct sources (key: cell * 2 + kind) -> row of the per-transfer source table
+    std::unordered_map<long long, int> row_of;
+    auto source_row = [&](long long cell, int kind) {
+        const auto it = row_of.emplace(cell * 2 + kind, (int)ucell.size());
+        if (it.second) {
+            ucell.push_back((int)cell);
+            ufine.push_back((uint8_t)kind);
+        }
+        return it.first->second;
+    };
     for (int64_t i = 0; i < n_c2f; ++i) {
         const long long tc = cell_of_code(F, dims, c2f_fine[i]);
         if (tc < 0) return fail(ctx, ZL_ETOPOLOGY, "level %d: interpolation target is not a node of the level", level);
@@ -1042,8 +1055,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
                     const long long cc = std::binary_search(excluded.begin(), excluded.end(), rc_code)
                                              ? -1 : cell_of_code(C, dims, rc_code);
                     if (cc >= 0) {
-                        src.push_back((int)cc);
-                        src_fine.push_back(0);
+                        src.push_back(source_row(cc, 0));
                     } else {
                         const uint64_t fcode = rc_code << dims;  // SFBitsetToNHigherLevel(1)
                         const long long fc = cell_of_code(F, dims, fcode);
@@ -1054,8 +1066,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
                             return fail(ctx, ZL_ETOPOLOGY,
                                         "level %d: an interpolation source is itself a target (order dependent)",
                                         level);
-                        src.push_back((int)fc);
-                        src_fine.push_back(1);
+                        src.push_back(source_row(fc, 1));
                     }
                     wts.push_back(w);
                 }
@@ -1072,11 +1083,15 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
         f2c_f.push_back((int)fc);
     }
     if ((rc = upload_vec(ctx, F.c2f_target, tgt)) || (rc = upload_vec(ctx, F.c2f_offset, off)) ||
-        (rc = upload_vec(ctx, F.c2f_src, src)) || (rc = upload_vec(ctx, F.c2f_fine, src_fine)) ||
-        (rc = upload_vec(ctx, F.c2f_w, wts)) || (rc = upload_vec(ctx, F.f2c_coarse, f2c_c)) ||
-        (rc = upload_vec(ctx, F.f2c_fine, f2c_f)))
+        (rc = upload_vec(ctx, F.c2f_src, src)) || (rc = upload_vec(ctx, F.c2f_ucell, ucell)) ||
+        (rc = upload_vec(ctx, F.c2f_ufine, ufine)) || (rc = upload_vec(ctx, F.c2f_w, wts)) ||
+        (rc = upload_vec(ctx, F.f2c_coarse, f2c_c)) || (rc = upload_vec(ctx, F.f2c_fine, f2c_f)))
         return rc;
     F.n_c2f = (int)tgt.size();
+    F.n_c2f_src = (int)ucell.size();
+    // source values in the storage's arithmetic type (FP64 for FP64 storage, FP32 otherwise)
+    const size_t g_elem = ctx->cfg.storage == ZL_STORAGE_F64 ? sizeof(double) : sizeof(float);
+    if ((rc = alloc(ctx, F.c2f_g, (size_t)std::max(F.n_c2f_src, 1) * ctx->q * g_elem))) return rc;
     F.n_f2c = (int)f2c_c.size();
     if ((rc = alloc(ctx, F.c2f_last, (size_t)std::max(F.n_c2f, 1) * ctx->q * sizeof(double)))) return rc;
     F.c2f_last_valid = false;

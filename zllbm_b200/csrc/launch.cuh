@@ -203,13 +203,19 @@ inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, 
                         const C2FStencil& st, double tau_ratio, double* save, const double* prev, int store,     \
                         cudaStream_t s) {                                                                        \
         if (st.n_targets <= 0) return cudaSuccess;                                                               \
+        const unsigned sblocks = (unsigned)((st.n_sources + 127) / 128);                                         \
         const unsigned blocks = (unsigned)((st.n_targets + 127) / 128);                                          \
-        if (dims == 2)                                                                                           \
-            c2f_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp, cp, \
-                                                       st, tau_ratio, save, prev, store);                        \
-        else                                                                                                     \
-            c2f_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, (const S*)fc, cgeo, c_even, fp,    \
-                                                        cp, st, tau_ratio, save, prev, store);                   \
+        if (dims == 2) {                                                                                         \
+            if (st.n_sources > 0)                                                                                \
+                c2f_sources_kernel<D2Q9, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,    \
+                                                                    cgeo, c_even, fp, cp, st, tau_ratio);        \
+            c2f_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, fp, st, save, prev, store);         \
+        } else {                                                                                                 \
+            if (st.n_sources > 0)                                                                                \
+                c2f_sources_kernel<D3Q19, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,   \
+                                                                     cgeo, c_even, fp, cp, st, tau_ratio);       \
+            c2f_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((S*)ff, fgeo, f_even, fp, st, save, prev, store);        \
+        }                                                                                                        \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t f2c_any(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc,                   \

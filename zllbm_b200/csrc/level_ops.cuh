@@ -258,13 +258,18 @@ __global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParam
 // ---------------------------------------------------------------- coarse <-> fine transfer
 // Interpolation stencil of one fine ghost node: entries [offset[t], offset[t+1]) of the source
 // arrays, in the reference's loop order (z outer, x inner, grid/grid_interpolation.cpp:485-517).
+// Every distinct source node is evaluated once per transfer (c2f_sources_kernel) into the
+// table g; the targets then form their weighted sums from the table.
 struct C2FStencil {
     const int* target;        // fine cell of every target node
     const int* offset;        // n_targets + 1
-    const int* src_cell;      // coarse cell (src_fine == 0) or fine cell (src_fine == 1)
-    const uint8_t* src_fine;
+    const int* src;           // entry -> row of the source table
     const double* weight;
     int n_targets;
+    const int* src_cell;      // per source: coarse cell (src_fine == 0) or fine cell (src_fine == 1)
+    const uint8_t* src_fine;
+    int n_sources;
+    void* g;                  // n_sources x Q source values (the storage's arithmetic type)
 };
 
 // Explosion (TransferInfoFromCoarseGrid, lbm_grid_interface.cpp:408-515): every fine ghost node
@@ -272,50 +277,72 @@ struct C2FStencil {
 // (NodeInfoCoarse2fine + PostStreamCoarse2Fine, lbm_grid_interface.cpp:570-588,
 // collision_model/lbm_collision_models.cpp:244-251) or the post-stream populations of the
 // coincident fine node when the coarse node is absent or flagged.
+// One thread per distinct source: g = feq(rho_c, u_c) + tau_c2f (f_c - feq) for a coarse source,
+// the post-stream populations for a fine one.
 template <class L, class S>
+__global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, const S* __restrict__ fc,
+                                   LevelGeom cgeo, int c_even, StepParams fp, StepParams cp, C2FStencil st,
+                                   double tau_ratio) {
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ;
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u >= st.n_sources) return;
+    T g[Q];
+    if (st.src_fine[u]) {
+        const Coord c = cell_coord(fgeo, st.src_cell[u]);
+#pragma unroll
+        for (int q = 0; q < Q; ++q) g[q] = St::load(ff + post_stream_slot<L>(fgeo, c, q, f_even), fp);
+    } else {
+        const Coord c = cell_coord(cgeo, st.src_cell[u]);
+        T fcq[Q];
+#pragma unroll
+        for (int q = 0; q < Q; ++q) fcq[q] = St::load(fc + post_stream_slot<L>(cgeo, c, q, c_even), cp);
+        if constexpr (St::kDeviation) {
+            float rho, ux, uy, uz, deq[Q];
+            macro_dev<L>(fcq, rho, ux, uy, uz);
+            feq_dev<L>(rho, ux, uy, uz, deq);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] = deq[q] + (float)tau_ratio * (fcq[q] - deq[q]);
+        } else {
+            double rho, ux, uy, uz, feq[Q];
+            macro_exact<L>(fcq, rho, ux, uy, uz);
+            feq_exact<L>(rho, ux, uy, uz, feq);
+#pragma unroll
+            for (int q = 0; q < Q; ++q) g[q] = feq[q] + tau_ratio * (fcq[q] - feq[q]);
+        }
+    }
+    T* out = static_cast<T*>(st.g) + (long long)u * Q;
+#pragma unroll
+    for (int q = 0; q < Q; ++q) out[q] = g[q];
+}
+
+// Explosion (TransferInfoFromCoarseGrid, lbm_grid_interface.cpp:408-515): every fine ghost node
+// becomes sum_k w_k g_k over its sources in the reference's order, g_k from the source table
+// (NodeInfoCoarse2fine + PostStreamCoarse2Fine, lbm_grid_interface.cpp:570-588,
+// collision_model/lbm_collision_models.cpp:244-251, or the post-stream populations of the
+// coincident fine node when the coarse node is absent or flagged).
 // save (optional) receives the targets' values (n_targets x Q, FP64); with prev (optional) the
 // targets get 0.5 (prev + value) instead, the time interpolation between the last transfer and
 // the coarse level's current state (no counterpart in the reference, whose explosion is spatial
 // only); store = 0 only saves.
-__global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, const S* __restrict__ fc, LevelGeom cgeo,
-                           int c_even, StepParams fp, StepParams cp, C2FStencil st, double tau_ratio,
+template <class L, class S>
+__global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, StepParams fp, C2FStencil st,
                            double* __restrict__ save, const double* __restrict__ prev, int store) {
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= st.n_targets) return;
+    const T* __restrict__ g = static_cast<const T*>(st.g);
     T acc[Q];
 #pragma unroll
     for (int q = 0; q < Q; ++q) acc[q] = (T)0;
     for (int k = st.offset[t]; k < st.offset[t + 1]; ++k) {
         const T w = (T)st.weight[k];
-        T g[Q];
-        if (st.src_fine[k]) {
-            const Coord c = cell_coord(fgeo, st.src_cell[k]);
+        const T* gk = g + (long long)st.src[k] * Q;
 #pragma unroll
-            for (int q = 0; q < Q; ++q) g[q] = St::load(ff + post_stream_slot<L>(fgeo, c, q, f_even), fp);
-        } else {
-            const Coord c = cell_coord(cgeo, st.src_cell[k]);
-            T fcq[Q];
-#pragma unroll
-            for (int q = 0; q < Q; ++q) fcq[q] = St::load(fc + post_stream_slot<L>(cgeo, c, q, c_even), cp);
-            if constexpr (St::kDeviation) {
-                float rho, ux, uy, uz, deq[Q];
-                macro_dev<L>(fcq, rho, ux, uy, uz);
-                feq_dev<L>(rho, ux, uy, uz, deq);
-#pragma unroll
-                for (int q = 0; q < Q; ++q) g[q] = deq[q] + (float)tau_ratio * (fcq[q] - deq[q]);
-            } else {
-                double rho, ux, uy, uz, feq[Q];
-                macro_exact<L>(fcq, rho, ux, uy, uz);
-                feq_exact<L>(rho, ux, uy, uz, feq);
-#pragma unroll
-                for (int q = 0; q < Q; ++q) g[q] = feq[q] + tau_ratio * (fcq[q] - feq[q]);
-            }
-        }
-#pragma unroll
-        for (int q = 0; q < Q; ++q) acc[q] = acc[q] + w * g[q];
+        for (int q = 0; q < Q; ++q) acc[q] = acc[q] + w * gk[q];
     }
     if (save) {
 #pragma unroll
