@@ -880,14 +880,15 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
         }
     };
 
-    // Full boxes with a ghost frame address neighbours through three per-thread pointers (cells
-    // x-1, x, x+1 of the node's row) plus offsets that are uniform across the launch (plane q and
-    // the row step dy a0 + dz a0 a1), unless a periodic y / z row wraps at this node.  Both routes
-    // reach the same slots; the uniform one needs no per-access index arithmetic.  The two routes
-    // are separate copies of the node update so that each is scheduled on its own.  (Fully
-    // periodic boxes take aa_node_periodic for such rows instead.)
+    // Nodes address their neighbours through three per-thread pointers (cells x-1, x, x+1 of the
+    // node's row) plus offsets that are uniform across the launch (plane q and the row step
+    // dy a0 + dz a0 a1), unless a periodic y / z row wraps at this node.  Both routes reach the
+    // same slots (a ghost frame or an absent cell of a masked box is memory of the box like any
+    // other); the uniform one needs no per-access index arithmetic.  The two routes are separate
+    // copies of the node update so that each is scheduled on its own.  (Fully periodic full
+    // boxes take aa_node_periodic for such rows before reaching here.)
     const bool uniform_rows =
-        Bnd && !Masked && (!geo.periodic[1] || (c.x[1] > 0 && c.x[1] < geo.n[1] - 1)) &&
+        (!geo.periodic[1] || (c.x[1] > 0 && c.x[1] < geo.n[1] - 1)) &&
         (L::kDims == 2 || !geo.periodic[2] || (c.x[2] > 0 && c.x[2] < geo.n[2] - 1));
     if (uniform_rows) {
         S* const px[3] = {f + (bx[0] + row_self), f + (bx[1] + row_self), f + (bx[2] + row_self)};

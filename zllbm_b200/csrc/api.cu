@@ -59,7 +59,8 @@ struct Level {
     DeviceBuffer mrt64_d;    // M^-1 (I - S/2) M (FP64 forced MRT)
     DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
     DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
-    int n_vertices = 0;
+    DeviceBuffer ib_nodes;   // every cell a vertex stencil touches, once
+    int n_vertices = 0, n_ib_nodes = 0;
     int ib_width = 4;        // immersed-boundary stencil: 4 (reference) or 3 (Roma et al.)
     DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q doubles)
     bool c2f_last_valid = false;
@@ -1157,11 +1158,8 @@ static IbVertices ib_view(zl_ctx* ctx, Level& L, int level) {
 
 static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     IbVertices v = ib_view(ctx, L, level);
-    int rc = reset_flag(ctx);
-    if (rc) return rc;
-    ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.map, L.params, L.even_layout, v,
-                                    (double*)L.force.ptr, (double*)L.ib_vel.ptr, (int*)ctx->scratch_flag.ptr,
-                                    ctx->stream));
+    ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.params, L.even_layout, (const int*)L.ib_nodes.ptr,
+                                    L.n_ib_nodes, (double*)L.force.ptr, (double*)L.ib_vel.ptr, ctx->stream));
     // one warp per vertex, kIbWarps vertices per block
     const unsigned blocks = (unsigned)((v.n + kIbWarps - 1) / kIbWarps), threads = 32 * kIbWarps;
     if (ctx->dims == 2) {
@@ -1196,22 +1194,46 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
     }
     L.n_vertices = (int)n;
     ++ctx->generation;
-    // every stencil node must exist on the level (the reference logs an error otherwise)
+    // every stencil node must exist on the level (the reference logs an error otherwise); the
+    // distinct stencil cells become the node list of the pass's first launch
+    L.n_ib_nodes = 0;
     if (n > 0) {
         IbVertices v = ib_view(ctx, L, level);
         if ((rc = reset_flag(ctx))) return rc;
-        DeviceBuffer scratch_force, scratch_vel;
-        if ((rc = alloc(ctx, scratch_force, (size_t)cells * 3 * 8)) || (rc = alloc(ctx, scratch_vel, (size_t)cells * 3 * 8)))
+        if (cells > 0x7fffffffll) return fail(ctx, ZL_ETOOLARGE, "level %d: box too large for the node list", level);
+        DeviceBuffer mark, sel, count, tmp;
+        if ((rc = alloc(ctx, mark, (size_t)cells * 4)) || (rc = alloc(ctx, sel, (size_t)cells * 4)) ||
+            (rc = alloc(ctx, count, sizeof(int))))
             return rc;
-        ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.map, L.params, L.even_layout, v,
-                                        (double*)scratch_force.ptr, (double*)scratch_vel.ptr,
-                                        (int*)ctx->scratch_flag.ptr, ctx->stream));
+        ZL_CUDA(ctx, cudaMemsetAsync(mark.ptr, 0, (size_t)cells * 4, ctx->stream));
+        const int K = ctx->dims == 3 ? v.width * v.width * v.width : v.width * v.width;
+        const unsigned blocks = (unsigned)(((long long)n * K + 127) / 128);
+        if (ctx->dims == 2)
+            ib_mark_kernel<2><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (uint32_t*)mark.ptr,
+                                                              (int*)ctx->scratch_flag.ptr);
+        else
+            ib_mark_kernel<3><<<blocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (uint32_t*)mark.ptr,
+                                                              (int*)ctx->scratch_flag.ptr);
+        ZL_CUDA(ctx, cudaGetLastError());
         int bad = 0;
         if ((rc = read_flag(ctx, &bad))) return rc;
         if (bad) {
             L.n_vertices = 0;
             return fail(ctx, ZL_ETOPOLOGY, "level %d: an immersed-boundary stencil node is not on the level", level);
         }
+        size_t tmp_bytes = 0;
+        ZL_CUDA(ctx, select_marked((const uint32_t*)mark.ptr, (int)cells, (int*)sel.ptr, (int*)count.ptr, nullptr,
+                                   &tmp_bytes, ctx->stream));
+        if ((rc = alloc(ctx, tmp, std::max<size_t>(tmp_bytes, 1)))) return rc;
+        ZL_CUDA(ctx, select_marked((const uint32_t*)mark.ptr, (int)cells, (int*)sel.ptr, (int*)count.ptr, tmp.ptr,
+                                   &tmp_bytes, ctx->stream));
+        int nodes = 0;
+        ZL_CUDA(ctx, cudaMemcpyAsync(&nodes, count.ptr, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+        ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        if ((rc = alloc(ctx, L.ib_nodes, (size_t)std::max(nodes, 1) * 4))) return rc;
+        ZL_CUDA(ctx, cudaMemcpyAsync(L.ib_nodes.ptr, sel.ptr, (size_t)nodes * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        L.n_ib_nodes = nodes;
     }
     return ZL_OK;
 }

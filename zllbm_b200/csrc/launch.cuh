@@ -31,9 +31,8 @@ struct LaunchSet {
     cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const int* coarse_cell,
                        const int* fine_cell, int n, const double* fine_macro, double tau_ratio, cudaStream_t s);
-    cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const LevelMap& m, const StepParams& p,
-                            int even_layout, const IbVertices& v, double* node_force, double* node_vel, int* bad,
-                            cudaStream_t s);
+    cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even_layout,
+                            const int* nodes, int n_nodes, double* node_force, double* node_vel, cudaStream_t s);
     // ext: kExtForce / kExtLes bits of the levels in the batch
     cudaError_t (*batch)(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s);
 };
@@ -232,18 +231,17 @@ inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, 
                                                         cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);   \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
-    cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const LevelMap& m,                   \
-                             const StepParams& p, int even, const IbVertices& v, double* node_force,             \
-                             double* node_vel, int* bad, cudaStream_t s) {                                       \
-        if (v.n <= 0) return cudaSuccess;                                                                        \
-        const int k = dims == 3 ? v.width * v.width * v.width : v.width * v.width;                               \
-        const unsigned blocks = (unsigned)(((long long)v.n * k + 127) / 128);                                    \
+    cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even,      \
+                             const int* nodes, int n_nodes, double* node_force, double* node_vel,               \
+                             cudaStream_t s) {                                                                   \
+        if (n_nodes <= 0) return cudaSuccess;                                                                    \
+        const unsigned blocks = (unsigned)((n_nodes + 127) / 128);                                               \
         if (dims == 2)                                                                                           \
-            ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, m, p, even, v, node_force,         \
-                                                            node_vel, bad);                                      \
+            ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,           \
+                                                            node_force, node_vel);                               \
         else                                                                                                     \
-            ib_touch_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)f, geo, m, p, even, v, node_force,        \
-                                                             node_vel, bad);                                     \
+            ib_touch_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,          \
+                                                             node_force, node_vel);                              \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     template <class L, int C>                                                                                    \

@@ -4,6 +4,8 @@
 // The neighbour arithmetic restates the reference's SFBitsetAux{2D,3D}::Find{X,Y,Z}{Neg,Pos}
 // (amr_project/grid/morton_aux.hpp:65-297) on 64-bit integers: a Neg step on a zero axis
 // field returns the input code unchanged, a Pos step carries through the other axes' bits.
+#include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include "topology.cuh"
 
 namespace zl {
@@ -230,6 +232,14 @@ cudaError_t launch_count_present(const uint32_t* info, long long cells, unsigned
     const long long blocks = std::min<long long>((cells + 255) / 256, 148 * 8);
     count_present_kernel<<<(unsigned)std::max<long long>(blocks, 1), 256, 0, s>>>(info, cells, count);
     return cudaGetLastError();
+}
+
+
+// Indices i < n with mark[i] != 0, ascending, into out; *count (device) gets their number.
+// With tmp == nullptr only *tmp_bytes is set.
+cudaError_t select_marked(const uint32_t* mark, int n, int* out, int* count, void* tmp, size_t* tmp_bytes,
+                          cudaStream_t s) {
+    return cub::DeviceSelect::Flagged(tmp, *tmp_bytes, thrust::counting_iterator<int>(0), mark, out, count, n, s);
 }
 
 }  // namespace zl
