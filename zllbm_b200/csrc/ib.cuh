@@ -1,8 +1,9 @@
 // Immersed-boundary direct forcing on one level (FsiImmersedBoundary::CalculateBodyForce,
 // lbm_project/immersed_boundary/immersed_boundary.cpp:35-364), split in three launches:
-//   1. every node of every vertex stencil drops its immersed-boundary force and records its
-//      velocity computed from the post-stream populations with the remaining (constant) force
-//      (the reference does this on the first touch of a node, :157-168);
+//   1. every node of every vertex stencil (each once, from a list built with the vertices) drops
+//      its immersed-boundary force and records its velocity computed from the post-stream
+//      populations with the remaining (constant) force (the reference does this on the first
+//      touch of a node, :157-168);
 //   2. every vertex interpolates the node velocities with the delta kernel and sets its force
 //      F = 2 (U_b - u) (:183-184, :318-320);
 //   3. every vertex spreads F delta area / (dt dx^(d-1)) into the node forces (:187-199, :322-339).
@@ -111,17 +112,16 @@ __device__ __forceinline__ double ib_stencil_node(const IbVertices& v, int dims,
     return weight;
 }
 
-template <class L, class S>
-__global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, LevelMap m, StepParams p, int even_layout,
-                                IbVertices v, double* __restrict__ node_force, double* __restrict__ node_vel,
-                                int* __restrict__ bad) {
-    using St = Storage<S>;
-    using T = typename St::T;
-    constexpr int Q = L::kQ, D = L::kDims;
+// Every node a vertex stencil touches, once (the set is built when the vertices are set):
+// launch 1 of the pass runs over this list rather than over (vertex, stencil node) pairs, which
+// visit a node of the surface band once per vertex whose stencil holds it.
+template <int D>
+__global__ void ib_mark_kernel(LevelGeom geo, LevelMap m, IbVertices v, uint32_t* __restrict__ mark,
+                               int* __restrict__ bad) {
     const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= v.n * K) return;
-    const int i = t / K, k = t % K;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)v.n * K) return;
+    const int i = (int)(t / K), k = (int)(t % K);
     long long first[3], nid[3];
     double dis[3];
     ib_reference(v, v.coord + i * 3, D, first, dis);
@@ -131,6 +131,19 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, LevelMap
         atomicExch(bad, 1);
         return;
     }
+    mark[cell] = 1u;
+}
+
+template <class L, class S>
+__global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, int even_layout,
+                                const int* __restrict__ nodes, int n_nodes, double* __restrict__ node_force,
+                                double* __restrict__ node_vel) {
+    using St = Storage<S>;
+    using T = typename St::T;
+    constexpr int Q = L::kQ, D = L::kDims;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_nodes) return;
+    const long long cell = nodes[t];
     Coord c = cell_coord(geo, (int)cell);
     T fv[Q];
 #pragma unroll
@@ -199,10 +212,46 @@ __device__ __forceinline__ double warp_sum_d(double x) {
     return x;
 }
 
+// The warp's vertex: its stencil origin and the 1-D delta weights of each axis, computed once
+// (lanes 0 .. D * width - 1) instead of once per stencil node; a stencil node's weight is their
+// product in axis order, as ib_stencil_node forms it.
+struct IbWarpStencil {
+    double w[kIbWarps][3][4];
+};
+
+template <int D>
+__device__ __forceinline__ void ib_warp_weights(const IbVertices& v, const double* dis, IbWarpStencil& ws, int w,
+                                                int lane) {
+    if (lane < D * v.width) {
+        const int a = lane / v.width, o = lane % v.width;
+        ws.w[w][a][o] = ib_weight(v, dis[a], o);
+    }
+    __syncwarp();
+}
+
+template <int D>
+__device__ __forceinline__ double ib_node_weight(const IbVertices& v, const IbWarpStencil& ws, int w,
+                                                 const long long* first, int k, long long* nid) {
+    const int n = v.width;
+    const int o[3] = {k % n, (k / n) % n, k / (n * n)};
+    double weight = 1.;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (a < D) {
+            nid[a] = first[a] + o[a];
+            weight *= ws.w[w][a][o[a]];
+        } else {
+            nid[a] = 0;
+        }
+    }
+    return weight;
+}
+
 template <int D>
 __global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(LevelGeom geo, LevelMap m, IbVertices v,
                                                                  const double* __restrict__ node_vel) {
     __shared__ IbStage s;
+    __shared__ IbWarpStencil ws;
     ib_stage(v, s);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kIbWarps + w;
@@ -210,10 +259,11 @@ __global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(LevelGeom geo, 
     long long first[3], nid[3];
     double dis[3];
     ib_reference(v, s.coord[w], D, first, dis);
+    ib_warp_weights<D>(v, dis, ws, w, lane);
     const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
     double ur = 0., vr = 0., wr = 0.;
     for (int k = lane; k < K; k += 32) {
-        const double delta = ib_stencil_node(v, D, first, dis, k, nid);
+        const double delta = ib_node_weight<D>(v, ws, w, first, k, nid);
         const long long cell = ib_cell(geo, m, nid, D);
         ur += node_vel[cell * 3] * delta;
         vr += node_vel[cell * 3 + 1] * delta;
@@ -233,6 +283,7 @@ template <int D>
 __global__ void __launch_bounds__(32 * kIbWarps) ib_spread_kernel(LevelGeom geo, LevelMap m, StepParams p,
                                                                   IbVertices v, double* __restrict__ node_force) {
     __shared__ IbStage s;
+    __shared__ IbWarpStencil ws;
     ib_stage(v, s);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kIbWarps + w;
@@ -240,11 +291,12 @@ __global__ void __launch_bounds__(32 * kIbWarps) ib_spread_kernel(LevelGeom geo,
     long long first[3], nid[3];
     double dis[3];
     ib_reference(v, s.coord[w], D, first, dis);
+    ib_warp_weights<D>(v, dis, ws, w, lane);
     const double area = D == 3 ? s.area[w] / p.dt / v.dx / v.dx : s.area[w] / p.dt / v.dx;
     const double F[3] = {v.force[i * 3], v.force[i * 3 + 1], v.force[i * 3 + 2]};
     const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
     for (int k = lane; k < K; k += 32) {
-        const double delta = ib_stencil_node(v, D, first, dis, k, nid);
+        const double delta = ib_node_weight<D>(v, ws, w, first, k, nid);
         const long long cell = ib_cell(geo, m, nid, D);
         const double dt = delta * area;
         for (int a = 0; a < D; ++a) atomicAdd(node_force + cell * 3 + a, F[a] * dt);
