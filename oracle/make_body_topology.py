@@ -1,9 +1,11 @@
-"""Node sets and interface layers of the multi-level cube-flow grid, generated by the reference's
-own grid builder (refinement around a GeometryInfoOrigin cube, AmrManager::SetupMesh) through
-the oracle harness, and saved as the input of ``python -m zllbm_b200.cube_flow``.
+"""Node sets and interface layers of a multi-level grid refined around a body, generated by the
+reference's own grid builder (refinement around a GeometryInfoOrigin cube or circle,
+AmrManager::SetupMesh) through the oracle harness, and saved as the input of
+``python -m zllbm_b200.cube_flow`` (3D cube) or ``python -m zllbm_b200.cylinder_flow`` (2D circle).
 
-    python oracle/make_cube_topology.py OUT.npz [--n 256,128,128] [--levels 2] [--cube 80,64,64,16]
+    python oracle/make_body_topology.py OUT.npz [--n 256,128,128] [--levels 2] [--cube 80,64,64,16]
                                                 [--ext 6] [--inner 16]
+    python oracle/make_body_topology.py OUT.npz --n 1024,512 --levels 3 --circle 256,256,2.5 --ext 6 --inner 8
 
 Needs the reference tree and ``make -C oracle ref``.  Per level l the archive holds the sorted
 Morton codes and flag_status of its nodes; per refined level the explosion targets (the
@@ -34,19 +36,27 @@ def main(argv=None):
     ap.add_argument("--n", default="256,128,128")
     ap.add_argument("--levels", type=int, default=2)
     ap.add_argument("--cube", default="80,64,64,16")
+    ap.add_argument("--circle", default=None, help="cx,cy,r: a 2D grid refined around a circle")
     ap.add_argument("--ext", default="6")
     ap.add_argument("--inner", default="16")
     a = ap.parse_args(argv)
     if not os.path.exists(REF_RUN):
         subprocess.run(["make", "-C", HERE, "ref"], check=True)
-    meta = {"dims": 3, "n": [int(v) for v in a.n.split(",")], "levels": a.levels, "cube": a.cube,
-            "ext": a.ext, "inner": a.inner}
+    dims = 2 if a.circle else 3
+    meta = {"dims": dims, "n": [int(v) for v in a.n.split(",")], "levels": a.levels, "ext": a.ext, "inner": a.inner}
+    if a.circle:
+        meta["circle"] = a.circle
+        geo = f"geo=circle:{a.circle}"
+        bcs = ["bc=xmin:neq:0.04,0", "bc=xmax:neq:0.04,0", "bc=ymin:bb", "bc=ymax:bb"]
+    else:
+        meta["cube"] = a.cube
+        geo = f"geo=cube:{a.cube}"
+        bcs = ["bc=xmin:neq:0.05,0,0", "bc=xmax:neq:0.05,0,0", "bc=ymin:bb", "bc=ymax:bb", "bc=zmin:bb", "bc=zmax:bb"]
     with tempfile.TemporaryDirectory() as tmp:
         dump = os.path.join(tmp, "l0.bin")
-        subprocess.run([REF_RUN, "dims=3", f"n={a.n}", f"levels={a.levels}", f"geo=cube:{a.cube}", f"ext={a.ext}",
-                        f"inner={a.inner}", "coll=srt", "nu=0.01", "steps=0", f"lout0={dump}",
-                        "bc=xmin:neq:0.05,0,0", "bc=xmax:neq:0.05,0,0", "bc=ymin:bb", "bc=ymax:bb", "bc=zmin:bb",
-                        "bc=zmax:bb"], check=True, cwd=tmp, stdout=subprocess.DEVNULL)
+        subprocess.run([REF_RUN, f"dims={dims}", f"n={a.n}", f"levels={a.levels}", geo, f"ext={a.ext}",
+                        f"inner={a.inner}", "coll=srt", "nu=0.01", "steps=0", f"lout0={dump}"] + bcs,
+                       check=True, cwd=tmp, stdout=subprocess.DEVNULL)
         _, _, levels = load_levels(dump)
     out = {"meta": json.dumps(meta)}
     empty = np.zeros(0, dtype=np.uint64)

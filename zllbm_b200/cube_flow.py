@@ -8,7 +8,7 @@ CUDA graph.
     python -m zllbm_b200.cube_flow --topology cube_topology.npz [--steps 64] [--warmup 4]
 
 The node sets and interface layers come from the host's grid builder: the reference's own
-(``oracle/make_cube_topology.py`` writes them from its AmrManager::SetupMesh).  Throughput counts
+(``oracle/make_body_topology.py`` writes them from its AmrManager::SetupMesh).  Throughput counts
 every node update the reference performs: the sum over levels of nodes x 2^level per coarse
 step.
 """
