@@ -16,7 +16,6 @@ struct F2 {
 __device__ __forceinline__ F2 operator+(F2 a, F2 b) { return {__fadd2_rn(a.v, b.v)}; }
 __device__ __forceinline__ F2 operator-(F2 a, F2 b) { return {__ffma2_rn(b.v, make_float2(-1.f, -1.f), a.v)}; }
 __device__ __forceinline__ F2 operator*(F2 a, F2 b) { return {__fmul2_rn(a.v, b.v)}; }
-__device__ __forceinline__ F2 operator/(F2 a, F2 b) { return {make_float2(a.v.x / b.v.x, a.v.y / b.v.y)}; }
 __device__ __forceinline__ F2 vfma(F2 a, F2 b, F2 c) { return {__ffma2_rn(a.v, b.v, c.v)}; }
 __device__ __forceinline__ F2 splat(float s) { return {make_float2(s, s)}; }
 
