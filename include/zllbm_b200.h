@@ -241,7 +241,10 @@ int zl_mrt_matrix(int lattice, double tau, double* out);
    coordinates and velocities as the reference's GeometryVertexImmersedBoundary coordinate_ /
    velocity_ (n * 3 doubles, domain offset included), area_ (n doubles).  Every later step of the
    level starts with the direct-forcing pass (CalculateBodyForce, :35-364, delta kernel of
-   stencil half-width 2, StencilDisTwo :372-384). */
+   stencil half-width 2, StencilDisTwo :372-384).  Calling it again between steps replaces the
+   set (the reference's per-step UpdateShape of a moving geometry, or a body with prescribed
+   motion): nodes that only the previous set's stencils touched drop their force, n = 0 removes
+   the boundary, and a captured graph is rebuilt on the next zl_advance. */
 int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordinates, const double* velocity,
                        const double* area);
 

@@ -267,10 +267,26 @@ def main():
             nbr = np.fromfile(fout, dtype=np.uint64).reshape(codes.size, 2 * dims)
             np.savez_compressed(os.path.join(HERE, f"morton_{dims}d.npz"), codes=codes, neighbors=nbr)
             print("morton", dims, codes.size)
+    run_topologies()
+
+
+# small grids refined around a body (the reference's own grid builder) for the multi-level flow drivers
+TOPO_CASES = {
+    "topo_cube_small": ["--n", "48,32,32", "--levels", "2", "--cube", "16,16,16,4", "--ext", "2", "--inner", "4"],
+    "topo_cylinder_small": ["--n", "96,48", "--levels", "2", "--circle", "24,24,1.5", "--ext", "3", "--inner", "3"],
+}
+
+
+def run_topologies():
+    for name, args in TOPO_CASES.items():
+        subprocess.run([sys.executable, os.path.join(ROOT, "oracle", "make_body_topology.py"),
+                        os.path.join(HERE, f"{name}.npz")] + args, check=True)
 
 
 if __name__ == "__main__":
-    if sys.argv[1:] == ["vtu"]:
+    if sys.argv[1:] == ["topo"]:
+        run_topologies()
+    elif sys.argv[1:] == ["vtu"]:
         if not os.path.exists(REF_RUN):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
         with tempfile.TemporaryDirectory() as tmp:

@@ -298,6 +298,9 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     const int dims = ctx->dims, q = ctx->q;
     Level& L = ctx->levels[level];
     L.active = false;
+    // the vertex set and its node list index the old box
+    L.n_vertices = 0;
+    L.n_ib_nodes = 0;
     ++ctx->generation;
 
     DeviceBuffer dcodes, dminmax;
@@ -469,7 +472,6 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
         ZL_CUDA(ctx, cudaMemset(L.force.ptr, 0, (size_t)cells * 3 * sizeof(double)));
         p.force = (const double*)L.force.ptr;
     }
-    L.n_vertices = 0;
     std::vector<double> feq_face(6 * q, 0.);
     for (int f = 0; f < 2 * dims; ++f) host_feq(dims, ctx->cfg.rho0, ctx->cfg.bc_velocity[f], &feq_face[f * q]);
     if ((rc = alloc(ctx, L.feq_face, feq_face.size() * sizeof(double)))) return rc;
@@ -1180,6 +1182,16 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
     if (!ctx->cfg.forcing) return fail(ctx, ZL_ESTATE, "immersed boundaries need config->forcing = 1");
     if (n < 0 || (n > 0 && (!coordinates || !velocity || !area))) return fail(ctx, ZL_EINVAL, "bad vertex arrays");
     Level& L = ctx->levels[level];
+    // the level has no vertex set (its pass does not run) unless this call completes
+    struct Incomplete {
+        Level& L;
+        bool done = false;
+        ~Incomplete() {
+            if (!done) L.n_vertices = 0;
+        }
+    } guard{L};
+    L.n_vertices = 0;
+    ++ctx->generation;
     if ((rc = alloc(ctx, L.ib_coord, (size_t)n * 3 * 8)) || (rc = alloc(ctx, L.ib_uvel, (size_t)n * 3 * 8)) ||
         (rc = alloc(ctx, L.ib_area, (size_t)n * 8)) || (rc = alloc(ctx, L.ib_force, (size_t)n * 3 * 8)) ||
         (rc = alloc(ctx, L.ib_total, 3 * 8)))
@@ -1193,10 +1205,20 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         ZL_CUDA(ctx, cudaMemset(L.ib_force.ptr, 0, (size_t)n * 3 * 8));
     }
     L.n_vertices = (int)n;
-    ++ctx->generation;
     // every stencil node must exist on the level (the reference logs an error otherwise); the
-    // distinct stencil cells become the node list of the pass's first launch
+    // distinct stencil cells become the node list of the pass's first launch.  Nodes of the
+    // previous list that no new stencil touches drop their force (all of them when the new set
+    // is empty or rejected).
+    const int old_nodes = L.n_ib_nodes;
     L.n_ib_nodes = 0;
+    auto release = [&](const void* mark) -> int {
+        if (old_nodes <= 0 || !L.force.ptr) return ZL_OK;
+        ib_release_kernel<<<(unsigned)((old_nodes + 255) / 256), 256, 0, ctx->stream>>>(
+            (const int*)L.ib_nodes.ptr, old_nodes, (const uint32_t*)mark, (double*)L.force.ptr);
+        ZL_CUDA(ctx, cudaGetLastError());
+        return ZL_OK;
+    };
+    if (n == 0 && (rc = release(nullptr))) return rc;
     if (n > 0) {
         IbVertices v = ib_view(ctx, L, level);
         if ((rc = reset_flag(ctx))) return rc;
@@ -1218,9 +1240,10 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         int bad = 0;
         if ((rc = read_flag(ctx, &bad))) return rc;
         if (bad) {
-            L.n_vertices = 0;
+            if ((rc = release(nullptr))) return rc;
             return fail(ctx, ZL_ETOPOLOGY, "level %d: an immersed-boundary stencil node is not on the level", level);
         }
+        if ((rc = release(mark.ptr))) return rc;
         size_t tmp_bytes = 0;
         ZL_CUDA(ctx, select_marked((const uint32_t*)mark.ptr, (int)cells, (int*)sel.ptr, (int*)count.ptr, nullptr,
                                    &tmp_bytes, ctx->stream));
@@ -1235,6 +1258,7 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         L.n_ib_nodes = nodes;
     }
+    guard.done = true;
     return ZL_OK;
 }
 

@@ -92,8 +92,9 @@ def run(topology: str, steps: int = 64, warmup: int = 4, graph: bool = True, bat
     drag = ctx.ib_get_forces(levels)[1]
     mass = [float(ctx.conservation(lv)[0]) for lv in range(levels + 1)]
     ctx.close()
-    res = {"workload": "D3Q19 SRT + Smagorinsky (Cs 0.1) flow past a cube, coarse 256x128x128, "
-                       f"{levels} refinement levels (1:2:4 sub-cycling), inflow {U_IN}, convective outflow, "
+    res = {"workload": "D3Q19 SRT + Smagorinsky (Cs 0.1) flow past a cube, "
+                       f"coarse {'x'.join(str(v) for v in meta['n'])}, {levels} refinement levels "
+                       f"({':'.join(str(1 << lv) for lv in range(levels + 1))} sub-cycling), inflow {U_IN}, convective outflow, "
                        f"Re {RE:.0f}, FP32, immersed-boundary cube ({nv} vertices)",
            "batched_level_steps": batching, "cuda_graph": graph,
            "nodes_per_level": nodes, "lups_per_coarse_step": lups_per_step, "coarse_steps": steps,

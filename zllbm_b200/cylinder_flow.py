@@ -75,8 +75,11 @@ def run(topology: str, steps: int = 400, warmup: int = 8, graph: bool = True, ba
     ms = a.elapsed_time(b)
     force = ctx.ib_get_forces(levels)[1]
     ctx.close()
-    res = {"workload": f"D2Q9 MRT flow past a cylinder (D = 40 finest cells, {VERTICES} immersed-boundary vertices), "
-                       f"coarse 1024x512, {levels} refinement levels (1:2:4:8 sub-cycling), inflow {U_IN}, "
+    diameter = 2.0 * float(meta["circle"].split(",")[2]) * (1 << levels)
+    cycles = ":".join(str(1 << lv) for lv in range(levels + 1))
+    res = {"workload": f"D2Q9 MRT flow past a cylinder (D = {diameter:g} finest cells, {VERTICES} immersed-boundary "
+                       f"vertices), coarse {'x'.join(str(v) for v in meta['n'])}, {levels} refinement levels "
+                       f"({cycles} sub-cycling), inflow {U_IN}, "
                        f"convective outflow, Re {RE:.0f}, FP32",
            "batched_level_steps": batching, "cuda_graph": graph,
            "nodes_per_level": nodes, "lups_per_coarse_step": lups_per_step, "coarse_steps": steps,
