@@ -5,14 +5,64 @@ refined by the reference's own grid builder (tests/golden/topo_*_small.npz, writ
 
 Each runs a few coarse steps as batched launches replayed from a CUDA graph and again launch by
 launch; the body forces and level masses agree (FP32 storage, node forces spread with atomics, so
-to a relative 1e-4) and stay finite.
+to a relative 1e-4) and stay finite.  Without a GPU: the fixtures' interface layers lie in their
+levels, and every stencil node of the drivers' body vertices exists on the finest level.
 """
+import itertools
+import json
+import math
 import os
 
 import numpy as np
 import pytest
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+TOPOS = ("topo_cube_small", "topo_cylinder_small")
+
+
+def load_topo(name):
+    z = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    return json.loads(str(z["meta"])), z
+
+
+def body_vertices(meta):
+    from zllbm_b200.cube_flow import cube_vertices
+    from zllbm_b200.cylinder_flow import VERTICES
+    h = 1.0 / (1 << meta["levels"])
+    if "cube" in meta:
+        cx, cy, cz, edge = (float(v) for v in meta["cube"].split(","))
+        return cube_vertices((cx, cy, cz), edge, h)[0]
+    cx, cy, r = (float(v) for v in meta["circle"].split(","))
+    t = 2.0 * math.pi * np.arange(VERTICES) / VERTICES
+    return np.stack([cx + r * np.cos(t), cy + r * np.sin(t), np.zeros(VERTICES)], axis=1)
+
+
+@pytest.mark.parametrize("name", TOPOS)
+def test_topology_fixture_layers_are_consistent(name):
+    meta, z = load_topo(name)
+    for lv in range(meta["levels"] + 1):
+        codes = z[f"codes{lv}"]
+        assert codes.size > 0 and z[f"flags{lv}"].size == codes.size
+        assert np.all(np.diff(codes.astype(np.uint64)) > 0)  # sorted, distinct
+    for lv in range(1, meta["levels"] + 1):
+        assert z[f"c2f_fine{lv}"].size > 0 and z[f"f2c_coarse{lv - 1}"].size > 0
+        assert np.isin(z[f"c2f_fine{lv}"], z[f"codes{lv}"]).all()
+        assert np.isin(z[f"f2c_coarse{lv - 1}"], z[f"codes{lv - 1}"]).all()
+
+
+@pytest.mark.parametrize("name", TOPOS)
+def test_every_body_stencil_node_is_on_the_finest_level(name):
+    """The drivers put the body's vertices on the finest level; the four-point stencil of each
+    (first node (uint32)(x / dx + 1e-6) - 1 per axis) must find all its nodes there."""
+    from oracle.port import morton_decode
+    meta, z = load_topo(name)
+    dims, levels = meta["dims"], meta["levels"]
+    have = set(map(tuple, morton_decode(z[f"codes{levels}"], dims).tolist()))
+    dx = 1.0 / (1 << levels)
+    for p in body_vertices(meta):
+        first = [int(p[a] / dx + 1e-6) - 1 for a in range(dims)]
+        for o in itertools.product(range(4), repeat=dims):
+            assert tuple(first[a] + o[a] for a in range(dims)) in have
 
 
 def quiet(*_):
