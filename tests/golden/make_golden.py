@@ -94,7 +94,19 @@ AMR_CASES.update({
 })
 
 
-def run_amr(name, case, tmp):
+# one step of the reference's direct forcing from a non-uniform (Taylor-Green) velocity field, to
+# pin the oracle's interpolation: the vertex forces after the step are those of the first pass,
+# which reads the initial populations
+IB_PIN_CASES = {
+    "ib2d": dict(dims=2, n=(40, 32), levels=0, ib="circle:20.5,16.5,3", ext=3, inner=2, coll="srt", nu=0.02,
+                 bc=["xmin:per", "xmax:per", "ymin:per", "ymax:per"], steps=1, init="tgv", u0=0.05),
+    "ib3d": dict(dims=3, n=(20, 16, 16), levels=0, ib="sphere:10.2,8.1,7.9,2.5", ext=2, inner=1, coll="srt",
+                 nu=0.03, bc=["xmin:per", "xmax:per", "ymin:per", "ymax:per", "zmin:per", "zmax:per"], steps=1,
+                 init="tgv", u0=0.05),
+}
+
+
+def run_amr(name, case, tmp, prefix="amr"):
     from oracle.port import load_levels
     wd = os.path.join(tmp, name)
     os.makedirs(wd, exist_ok=True)
@@ -102,7 +114,7 @@ def run_amr(name, case, tmp):
             f"coll={case['coll']}", f"nu={case['nu']!r}", f"steps={case['steps']}",
             "lout0=" + os.path.join(wd, "l0.bin"), "lout=" + os.path.join(wd, "l1.bin")] + \
            [f"bc={b}" for b in case["bc"]]
-    for key in ("geo", "ib", "ext", "inner", "cforce"):
+    for key in ("geo", "ib", "ext", "inner", "cforce", "init", "u0"):
         if key in case:
             args.append(f"{key}={case[key]}")
     if "ib" in case:
@@ -129,7 +141,7 @@ def run_amr(name, case, tmp):
             raw = open(os.path.join(wd, fn), "rb").read()
             nv = int(np.frombuffer(raw[:8], np.int64)[0])
             out[f"vertices_{tag}"] = np.frombuffer(raw[8:], np.float64, count=nv * 10).reshape(nv, 10)
-    np.savez_compressed(os.path.join(HERE, f"amr_{name}.npz"), **out)
+    np.savez_compressed(os.path.join(HERE, f"{prefix}_{name}.npz"), **out)
     print(name, [len(l["nodes"]) for l in before], "nodes per level")
 
 
@@ -244,6 +256,7 @@ def main():
             print(name, before.size, "nodes")
         for name, case in AMR_CASES.items():
             run_amr(name, case, tmp)
+        run_ib_pins(tmp)
         for name in CKPT_CASES:
             run_checkpoint(name, AMR_CASES[name], tmp)
         for name, case in VTU_CASES.items():
@@ -283,9 +296,19 @@ def run_topologies():
                         os.path.join(HERE, f"{name}.npz")] + args, check=True)
 
 
+def run_ib_pins(tmp):
+    for name, case in IB_PIN_CASES.items():
+        run_amr(name, case, tmp, prefix="ibpin")
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["topo"]:
         run_topologies()
+    elif sys.argv[1:] == ["ibpin"]:
+        if not os.path.exists(REF_RUN):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            run_ib_pins(tmp)
     elif sys.argv[1:] == ["vtu"]:
         if not os.path.exists(REF_RUN):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
