@@ -53,3 +53,18 @@ def test_box_codes_helper():
     c = zl.box_codes(3, (1, 2, 3), (4, 5, 6))
     idx = morton_decode(c, 3)
     assert idx[0].tolist() == [1, 2, 3] and idx[1].tolist() == [2, 2, 3] and idx[-1].tolist() == [4, 5, 6]
+
+
+def test_missing_library_fails_loudly(monkeypatch, tmp_path):
+    monkeypatch.setattr(zl, "_lib", None)
+    with pytest.raises(RuntimeError, match="not built"):
+        zl.load_library(str(tmp_path / "libzllbm_b200.so"))
+
+
+def test_no_cpu_fallback_without_a_gpu():
+    """With no CUDA device the solver refuses to start instead of computing on the host."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(zl.ZlError):
+        zl.Context(zl.SolverConfig(domain_min=(1, 1, 1), domain_max=(8, 8, 8)))
