@@ -138,8 +138,8 @@ __global__ void ib_mark_kernel(LevelGeom geo, LevelMap m, IbVertices v, uint32_t
 // new set's stencils do not (all of them when mark is null) drop the force they last received.
 // The reference resets only the nodes of the current stencils (immersed_boundary.cpp:157-167),
 // which never differ from the previous ones because its shapes move no vertex.
-static __global__ void ib_release_kernel(const int* __restrict__ nodes, int n_nodes, const uint32_t* __restrict__ mark,
-                                  double* __restrict__ node_force) {
+static __global__ void ib_release_kernel(const int* __restrict__ nodes, int n_nodes,
+                                         const uint32_t* __restrict__ mark, double* __restrict__ node_force) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n_nodes) return;
     const long long cell = nodes[t];
