@@ -7,7 +7,9 @@ interpolation for the tests:
   * `delta_three`: the three-point kernel of Roma, Peskin and Berger (J. Comput. Phys. 153,
     1999), which the reference does not have;
   * `vertex_forces`: F = 2 (U_b - sum delta u) (immersed_boundary.cpp:183-184, :318-320) with
-    the stencil placement of each width.
+    the stencil placement of each width;
+  * `spread`: node force += F delta area / (dt dx^(d-1)) over the same stencil
+    (immersed_boundary.cpp:186-199, :322-339).
 """
 from __future__ import annotations
 
@@ -65,3 +67,21 @@ def vertex_forces(u_of, coords, vel, dx: float, width: int, dims: int = 2):
                         acc += u_of(jx, jy, jz) * (wx * wy * wz)
         out[i, :dims] = 2.0 * (np.asarray(ub[:dims]) - acc[:dims])
     return out
+
+
+def spread(forces, coords, area, dx: float, dt: float, width: int, dims: int, add):
+    """Share of every vertex force on its stencil nodes: add(node indices, share[3]) is called once
+    per (vertex, stencil node), share = F * (delta * area / (dt dx^(d-1)))."""
+    for c, force, a in zip(coords, forces, area):
+        axes = [stencil(c[k] / dx, width) for k in range(dims)]
+        scale = a / dt / dx if dims == 2 else a / dt / dx / dx
+        force = np.asarray(force, dtype=np.float64)
+        if dims == 2:
+            for jy, wy in zip(*axes[1]):
+                for jx, wx in zip(*axes[0]):
+                    add((int(jx), int(jy)), force * (wx * wy * scale))
+        else:
+            for jz, wz in zip(*axes[2]):
+                for jy, wy in zip(*axes[1]):
+                    for jx, wx in zip(*axes[0]):
+                        add((int(jx), int(jy), int(jz)), force * (wx * wy * wz * scale))

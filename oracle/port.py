@@ -93,6 +93,7 @@ class ZlpLevel(ctypes.Structure):
         ("les_cs", ctypes.c_double),
         ("has_force", ctypes.c_int),
         ("force", ctypes.c_double * 3),
+        ("node_force", ctypes.POINTER(ctypes.c_double)),
     ]
 
 
@@ -111,6 +112,7 @@ class LevelConfig:
     les: int = 0
     les_cs: float = 0.16
     force: tuple | None = None
+    node_force: np.ndarray | None = None  # (nodes, 3) float64 in grid order, added to `force`
     extra: dict = field(default_factory=dict)
 
     @property
@@ -137,6 +139,10 @@ class LevelConfig:
         if self.force is not None:
             for a in range(len(self.force)):
                 c.force[a] = float(self.force[a])
+        if self.node_force is not None:
+            nf = self.node_force
+            assert nf.dtype == np.float64 and nf.flags.c_contiguous and nf.shape[-1] == 3
+            c.node_force = nf.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
         return c
 
     def harness_args(self) -> list:

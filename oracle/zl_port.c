@@ -387,7 +387,16 @@ int zlp_run(const zlp_level* c, double* f, double* fc, int steps) {
     const int nz = c->dims == 3 ? c->n[2] : 1;
     const long nn = (long)c->n[0] * c->n[1] * nz;
     for (int step = 0; step < steps; ++step) {
-        for (long i = 0; i < nn; ++i) collide_node(&l, c, dt, tau0, mrt_s, mrt_d, f + i * q, fc + i * q);
+        for (long i = 0; i < nn; ++i) {
+            if (c->node_force) {
+                zlp_level cn = *c;
+                cn.has_force = 1;
+                for (int a = 0; a < 3; ++a) cn.force[a] = (c->has_force ? c->force[a] : 0.) + c->node_force[i * 3 + a];
+                collide_node(&l, &cn, dt, tau0, mrt_s, mrt_d, f + i * q, fc + i * q);
+            } else {
+                collide_node(&l, c, dt, tau0, mrt_s, mrt_d, f + i * q, fc + i * q);
+            }
+        }
         for (int z = 0; z < nz; ++z)
             for (int y = 0; y < c->n[1]; ++y)
                 for (int x = 0; x < c->n[0]; ++x) {

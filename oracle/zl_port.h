@@ -38,6 +38,10 @@ typedef struct zlp_level {
     double les_cs;       /* Smagorinsky constant (the reference hard-wires 0.16) */
     int has_force;       /* constant body force (Guo forcing) */
     double force[3];
+    /* per-node force (GridNodeLbm::force_ of one force group, nodes x 3, x y z) added to the
+       constant force in the collision (GetAllForcesForANode, lbm_solver_interface.cpp:132-144);
+       NULL: none.  The boundary faces see the constant force only. */
+    const double* node_force;
 } zlp_level;
 
 /* Advance `steps` time steps in place.  f is the post-stream state (the
