@@ -1,5 +1,6 @@
 """CPU tests of the C ABI library: it loads, exports every declared symbol, validates arguments."""
 import ctypes
+import os
 
 import numpy as np
 import pytest
@@ -68,3 +69,30 @@ def test_no_cpu_fallback_without_a_gpu():
         pytest.skip("a GPU is present")
     with pytest.raises(zl.ZlError):
         zl.Context(zl.SolverConfig(domain_min=(1, 1, 1), domain_max=(8, 8, 8)))
+
+
+@pytest.mark.parametrize("compiler,std", [("gcc", "-std=c99"), ("g++", "-std=c++17")])
+def test_header_is_plain_c_and_links(tmp_path, compiler, std):
+    """The boundary a host binds: the header compiles as C99 and as C++, and a program linked
+    against the library calls it (no device work: the ABI version and a rejected config)."""
+    import shutil
+    import subprocess
+    if shutil.which(compiler) is None:
+        pytest.skip(f"{compiler} not found")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    lib_dir = os.path.join(root, "zllbm_b200")
+    src = tmp_path / ("probe.c" if compiler == "gcc" else "probe.cpp")
+    src.write_text(
+        '#include <stdio.h>\n#include <string.h>\n#include "zllbm_b200.h"\n'
+        "int main(void) {\n"
+        "    zl_config cfg;\n"
+        "    zl_ctx* ctx = NULL;\n"
+        "    memset(&cfg, 0, sizeof(cfg));\n"
+        "    cfg.lattice = 5;\n"
+        '    printf("%d %d %d\\n", zl_abi_version(), ZL_ABI_VERSION, zl_create(&cfg, &ctx) != ZL_OK && ctx == NULL);\n'
+        "    return 0;\n}\n")
+    exe = tmp_path / "probe"
+    subprocess.run([compiler, std, "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src), "-o", str(exe),
+                    "-L", lib_dir, "-lzllbm_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    assert out == ["1", "1", "1"]
