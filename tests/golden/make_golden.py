@@ -11,7 +11,12 @@ node (reference order: sorted codes) and the populations before and after
 holds codes and the reference's FindXNeg/FindXPos/... results for them.  ``vtu_<name>.npz``
 holds the .vtu/.pvtu files the reference's own VTK writer produced after a run (binary and
 ASCII), with each level's codes, flags, populations and node member rho_ at that time
-(``python tests/golden/make_golden.py vtu`` regenerates only those).
+(``python tests/golden/make_golden.py vtu`` regenerates only those).  ``amr_<name>.npz`` holds
+multi-level and immersed-boundary runs with their interface layers and vertex records,
+``ckpt_<name>.npz`` the reference's checkpoint files (``checkpoints``), ``ibpin_<name>.npz`` one
+immersed-boundary step from a Taylor-Green field (``ibpin``), and ``topo_*_small.npz`` small grids
+refined around a body by the reference's grid builder (``topo``); the word in brackets is the
+argument that regenerates only that group.
 """
 from __future__ import annotations
 
