@@ -330,6 +330,7 @@ def run_ours(args):
         for _ in range(args.warmup):
             ctx.step_level(0)
     ctx.synchronize()
+    mass_before = ctx.conservation(0)[0]  # outside the timed region
 
     barrier(dist)
     torch.cuda.synchronize()
@@ -423,6 +424,7 @@ def run_ours(args):
             "gpu_launches": args.steps,
             "clocks": clocks.summary(),
             "mass_after": mass,
+            "mass_drift": (mass - mass_before) / mass_before,
         }
         if variants:
             out["storage_variants"] = variants
