@@ -98,3 +98,17 @@ def test_cylinder_flow_graph_matches_plain():
     fast = cylinder_flow.run(topo, steps=6, warmup=2, graph=True, batching=True, log=quiet)
     plain = cylinder_flow.run(topo, steps=6, warmup=2, graph=False, batching=False, log=quiet)
     check_pair(fast, plain)
+
+
+def test_cube_surface_vertices():
+    """Host geometry of the cube-flow driver: every grid point of the six faces once, on the
+    surface, with areas summing to the cube's surface."""
+    from zllbm_b200.cube_flow import cube_vertices
+    edge, h, centre = 4.0, 0.25, np.array([16.0, 16.0, 16.0])
+    xyz, area = cube_vertices(tuple(centre), edge, h)
+    m = int(edge / h)
+    assert len(xyz) == (m + 1) ** 3 - (m - 1) ** 3  # surface points of an (m+1)^3 lattice cube
+    assert len(np.unique(np.round(xyz / h).astype(np.int64), axis=0)) == len(xyz)
+    d = np.abs(xyz - centre)
+    assert np.all(np.isclose(d.max(1), edge / 2))  # on the surface
+    assert area.sum() == pytest.approx(6 * edge * edge, rel=1e-12)
