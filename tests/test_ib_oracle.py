@@ -73,3 +73,19 @@ def test_one_forced_step_matches_reference(name, port):
     # node forces sum the vertex shares in another order than the reference's unordered_map walk:
     # populations agree to an ulp (about 3e-17 here), not bit for bit
     np.testing.assert_allclose(f[lin], z["f_after0"], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["amr_ib2d_l0", "amr_ib2d_l1", "ibpin_ib2d"])
+def test_reference_circle_vertex_count_and_arc(name):
+    """The reference's circle (geometry_default_shape_2d.cpp:34) has floor(2 pi r / dx_l) + 1
+    vertices on its level, each with arc 2 pi r / count (UpdateShape), placed on the circle."""
+    import math
+    z = np.load(os.path.join(HERE, "golden", f"{name}.npz"))
+    meta = json.loads(str(z["meta"]))
+    r = float(meta["ib"].split(":")[1].split(",")[2])
+    dx = 1.0 / (1 << meta["levels"])
+    v = z["vertices_before"]
+    assert len(v) == math.floor(2 * math.pi * r / dx) + 1
+    np.testing.assert_allclose(v[:, 6], 2 * math.pi * r / len(v), rtol=1e-12)
+    rad = np.hypot(v[:, 0] - v[:, 0].mean(), v[:, 1] - v[:, 1].mean())
+    np.testing.assert_allclose(rad, r, rtol=1e-9)
