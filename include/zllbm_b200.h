@@ -128,7 +128,11 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
 /* Write / read the post-stream populations f_ (GridNodeLbm::f_, lbm_interface.h:37) of the
    nodes with the given codes; f holds n * q doubles, node-major.  On periodic axes the
    reference stores the maximum plane as a duplicate of the minimum plane
-   (grid/grid_manager3d.cpp:106-112); both codes address the same device node.  The device
+   (grid/grid_manager3d.cpp:106-112); both codes address the same device node, which is stored
+   once.  zl_set_populations writes that node from the minimum-plane code only and ignores the
+   maximum-plane row (the reference keeps the two copies equal; if a caller's copies disagree,
+   the minimum-plane copy is kept); zl_get_populations returns the node's values for both codes.
+   The device
    staging of these calls (and of zl_get_macros) grows to the largest exchange and stays with the
    context until zl_destroy, so repeated exchanges allocate nothing. */
 int zl_set_populations(zl_ctx* ctx, int level, const uint64_t* codes, const double* f, int64_t n);

@@ -30,16 +30,23 @@ ZL_HD uint64_t morton_encode(const uint32_t* idx, int dims) {
     return code;
 }
 
-__device__ __forceinline__ bool code_to_node(uint64_t code, const LevelMap& m, Coord& c) {
+// `folded` (optional) is set when the code lies on the duplicated maximum plane of a periodic
+// axis and was folded onto coordinate 0.
+__device__ __forceinline__ bool code_to_node(uint64_t code, const LevelMap& m, Coord& c, bool* folded = nullptr) {
     uint32_t idx[3];
     morton_decode(code, m.dims, idx);
     c.x[2] = 0;
+    bool fold = false;
     for (int a = 0; a < m.dims; ++a) {
         int v = (int)idx[a] - m.lo[a];
-        if (m.periodic[a] && v == m.n[a]) v = 0;
+        if (m.periodic[a] && v == m.n[a]) {
+            v = 0;
+            fold = true;
+        }
         if (v < 0 || v >= m.n[a]) return false;
         c.x[a] = v;
     }
+    if (folded) *folded = fold;
     return true;
 }
 
@@ -402,10 +409,15 @@ __global__ void scatter_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, L
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= n) return;
     Coord c;
-    if (!code_to_node(codes[i], m, c)) {
+    bool folded = false;
+    if (!code_to_node(codes[i], m, c, &folded)) {
         atomicExch(bad, 1);
         return;
     }
+    // A periodic axis stores its duplicated maximum plane once, at coordinate 0.  Only the
+    // minimum-plane code writes that node; the maximum-plane copy is ignored, so the result
+    // does not depend on which of two disagreeing copies a thread happens to write last.
+    if (folded) return;
     for (int q = 0; q < L::kQ; ++q) {
         double v = fin[i * L::kQ + q];
         if constexpr (St::kDeviation) v -= Tables<L>::w(q);

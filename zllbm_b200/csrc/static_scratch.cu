@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 #include <mutex>
 #include "zllbm_b200.h"
+#include "lattice.cuh"
 
 namespace {
 
@@ -27,38 +28,28 @@ static __device__ __align__(256) double g_moment_scratch[kMaxBlocks * 4];
 
 namespace {
 
-__global__ void __launch_bounds__(kThreads) moments_partial_static(const double* __restrict__ f, long long n, int q,
-                                                                   int dims, double* __restrict__ partial) {
+// Per-block partial sums of rho, jx, jy, jz over kNodesPerBlock nodes; the direction tables
+// are compile-time constants of the lattice (reference direction order), folded after unrolling.
+template <class L>
+__global__ void __launch_bounds__(kThreads) moments_partial_static(const double* __restrict__ f, long long n,
+                                                                   double* __restrict__ partial) {
+    using Tb = zl::Tables<L>;
+    constexpr int Q = L::kQ;
     __shared__ double red[4][kThreads / 32];
     const long long first = (long long)blockIdx.x * kNodesPerBlock;
     const long long last = first + kNodesPerBlock < n ? first + kNodesPerBlock : n;
     double acc[4] = {0., 0., 0., 0.};
     for (long long i = first + threadIdx.x; i < last; i += kThreads) {
-        const double* node = f + i * q;
-        for (int k = 0; k < q; ++k) {
+        const double* node = f + i * Q;
+#pragma unroll
+        for (int k = 0; k < Q; ++k) {
             const double v = node[k];
-            // lattice velocities in the reference's direction order
-            int cx, cy, cz = 0;
-            if (q == 9) {
-                const int tx[9] = {0, 1, 0, -1, 0, 1, -1, -1, 1};
-                const int ty[9] = {0, 0, 1, 0, -1, 1, 1, -1, -1};
-                cx = tx[k];
-                cy = ty[k];
-            } else {
-                const int tx[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, 1, -1, 1, -1, 1, -1, 0, 0, 0, 0};
-                const int ty[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, -1, 1, -1};
-                const int tz[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, -1, -1, 1, 1, -1, -1};
-                cx = tx[k];
-                cy = ty[k];
-                cz = tz[k];
-            }
             acc[0] += v;
-            acc[1] += cx * v;
-            acc[2] += cy * v;
-            acc[3] += cz * v;
+            if (Tb::cx(k)) acc[1] += Tb::cx(k) > 0 ? v : -v;
+            if (Tb::cy(k)) acc[2] += Tb::cy(k) > 0 ? v : -v;
+            if (Tb::cz(k)) acc[3] += Tb::cz(k) > 0 ? v : -v;
         }
     }
-    (void)dims;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
@@ -112,12 +103,20 @@ extern "C" int zl_moments_noalloc(int lattice, const double* f_device, int64_t n
     double* partial = nullptr;
     const int rc = scratch_address(&partial);
     if (rc != ZL_OK) return rc;
-    const int q = lattice == ZL_D2Q9 ? 9 : 19;
     const int blocks = (int)((n + kNodesPerBlock - 1) / kNodesPerBlock);
     cudaStream_t s = static_cast<cudaStream_t>(stream);
-    moments_partial_static<<<blocks, kThreads, 0, s>>>(f_device, n, q, lattice, partial);
-    if (cudaGetLastError() != cudaSuccess) return ZL_EDEVICE;
-    moments_final_static<<<1, 32, 0, s>>>(partial, blocks, out_device);
-    if (cudaGetLastError() != cudaSuccess) return ZL_EDEVICE;
+    // cudaLaunchKernel returns the status of this launch only; the runtime's last-error slot,
+    // which may hold an earlier unrelated failure of the caller, is neither read nor cleared.
+    const void* partial_fn = lattice == ZL_D2Q9 ? (const void*)moments_partial_static<zl::D2Q9>
+                                                 : (const void*)moments_partial_static<zl::D3Q19>;
+    long long nn = n;
+    void* partial_args[] = {(void*)&f_device, (void*)&nn, (void*)&partial};
+    if (cudaLaunchKernel(partial_fn, dim3(blocks), dim3(kThreads), partial_args, 0, s) != cudaSuccess)
+        return ZL_EDEVICE;
+    const double* partial_in = partial;
+    int nb = blocks;
+    void* final_args[] = {(void*)&partial_in, (void*)&nb, (void*)&out_device};
+    if (cudaLaunchKernel((const void*)moments_final_static, dim3(1), dim3(32), final_args, 0, s) != cudaSuccess)
+        return ZL_EDEVICE;
     return ZL_OK;
 }
