@@ -280,3 +280,69 @@ def test_two_nodes_per_thread_kernel_even_rows(coll, storage, tol, port):
         else:
             ue, ug = velocity(meta, f1), velocity(meta, got)
             assert np.linalg.norm(ug - ue) / np.linalg.norm(ue) <= tol
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage,tol", [(2, 5e-3), (3, 5e-2)])
+@pytest.mark.parametrize("coll", ["mrt", "srt"])
+@pytest.mark.parametrize("n", [(129, 9, 8), (257, 8, 8)])
+def test_row_kernel(n, coll, storage, tol, port):
+    """The one-warp-per-row kernel (128- and 256-node periodic rows, 1, 2 and 4 rows per block,
+    the last block partly empty) against the oracle restatement after 13 steps (same tolerances
+    as the scalar kernel) and against the two-nodes-per-thread kernel after two steps, bit for
+    bit on the nodes whose populations depend only on rows the pair kernel updates with the same
+    packed collision (its wrapped edge rows take the scalar kernel, which rounds differently)."""
+    import zllbm_b200 as zl
+    from fixtures import grid_order, solver_config
+    from oracle.port import BC_PERIODIC, MRT, SRT, LevelConfig, morton_decode, tgv_init
+    from test_gpu_parity import velocity
+    cfg = LevelConfig(dims=3, n=n, collision=MRT if coll == "mrt" else SRT, nu=0.05 / 3,
+                      bc_kind=(BC_PERIODIC,) * 6)
+    steps = 13
+    f = np.ascontiguousarray(tgv_init(cfg, 0.05, port).reshape(-1, cfg.q))
+    codes = zl.box_codes(3, [1, 1, 1], list(cfg.n))
+    lin = grid_order(codes, 3, cfg.n)
+    f0 = f[lin].copy()
+    port.run(cfg, f, f.copy(), steps)
+    f1 = f[lin]
+    meta = dict(dims=3, n=list(cfg.n), collision=cfg.collision, nu=cfg.nu, rho0=cfg.rho0,
+                bc_kind=list(cfg.bc_kind), bc_vel=[list(v) for v in cfg.bc_vel], steps=steps)
+
+    def run(shape, k):
+        with zl.Context(solver_config(meta, storage)) as ctx:
+            ctx.set_level_nodes(0, codes)
+            ctx.set_populations(0, codes, f0)
+            ctx.set_block(0, *shape)
+            ctx.advance(k)
+            return ctx.get_populations(0, codes)
+
+    rows = [(zl.BLOCK_ROW, 4), (zl.BLOCK_ROW, 2), (zl.BLOCK_ROW, 1)]
+    ue = velocity(meta, f1)
+    out = [run(shape, steps) for shape in rows]
+    for got in out:
+        ug = velocity(meta, got)
+        assert np.linalg.norm(ug - ue) / np.linalg.norm(ue) <= tol
+    assert np.array_equal(out[0], out[1]) and np.array_equal(out[0], out[2])
+    # two steps (even, odd): node x's populations come from the odd-step collisions of its
+    # neighbours, whose inputs the neighbours' neighbours wrote in the even step
+    idx = morton_decode(codes, 3) - 1
+    uniq = [v - 1 for v in n]
+    inner = np.ones(len(codes), dtype=bool)
+    for a in (1, 2):
+        inner &= (idx[:, a] >= 3) & (idx[:, a] <= uniq[a] - 4)
+    assert inner.sum() >= uniq[0]
+    pair2 = run((-64, 1), 2)
+    row2 = run(rows[0], 2)
+    assert np.array_equal(row2[inner], pair2[inner])
+
+
+@pytest.mark.gpu
+def test_row_kernel_refused_where_it_does_not_apply():
+    import zllbm_b200 as zl
+    from fixtures import load_lbm, solver_config
+    meta, codes, f0, _ = load_lbm("tgv3d_mrt")  # 10-node rows
+    for storage in (1, 2):
+        with zl.Context(solver_config(meta, storage)) as ctx:
+            ctx.set_level_nodes(0, codes)
+            with pytest.raises(zl.ZlError):
+                ctx.set_block(0, zl.BLOCK_ROW, 4)

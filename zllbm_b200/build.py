@@ -35,6 +35,31 @@ SOURCES = {
     "vtu.cu": [],
 }
 
+# The fused step and batched step kernels, one translation unit per (storage, lattice, collision,
+# part) so that they compile in parallel: (object stem, storage type, extra flags).
+STEP_STORAGES = [("f64", "double", ["-fmad=false"]), ("f32", "float", []),
+                 ("f16", "__half", []), ("bf16", "__nv_bfloat16", [])]
+STEP_LATTICES = [("d2q9", "zl::D2Q9"), ("d3q19", "zl::D3Q19")]
+STEP_COLLISIONS = [("srt", "zl::kSrt"), ("mrt", "zl::kMrt")]
+# even / odd step, then the batched step with no extension, force, LES, force + LES
+STEP_PARTS = ["even", "odd", "batch", "batch_force", "batch_les", "batch_force_les"]
+
+
+def units() -> list[tuple[str, str, list[str]]]:
+    """(source, object, flags) of every translation unit of the library."""
+    out = []
+    step_src = os.path.join(CSRC, "step_inst.cu")
+    for st, ty, flags in STEP_STORAGES:
+        for lt, lty in STEP_LATTICES:
+            for ct, cty in STEP_COLLISIONS:
+                for part, name in enumerate(STEP_PARTS):
+                    defs = [f"-DZL_STEP_S={ty}", f"-DZL_STEP_L={lty}", f"-DZL_STEP_C={cty}", f"-DZL_STEP_PART={part}"]
+                    out.append((step_src, os.path.join(BUILD, f"step_{st}_{lt}_{ct}_{name}.o"), flags + defs))
+    # the step units are the longest compiles: they come first in the job list
+    out += [(os.path.join(CSRC, src), os.path.join(BUILD, src.replace(".cu", ".o")), flags)
+            for src, flags in SOURCES.items()]
+    return out
+
 
 def nvcc() -> str:
     path = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
@@ -43,25 +68,33 @@ def nvcc() -> str:
     return path
 
 
+def _deps(obj: str) -> list[str] | None:
+    """Files the object was built from, read from the dependency file nvcc wrote beside it."""
+    d = obj[:-2] + ".d"
+    if not os.path.exists(d):
+        return None
+    text = open(d).read().replace("\\\n", " ")
+    _, _, rest = text.partition(":")
+    return rest.split()
+
+
 def _stale(target: str, deps: list[str]) -> bool:
     if not os.path.exists(target):
         return True
     t = os.path.getmtime(target)
-    return any(os.path.getmtime(d) > t for d in deps)
+    return any(not os.path.exists(d) or os.path.getmtime(d) > t for d in deps)
 
 
 def build(verbose: bool = False, extra: list[str] | None = None) -> str:
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, h) for h in os.listdir(CSRC) if h.endswith((".cuh", ".h"))]
-    headers.append(os.path.join(ROOT, "include", "zllbm_b200.h"))
     objs = []
     jobs = []
-    for src, flags in SOURCES.items():
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src.replace(".cu", ".o"))
-        objs.append(o)
-        if _stale(o, [s, __file__] + headers):
-            cmd = [nvcc()] + ARCH + COMMON + flags + (extra or []) + ["-c", s, "-o", o]
+    for src, obj, flags in units():
+        objs.append(obj)
+        deps = _deps(obj)
+        if deps is None or _stale(obj, deps + [src, __file__]):
+            cmd = ([nvcc()] + ARCH + COMMON + flags + (extra or []) +
+                   ["-MD", "-MF", obj[:-2] + ".d", "-c", src, "-o", obj])
             jobs.append(cmd)
 
     def run(cmd):

@@ -4,7 +4,7 @@
 #pragma once
 #include <cuda_runtime.h>
 #include "ib.cuh"
-#include "pair_kernel.cuh"
+#include "row_kernel.cuh"
 
 namespace zl {
 
@@ -48,6 +48,7 @@ const LaunchSet& launch_set_bf16();
 inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) {
     int bx = geo.block[0], by = geo.block[1];
     int nx = geo.n[0];
+    if (bx == kRowKernelBlockX) bx = by = 0;  // row-kernel choice: other kernels take the default shape
     if (bx < 0) {
         bx = -bx;
         nx = (nx + 1) / 2;
@@ -67,68 +68,45 @@ inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, 
     return dims == 3 && !bnd && !masked && !p.forced && !p.les && elem_bytes < 8;
 }
 
+// The one-warp-per-row kernel (row_kernel.cuh): full periodic D3Q19 boxes in 16-bit storage
+// with rows of 128 or 256 nodes, no forcing or LES.
+inline bool row_eligible(int dims, bool bnd, bool masked, const StepParams& p, int elem_bytes,
+                         const LevelGeom& geo) {
+    return pair_eligible(dims, bnd, masked, p, elem_bytes) && elem_bytes == 2 && row_kernel_width(geo) != 0;
+}
+
+// Fused step launchers of one (storage, lattice, collision, parity) and batched step launchers
+// of one (storage, lattice, collision, extensions), defined in step_launch.cuh and instantiated
+// in step_inst.cu (one translation unit per combination).
+template <class S, class L, int C, bool O>
+cudaError_t step_lco(bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s);
+template <class S, class L, int C, int X>
+cudaError_t batch_lcx(const LevelBatch& b, cudaStream_t s);
+template <class S, class L, int C>
+cudaError_t batch_lc(int ext, const LevelBatch& b, cudaStream_t s) {
+    switch (ext) {
+        case 0: return batch_lcx<S, L, C, 0>(b, s);
+        case kExtForce: return batch_lcx<S, L, C, kExtForce>(b, s);
+        case kExtLes: return batch_lcx<S, L, C, kExtLes>(b, s);
+        default: return batch_lcx<S, L, C, kExtForce | kExtLes>(b, s);
+    }
+}
+template <class S, class L, int C>
+cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,
+                    cudaStream_t s) {
+    return odd ? step_lco<S, L, C, true>(bnd, masked, f, geo, p, s) : step_lco<S, L, C, false>(bnd, masked, f, geo, p, s);
+}
+
 #define ZL_DEFINE_LAUNCH_SET(NAME, S)                                                                            \
     namespace NAME##_impl {                                                                                      \
-    template <class L, int C, bool O, bool B, bool M, int X = 0>                                                 \
-    cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {                      \
-        dim3 g, b;                                                                                               \
-        step_shape(geo, L::kDims, g, b);                                                                         \
-        aa_step_kernel<L, S, C, O, B, M, X><<<g, b, 0, s>>>(f, geo, p);                                          \
-        return cudaGetLastError();                                                                               \
-    }                                                                                                            \
-    template <class L, int C, int X>                                                                             \
-    cudaError_t step_ext(bool odd, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {            \
-        return odd ? step_one<L, C, true, true, true, X>(f, geo, p, s)                                           \
-                   : step_one<L, C, false, true, true, X>(f, geo, p, s);                                         \
-    }                                                                                                            \
-    template <int C>                                                                                             \
-    cudaError_t step_pair(bool odd, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {           \
-        if constexpr (Storage<S>::kDeviation) {                                                                  \
-            if ((geo.n[0] & 1) || (geo.stride & 1)) {                                                            \
-                /* pair accesses need an even row length and plane stride: scalar kernel instead */             \
-                LevelGeom g1 = geo;                                                                              \
-                g1.block[0] = g1.block[1] = 0;                                                                   \
-                return odd ? step_one<D3Q19, C, true, false, false>(f, g1, p, s)                                 \
-                           : step_one<D3Q19, C, false, false, false>(f, g1, p, s);                               \
-            }                                                                                                    \
-            dim3 g, b;                                                                                           \
-            step_shape(geo, 3, g, b);                                                                            \
-            if (odd) aa_pair_kernel<S, C, true><<<g, b, 0, s>>>(f, geo, p);                                      \
-            else aa_pair_kernel<S, C, false><<<g, b, 0, s>>>(f, geo, p);                                         \
-            return cudaGetLastError();                                                                           \
-        }                                                                                                        \
-        return cudaErrorInvalidValue;                                                                            \
-    }                                                                                                            \
-    template <class L, int C>                                                                                    \
-    cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p,        \
-                        cudaStream_t s) {                                                                        \
-        if (L::kDims == 3 && geo.block[0] < 0 && pair_eligible(3, bnd, masked, p, (int)sizeof(S)))               \
-            return step_pair<C>(odd, f, geo, p, s);                                                              \
-        if (p.forced || p.les) {                                                                                 \
-            if (!masked) return cudaErrorInvalidValue;                                                           \
-            if (p.forced && p.les) return step_ext<L, C, kExtForce | kExtLes>(odd, f, geo, p, s);                \
-            if (p.forced) return step_ext<L, C, kExtForce>(odd, f, geo, p, s);                                   \
-            return step_ext<L, C, kExtLes>(odd, f, geo, p, s);                                                   \
-        }                                                                                                        \
-        if (masked) {                                                                                            \
-            return odd ? step_one<L, C, true, true, true>(f, geo, p, s)                                          \
-                       : step_one<L, C, false, true, true>(f, geo, p, s);                                        \
-        }                                                                                                        \
-        if (bnd) {                                                                                               \
-            return odd ? step_one<L, C, true, true, false>(f, geo, p, s)                                         \
-                       : step_one<L, C, false, true, false>(f, geo, p, s);                                       \
-        }                                                                                                        \
-        return odd ? step_one<L, C, true, false, false>(f, geo, p, s)                                            \
-                   : step_one<L, C, false, false, false>(f, geo, p, s);                                          \
-    }                                                                                                            \
     cudaError_t step_any(int dims, int coll, bool odd, bool bnd, bool masked, void* fv, const LevelGeom& geo,    \
                          const StepParams& p, cudaStream_t s) {                                                  \
         S* f = static_cast<S*>(fv);                                                                              \
         if (dims == 2)                                                                                           \
-            return coll == kMrt ? step_lc<D2Q9, kMrt>(odd, bnd, masked, f, geo, p, s)                            \
-                                : step_lc<D2Q9, kSrt>(odd, bnd, masked, f, geo, p, s);                           \
-        return coll == kMrt ? step_lc<D3Q19, kMrt>(odd, bnd, masked, f, geo, p, s)                               \
-                            : step_lc<D3Q19, kSrt>(odd, bnd, masked, f, geo, p, s);                              \
+            return coll == kMrt ? step_lc<S, D2Q9, kMrt>(odd, bnd, masked, f, geo, p, s)                            \
+                                : step_lc<S, D2Q9, kSrt>(odd, bnd, masked, f, geo, p, s);                           \
+        return coll == kMrt ? step_lc<S, D3Q19, kMrt>(odd, bnd, masked, f, geo, p, s)                               \
+                            : step_lc<S, D3Q19, kSrt>(odd, bnd, masked, f, geo, p, s);                              \
     }                                                                                                            \
     cudaError_t neq_any(int dims, void* fv, const LevelGeom& geo, const StepParams& p, int face, int even,       \
                         const double* feq_b, cudaStream_t s) {                                                   \
@@ -244,24 +222,10 @@ inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, 
                                                              node_force, node_vel);                              \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
-    template <class L, int C>                                                                                    \
-    cudaError_t batch_lc(int ext, const LevelBatch& b, cudaStream_t s) {                                         \
-        const long long total = b.first[b.count];                                                                \
-        if (total <= 0) return cudaSuccess;                                                                      \
-        const long long want = (total + 255) / 256, cap = 148 * 6;                                               \
-        const unsigned blocks = (unsigned)(want < cap ? want : cap);                                             \
-        switch (ext) {                                                                                           \
-            case 0: aa_batch_kernel<L, S, C, 0><<<blocks, 256, 0, s>>>(b); break;                                \
-            case kExtForce: aa_batch_kernel<L, S, C, kExtForce><<<blocks, 256, 0, s>>>(b); break;                \
-            case kExtLes: aa_batch_kernel<L, S, C, kExtLes><<<blocks, 256, 0, s>>>(b); break;                    \
-            default: aa_batch_kernel<L, S, C, kExtForce | kExtLes><<<blocks, 256, 0, s>>>(b); break;             \
-        }                                                                                                        \
-        return cudaGetLastError();                                                                               \
-    }                                                                                                            \
     cudaError_t batch_any(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s) {                    \
         if (dims == 2)                                                                                           \
-            return coll == kMrt ? batch_lc<D2Q9, kMrt>(ext, b, s) : batch_lc<D2Q9, kSrt>(ext, b, s);             \
-        return coll == kMrt ? batch_lc<D3Q19, kMrt>(ext, b, s) : batch_lc<D3Q19, kSrt>(ext, b, s);               \
+            return coll == kMrt ? batch_lc<S, D2Q9, kMrt>(ext, b, s) : batch_lc<S, D2Q9, kSrt>(ext, b, s);             \
+        return coll == kMrt ? batch_lc<S, D3Q19, kMrt>(ext, b, s) : batch_lc<S, D3Q19, kSrt>(ext, b, s);               \
     }                                                                                                            \
     }                                                                                                            \
     const LaunchSet& NAME() {                                                                                    \

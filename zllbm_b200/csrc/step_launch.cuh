@@ -1,0 +1,83 @@
+// Launchers of the fused step (one parity of the AA pattern) and of the batched multi-level
+// step (one set of extensions) for one (storage, lattice, collision).  Only step_inst.cu includes this file: it is
+// compiled once per combination, each with an explicit instantiation, so the build compiles the
+// step kernel variants in parallel translation units.  The launch sets of launch.cuh call them
+// through the declarations there.
+#pragma once
+#include "launch.cuh"
+
+namespace zl {
+namespace step_impl {
+
+template <class S, class L, int C, bool O, bool B, bool M, int X = 0>
+cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {
+    dim3 g, b;
+    step_shape(geo, L::kDims, g, b);
+    aa_step_kernel<L, S, C, O, B, M, X><<<g, b, 0, s>>>(f, geo, p);
+    return cudaGetLastError();
+}
+
+template <class S, int C, bool O>
+cudaError_t step_pair(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {
+    if constexpr (Storage<S>::kDeviation) {
+        if ((geo.n[0] & 1) || (geo.stride & 1)) {
+            // pair accesses need an even row length and plane stride: scalar kernel instead
+            LevelGeom g1 = geo;
+            g1.block[0] = g1.block[1] = 0;
+            return step_one<S, D3Q19, C, O, false, false>(f, g1, p, s);
+        }
+        dim3 g, b;
+        step_shape(geo, 3, g, b);
+        aa_pair_kernel<S, C, O><<<g, b, 0, s>>>(f, geo, p);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+template <class S, int C, bool O>
+cudaError_t step_row(S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {
+    if constexpr (sizeof(S) == 2) {
+        const int v = row_kernel_width(geo);
+        const int rows = geo.block[1];
+        if (v == 0 || rows < 1 || rows > 4) return cudaErrorInvalidValue;
+        const dim3 b(32 * rows), g((geo.n[1] + rows - 1) / rows, geo.n[2]);
+        if (v == 8) aa_row_kernel<S, C, O, 8><<<g, b, 0, s>>>(f, geo, p);
+        else aa_row_kernel<S, C, O, 4><<<g, b, 0, s>>>(f, geo, p);
+        return cudaGetLastError();
+    }
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace step_impl
+
+template <class S, class L, int C, bool O>
+cudaError_t step_lco(bool bnd, bool masked, S* f, const LevelGeom& geo, const StepParams& p, cudaStream_t s) {
+    using namespace step_impl;
+    if constexpr (L::kDims == 3) {
+        if (geo.block[0] == kRowKernelBlockX && row_eligible(3, bnd, masked, p, (int)sizeof(S), geo))
+            return step_row<S, C, O>(f, geo, p, s);
+        if (geo.block[0] < 0 && pair_eligible(3, bnd, masked, p, (int)sizeof(S)))
+            return step_pair<S, C, O>(f, geo, p, s);
+    }
+    if (p.forced || p.les) {
+        if (!masked) return cudaErrorInvalidValue;
+        if (p.forced && p.les) return step_one<S, L, C, O, true, true, kExtForce | kExtLes>(f, geo, p, s);
+        if (p.forced) return step_one<S, L, C, O, true, true, kExtForce>(f, geo, p, s);
+        return step_one<S, L, C, O, true, true, kExtLes>(f, geo, p, s);
+    }
+    if (masked) return step_one<S, L, C, O, true, true>(f, geo, p, s);
+    if (bnd) return step_one<S, L, C, O, true, false>(f, geo, p, s);
+    return step_one<S, L, C, O, false, false>(f, geo, p, s);
+}
+
+template <class S, class L, int C, int X>
+cudaError_t batch_lcx(const LevelBatch& b, cudaStream_t s) {
+    const long long total = b.first[b.count];
+    if (total <= 0) return cudaSuccess;
+    const long long want = (total + kBatchThreads - 1) / kBatchThreads, cap = 148 * 6;
+    const unsigned blocks = (unsigned)(want < cap ? want : cap);
+    aa_batch_kernel<L, S, C, X><<<blocks, kBatchThreads, 0, s>>>(b);
+    return cudaGetLastError();
+}
+
+}  // namespace zl

@@ -1,6 +1,7 @@
 """Small single-kernel workloads for profiling (one launch type each, few launches).
 
-    python -m zllbm_b200.kernel_cases step --storage f16 --cells 192 [--collision mrt] [--block 128]
+    python -m zllbm_b200.kernel_cases step --storage f16 --cells 192 [--collision mrt] [--block 128|-64|row]
+        [--block-y 1]
     python -m zllbm_b200.kernel_cases learned --cells 128
     python -m zllbm_b200.kernel_cases train [--samples 151552]
 
@@ -33,7 +34,7 @@ def _events(stream, fn, reps: int, warmup: int = 2) -> float:
     return a.elapsed_time(b)
 
 
-def step_case(storage: str, cells: int, collision: str, block: int, steps: int = 6) -> float:
+def step_case(storage: str, cells: int, collision: str, block: int, steps: int = 6, block_y: int = 1) -> float:
     import torch
     from zllbm_b200.hit import box_context
     u0 = 0.05
@@ -50,11 +51,12 @@ def step_case(storage: str, cells: int, collision: str, block: int, steps: int =
         del x, y, z, p
         ctx.set_equilibrium_dense(0, rho.data_ptr(), u.data_ptr())
         if block:
-            ctx.set_block(0, block, 1)
+            ctx.set_block(0, block, block_y)
         ms = _events(ctx.stream(), lambda: ctx.step_level(0), steps)
         ctx.close()
     mlups = cells ** 3 * steps / (ms * 1e-3) / 1e6
-    print(f"step {storage} {collision} {cells}^3 block {block or 'default'}: {mlups:.0f} MLUPS", flush=True)
+    shape = "default" if not block else ("row" if block == zl.BLOCK_ROW else str(block))
+    print(f"step {storage} {collision} {cells}^3 block {shape} x {block_y}: {mlups:.0f} MLUPS", flush=True)
     return mlups
 
 
@@ -97,11 +99,15 @@ def main(argv=None):
     ap.add_argument("--storage", default="f32", choices=sorted(zl.STORAGE_NAMES))
     ap.add_argument("--collision", default="mrt", choices=["mrt", "srt"])
     ap.add_argument("--cells", type=int, default=192)
-    ap.add_argument("--block", type=int, default=0, help="block x of the step kernel (0: library default)")
+    ap.add_argument("--block", default="0",
+                    help="block x of the step kernel (0: library default; negative: two nodes per thread; "
+                         "row: one warp per x-row)")
+    ap.add_argument("--block-y", type=int, default=1, help="block y (row kernel: rows per block)")
     ap.add_argument("--samples", type=int, default=128 * 148 * 8)
     a = ap.parse_args(argv)
     if a.case == "step":
-        step_case(a.storage, a.cells, a.collision, a.block)
+        block = zl.BLOCK_ROW if a.block == "row" else int(a.block)
+        step_case(a.storage, a.cells, a.collision, block, block_y=a.block_y)
     elif a.case == "learned":
         learned_case(a.cells)
     else:
