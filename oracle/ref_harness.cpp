@@ -15,6 +15,10 @@
 //   vtu=<prefix> vtu_binary=0|1  (after stepping and rout, the reference's own field output
 //                 IoManager::OutputMeshData: folder <prefix>_data with per-level .vtu and a .pvtu)
 //   timing=1 (print wall-clock seconds of the TimeMarching loop)  warmup=W (untimed steps first)
+//   fhist=<file>  (immersed boundary: the vertex force sum after every background step)
+//   b200=f64|f32  (only in the zl_ref_run_b200 build: the levels' AdvancingAtCurrentTime runs on the
+//                  GPU through the GridInfoLbmB200 plugin, storage f64 or f32; populations are
+//                  brought back into the nodes before the dumps)
 //
 // Dump format (little endian): int32 dims, int32 q, int64 n, then n records of
 // uint64 morton code, int32 flag, int32 pad, double f[q]; records sorted by code.
@@ -36,6 +40,9 @@
 #include "immersed_boundary/immersed_boundary.h"
 #include "immersed_boundary/geometry_ib_shape.h"
 #include "les_models/lbm_les_models.h"
+#ifdef ZL_B200_PLUGIN
+#include "grid_info_lbm_b200.h"
+#endif
 
 using namespace rootproject;
 using amrproject::EDomainBoundaryDirection;
@@ -358,6 +365,20 @@ int main(int argc, char* argv[]) {
     } else {
         amr->AddSolverToGridManager(c3);
     }
+#ifdef ZL_B200_PLUGIN
+    std::unique_ptr<zllbm::B200Session> b200;
+    if (kv.count("b200")) {
+        zllbm::B200Options opt;
+        opt.storage = kv["b200"] == "f32" ? ZL_STORAGE_F32 : ZL_STORAGE_F64;
+        for (auto& bc : bcs) {
+            std::vector<double> v = bc.vel;
+            v.resize(dims, 0.);
+            opt.boundary_values[bc.dir] = v;
+        }
+        b200 = std::make_unique<zllbm::B200Session>(opt);
+        b200->Install(dynamic_cast<lbmproject::SolverLbmInterface*>(amr->ptr_grid_manager_->vec_ptr_solver_.at(0).get()));
+    }
+#endif
     amr->SetSameSolverDependentInfoForAllGrids(amr->ptr_grid_manager_->vec_ptr_solver_.at(0));
     auto& solver = *dynamic_cast<lbmproject::SolverLbmInterface*>(
         amr->ptr_grid_manager_->vec_ptr_solver_.at(0).get());
@@ -449,8 +470,35 @@ int main(int argc, char* argv[]) {
     const int warmup = kv.count("warmup") ? std::atoi(kv["warmup"].c_str()) : 0;
     for (int it = 0; it < warmup; ++it) amr->TimeMarching(it);
     auto t0 = std::chrono::steady_clock::now();
-    for (int it = warmup; it < warmup + steps; ++it) amr->TimeMarching(it);
+    // fhist=<file>: after every background step, the immersed-boundary force sum over the vertices
+    // (vertex order by key), sum F area (WriteTimeHisLagrangianForce, immersed_boundary.cpp:596-642,
+    // with dx = 1 at the background level): int64 steps, then steps x double[3]
+    std::vector<double> fhist;
+    for (int it = warmup; it < warmup + steps; ++it) {
+        amr->TimeMarching(it);
+        if (ib_geo && kv.count("fhist")) {
+            std::vector<std::pair<DefSizet, lbmproject::GeometryVertexImmersedBoundary*>> vs;
+            for (auto& [key, v] : ib_geo->map_vertices_info_)
+                vs.emplace_back(key, dynamic_cast<lbmproject::GeometryVertexImmersedBoundary*>(v.get()));
+            std::sort(vs.begin(), vs.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+            double tot[3] = {0., 0., 0.};
+            for (auto& [key, v] : vs)
+                for (int d = 0; d < dims; ++d) tot[d] += v->force_[d] * v->area_;
+            fhist.insert(fhist.end(), tot, tot + 3);
+        }
+    }
     auto t1 = std::chrono::steady_clock::now();
+#ifdef ZL_B200_PLUGIN
+    if (b200) b200->Download(*amr->ptr_grid_manager_);
+#endif
+    if (kv.count("fhist")) {
+        FILE* fp = std::fopen(kv["fhist"].c_str(), "wb");
+        if (!fp) { std::perror(kv["fhist"].c_str()); return 3; }
+        int64_t nh = static_cast<int64_t>(fhist.size() / 3);
+        std::fwrite(&nh, sizeof(nh), 1, fp);
+        std::fwrite(fhist.data(), sizeof(double), fhist.size(), fp);
+        std::fclose(fp);
+    }
     if (kv.count("out")) dump(kv["out"], dims, q, grid0);
     if (kv.count("lout")) dump_levels(kv["lout"], dims, q, *amr->ptr_grid_manager_);
     if (ib_geo && kv.count("vout")) dump_vertices(kv["vout"]);
