@@ -14,9 +14,11 @@ ASCII), with each level's codes, flags, populations and node member rho_ at that
 (``python tests/golden/make_golden.py vtu`` regenerates only those).  ``amr_<name>.npz`` holds
 multi-level and immersed-boundary runs with their interface layers and vertex records,
 ``ckpt_<name>.npz`` the reference's checkpoint files (``checkpoints``), ``ibpin_<name>.npz`` one
-immersed-boundary step from a Taylor-Green field (``ibpin``), and ``topo_*_small.npz`` small grids
-refined around a body by the reference's grid builder (``topo``); the word in brackets is the
-argument that regenerates only that group.
+immersed-boundary step from a Taylor-Green field (``ibpin``), ``topo_*_small.npz`` small grids
+refined around a body by the reference's grid builder (``topo``), and ``config_<name>.npz`` the
+benchmark configurations at full length (``config``; ``c4`` regenerates only the cylinder's force
+series); the word in brackets is the argument that regenerates only that group.  ``main`` (no
+argument) regenerates every group but ``config``, which takes about half an hour of CPU time.
 """
 from __future__ import annotations
 
@@ -306,9 +308,112 @@ def run_ib_pins(tmp):
         run_amr(name, case, tmp, prefix="ibpin")
 
 
+# the benchmark configurations at full length (``config``): the 256^2 cavity of the plain method
+# (20,000 steps) and the D3Q19 MRT Taylor-Green vortex at 64^3 (5,000 steps).  The populations
+# after the run are kept as a SHA-256 of their bytes (sorted codes, float64 little endian) for the
+# bit-exact FP64 check, plus the reference's output velocity (cavity: the whole field; TGV: the
+# kinetic energy and one x-line), recomputed from f_ as its output rule does.
+CONFIG_CASES = {
+    "c1_cavity256": (LevelConfig(dims=2, n=(256, 256), collision=SRT, nu=0.1 * 256 / 100,
+                                 bc_kind=(BC_BOUNCE_BACK,) * 4 + (0, 0),
+                                 bc_vel=(Z3, Z3, Z3, (0.1, 0.0, 0.0), Z3, Z3)), 20000, "eq"),
+    "c2_tgv64": (LevelConfig(dims=3, n=(65, 65, 65), collision=MRT, nu=0.05 / 3.0,
+                             bc_kind=(BC_PERIODIC,) * 6), 5000, "tgv"),
+}
+
+# the immersed-boundary cylinder of the D2Q9 MRT configuration, reduced: 4 levels on a 128 x 64
+# coarse domain (the full case's 1024 x 512 divided by 8 per axis), diameter 40 finest cells,
+# inflow 0.04, Re 200 (nu = 0.04 * 5 / 200 at the background level), every node starting at
+# feq(1, (0.04, 0)) so that the body is loaded from the first step; 200 background steps
+# (1,600 finest steps).  Kept: each level's codes, flags and interface layers, the vertices, and
+# the force sum F area after every background step.
+C4_CASE = dict(dims=2, n=(128, 64), levels=3, ib="circle:40.3,32.1,2.5", ext=3, inner=2, coll="mrt",
+               nu=0.04 * 5 / 200, vel="0.04,0", bc=["xmin:neq:0.04,0", "xmax:neq:0.04,0", "ymin:bb", "ymax:bb"],
+               steps=200)
+
+
+def output_velocity(f, dims):
+    """The reference's output velocity: recomputed from f_ (lbm_grid_interface.cpp:614-657)."""
+    from oracle.port import LATTICE_C
+    c = np.array(LATTICE_C[dims], dtype=np.float64)
+    return (f @ c) / f.sum(1)[:, None]
+
+
+def run_configs(tmp):
+    import hashlib
+    for name, (cfg, steps, init) in CONFIG_CASES.items():
+        before, after = run_reference(cfg, steps, os.path.join(tmp, name), init=init, u0=0.05)
+        assert np.array_equal(before["code"], after["code"])
+        f = np.ascontiguousarray(after["f"], dtype="<f8")
+        meta = dict(dims=cfg.dims, n=list(cfg.n), collision=cfg.collision, nu=cfg.nu, rho0=cfg.rho0,
+                    bc_kind=list(cfg.bc_kind), bc_vel=[list(v) for v in cfg.bc_vel], steps=steps, init=init,
+                    u0=0.05, f_after_sha256=hashlib.sha256(f.tobytes()).hexdigest())
+        u = output_velocity(f, cfg.dims)
+        out = dict(meta=json.dumps(meta), codes=before["code"])
+        if cfg.dims == 2:
+            out["velocity_after"] = u
+        else:
+            from oracle.port import morton_decode
+            idx = morton_decode(before["code"], cfg.dims) - 1
+            line = (idx[:, 1] == cfg.n[1] // 4) & (idx[:, 2] == cfg.n[2] // 4)
+            order = np.argsort(idx[line, 0])
+            out["line_codes"] = before["code"][line][order]
+            out["line_velocity"] = u[line][order]
+            rho = f.sum(1)
+            out["kinetic_energy"] = np.array(0.5 * (rho * (u * u).sum(1)).sum())
+        np.savez_compressed(os.path.join(HERE, f"config_{name}.npz"), **out)
+        print(name, before.size, "nodes", steps, "steps")
+    run_c4(tmp)
+
+
+def run_c4(tmp):
+    from oracle.port import load_levels
+    case = C4_CASE
+    wd = os.path.join(tmp, "c4")
+    os.makedirs(wd, exist_ok=True)
+    args = [REF_RUN, f"dims={case['dims']}", "n=" + ",".join(str(v) for v in case["n"]), f"levels={case['levels']}",
+            f"coll={case['coll']}", f"nu={case['nu']!r}", f"steps={case['steps']}", f"vel={case['vel']}",
+            f"ib={case['ib']}", f"ext={case['ext']}", f"inner={case['inner']}",
+            "lout0=" + os.path.join(wd, "l0.bin"), "vout0=" + os.path.join(wd, "v0.bin"),
+            "vout=" + os.path.join(wd, "v1.bin"), "fhist=" + os.path.join(wd, "fh.bin")] + \
+           [f"bc={b}" for b in case["bc"]]
+    subprocess.run(args, check=True, cwd=wd, stdout=subprocess.DEVNULL)
+    dims, q, before = load_levels(os.path.join(wd, "l0.bin"))
+    out = {"meta": json.dumps(case)}
+    for lv, b in enumerate(before):
+        out[f"codes{lv}"] = b["nodes"]["code"]
+        out[f"flags{lv}"] = b["nodes"]["flag"]
+        lay = b["layers"]
+        empty = np.zeros(0, dtype=np.uint64)
+        out[f"c2f_fine{lv}"] = np.union1d(np.union1d(lay.get((2, 1), empty), lay.get((3, 1), empty)),
+                                          np.union1d(lay.get((2, 2), empty), lay.get((3, 2), empty)))
+        out[f"f2c_coarse{lv}"] = np.union1d(lay.get((0, 1), empty), lay.get((1, 1), empty))
+        # every node starts at the same equilibrium: keep one node's populations
+        f0 = b["nodes"]["f"]
+        assert np.array_equal(f0, np.broadcast_to(f0[0], f0.shape))
+        out[f"f_init{lv}"] = f0[0].copy()
+    for tag, fn in (("before", "v0.bin"), ("after", "v1.bin")):
+        raw = open(os.path.join(wd, fn), "rb").read()
+        nv = int(np.frombuffer(raw[:8], np.int64)[0])
+        out[f"vertices_{tag}"] = np.frombuffer(raw[8:], np.float64, count=nv * 10).reshape(nv, 10)
+    raw = open(os.path.join(wd, "fh.bin"), "rb").read()
+    nh = int(np.frombuffer(raw[:8], np.int64)[0])
+    out["force_history"] = np.frombuffer(raw[8:], np.float64, count=nh * 3).reshape(nh, 3)
+    np.savez_compressed(os.path.join(HERE, "config_c4_cylinder_reduced.npz"), **out)
+    print("c4", [len(l["nodes"]) for l in before], "nodes per level,", nh, "force samples")
+
+
 if __name__ == "__main__":
     if sys.argv[1:] == ["topo"]:
         run_topologies()
+    elif sys.argv[1:] == ["config"]:
+        if not os.path.exists(REF_RUN):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        with tempfile.TemporaryDirectory() as tmp:
+            run_configs(tmp)
+    elif sys.argv[1:] == ["c4"]:
+        with tempfile.TemporaryDirectory() as tmp:
+            run_c4(tmp)
     elif sys.argv[1:] == ["ibpin"]:
         if not os.path.exists(REF_RUN):
             subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
