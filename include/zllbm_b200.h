@@ -132,9 +132,11 @@ int zl_set_level_nodes(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n)
    once.  zl_set_populations writes that node from the minimum-plane code only and ignores the
    maximum-plane row (the reference keeps the two copies equal; if a caller's copies disagree,
    the minimum-plane copy is kept); zl_get_populations returns the node's values for both codes.
-   The device
-   staging of these calls (and of zl_get_macros) grows to the largest exchange and stays with the
-   context until zl_destroy, so repeated exchanges allocate nothing. */
+   codes may be NULL: the exchange then covers the level's own node list, in the order given to
+   zl_set_level_nodes (n must be its length), which the context keeps on the device, so repeated
+   exchanges send no codes.  The device staging of these calls (and of zl_get_macros) grows to the
+   largest exchange and stays with the context until zl_destroy, so repeated exchanges allocate
+   nothing. */
 int zl_set_populations(zl_ctx* ctx, int level, const uint64_t* codes, const double* f, int64_t n);
 int zl_get_populations(zl_ctx* ctx, int level, const uint64_t* codes, double* f, int64_t n);
 
@@ -193,7 +195,11 @@ int zl_set_graph(zl_ctx* ctx, int enabled);
 
 /* Thread-block shape of a level's step kernel: x (a multiple of 32) by y threads, at most 256;
    a negative x selects the kernel that updates two nodes per thread with packed FP32 pairs
-   (full periodic D3Q19 boxes in FP32/FP16/BF16 storage, no forcing or LES). */
+   (full periodic D3Q19 boxes in FP32/FP16/BF16 storage, no forcing or LES); x = ZL_BLOCK_ROW
+   selects the kernel that gives each warp one whole x-row (y = 1, 2 or 4 rows per block; full
+   periodic D3Q19 boxes in FP16/BF16 storage whose rows hold 128 or 256 nodes, no forcing or
+   LES). */
+#define ZL_BLOCK_ROW (1 << 20)
 int zl_set_block(zl_ctx* ctx, int level, int x, int y);
 
 /* Choose the thread-block shape of a level's step kernel by timing candidate shapes (on a saved
@@ -255,7 +261,8 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
 /* Delta kernel of a level's immersed boundary: ZL_IB_DELTA_4, the reference's four-point
    StencilDisTwo (immersed_boundary.cpp:365-384, the default), or ZL_IB_DELTA_3, the three-point
    kernel of Roma, Peskin and Berger (1999), which the reference does not have.  Set it before
-   zl_ib_set_vertices (the stencil check uses it). */
+   zl_ib_set_vertices (the stencil check and the list of stencil nodes use it); changing it while
+   the level has vertices returns ZL_ESTATE. */
 #define ZL_IB_DELTA_4 4
 #define ZL_IB_DELTA_3 3
 int zl_ib_set_delta(zl_ctx* ctx, int level, int width);

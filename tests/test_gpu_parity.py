@@ -141,3 +141,33 @@ def test_error_paths():
         with pytest.raises(zl.ZlError) as e:
             ctx.set_level_nodes(0, zl.box_codes(2, [1, 1], [40, 40]))
         assert e.value.code == -2
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("storage", [0, 2])
+def test_exchange_without_codes_uses_the_level_order(storage):
+    """Node exchanges with codes = NULL cover the level's own node list in the order handed to
+    zl_set_level_nodes (kept on the device): same results as passing those codes, and a count
+    other than the level's is refused."""
+    import zllbm_b200 as zl
+    meta, codes, f0, _ = load_lbm("box3d_mixed")
+    order = np.random.default_rng(3).permutation(codes.size)
+    shuffled = codes[order]
+    with zl.Context(solver_config(meta, storage)) as ctx:
+        ctx.set_level_nodes(0, shuffled)
+        ctx.set_populations(0, None, f0[order])
+        ctx.advance(3)
+        a = ctx.get_populations(0, shuffled)
+        b = ctx.get_populations(0, None, codes.size)
+        assert np.array_equal(a, b)
+        rho_a, u_a = ctx.get_macros(0, shuffled)
+        rho_b, u_b = ctx.get_macros(0, None, codes.size)
+        assert np.array_equal(rho_a, rho_b) and np.array_equal(u_a, u_b)
+        with pytest.raises(zl.ZlError) as e:
+            ctx.get_populations(0, None, codes.size - 1)
+        assert e.value.code == -1  # ZL_EINVAL
+    with zl.Context(solver_config(meta, storage)) as ctx:
+        ctx.set_level_nodes(0, shuffled)
+        ctx.set_populations(0, shuffled, f0[order])
+        ctx.advance(3)
+        assert np.array_equal(ctx.get_populations(0, shuffled), a)

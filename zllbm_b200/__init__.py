@@ -22,6 +22,7 @@ SRT, MRT = 0, 1
 BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION, BC_CONVECTIVE_OUTFLOW = 0, 1, 2, 3, 4
 STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORAGE_F64, "f32": STORAGE_F32, "f16": STORAGE_F16, "bf16": STORAGE_BF16}
+BLOCK_ROW = 1 << 20  # zl_set_block x: one warp per x-row (ZL_BLOCK_ROW)
 ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE",
           -7: "ETOOLARGE"}
 
@@ -283,25 +284,34 @@ class Context:
         c = _u64(codes)
         self._check(self.lib.zl_set_level_nodes(self.handle, level, _p(c, ctypes.c_uint64), c.size))
 
-    def set_populations(self, level: int, codes, f):
-        c, ff = _u64(codes), _f64(f)
-        assert ff.size == c.size * self.config.q
-        self._check(self.lib.zl_set_populations(self.handle, level, _p(c, ctypes.c_uint64),
-                                                _p(ff, ctypes.c_double), c.size))
-
-    def get_populations(self, level: int, codes) -> np.ndarray:
+    def _node_list(self, codes, n: int | None = None):
+        """(pointer, count) of an exchange's node list; codes None: the level's own list in the
+        order of set_level_nodes (count n), kept on the device and not uploaded again."""
+        if codes is None:
+            if n is None:
+                raise ValueError("without codes the node count is needed")
+            return None, int(n), None
         c = _u64(codes)
-        out = np.empty((c.size, self.config.q))
-        self._check(self.lib.zl_get_populations(self.handle, level, _p(c, ctypes.c_uint64),
-                                                _p(out, ctypes.c_double), c.size))
+        return _p(c, ctypes.c_uint64), c.size, c
+
+    def set_populations(self, level: int, codes, f):
+        ff = _f64(f)
+        ptr, n, keep = self._node_list(codes, ff.size // self.config.q)
+        assert ff.size == n * self.config.q
+        self._check(self.lib.zl_set_populations(self.handle, level, ptr, _p(ff, ctypes.c_double), n))
+
+    def get_populations(self, level: int, codes, n: int | None = None) -> np.ndarray:
+        ptr, n, keep = self._node_list(codes, n)
+        out = np.empty((n, self.config.q))
+        self._check(self.lib.zl_get_populations(self.handle, level, ptr, _p(out, ctypes.c_double), n))
         return out
 
-    def get_macros(self, level: int, codes):
-        c = _u64(codes)
-        rho = np.empty(c.size)
-        u = np.empty((c.size, self.config.dims))
-        self._check(self.lib.zl_get_macros(self.handle, level, _p(c, ctypes.c_uint64), _p(rho, ctypes.c_double),
-                                           _p(u, ctypes.c_double), c.size))
+    def get_macros(self, level: int, codes, n: int | None = None):
+        ptr, n, keep = self._node_list(codes, n)
+        rho = np.empty(n)
+        u = np.empty((n, self.config.dims))
+        self._check(self.lib.zl_get_macros(self.handle, level, ptr, _p(rho, ctypes.c_double),
+                                           _p(u, ctypes.c_double), n))
         return rho, u
 
     def set_level_interface(self, level: int, c2f_fine, f2c_coarse, coarse_excluded):
@@ -319,7 +329,8 @@ class Context:
         self._check(self.lib.zl_interpolate_interface(self.handle, fine_level))
 
     def set_block(self, level: int, x: int, y: int = 1):
-        """Step-kernel block shape; negative x: two nodes per thread (packed FP32 pairs)."""
+        """Step-kernel block shape; negative x: two nodes per thread (packed FP32 pairs);
+        x = BLOCK_ROW: one warp per x-row, y rows per block."""
         self._check(self.lib.zl_set_block(self.handle, level, x, y))
 
     def write_checkpoint_nodes(self, path: str, codes: list, flags: list):

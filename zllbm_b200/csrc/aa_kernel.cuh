@@ -32,6 +32,7 @@ enum Collision : int { kSrt = 0, kMrt = 1 };
 // Per-cell information for levels whose node set does not fill its box.
 constexpr uint32_t kInfoPresent = 1u << 31;
 constexpr uint32_t kInfoSaveMacro = 1u << 30;  // keep rho, u of the last collision (coarse/fine transfer source)
+constexpr uint32_t kInfoForce = 1u << 23;  // node force may be non-zero (a stencil node of the immersed boundary)
 constexpr int kInfoFaceShift = 24;  // 6 bits: on face xmin..zmax (reference boundary node sets)
 
 // extended-physics bits of the step kernel's Ext template argument
@@ -843,9 +844,12 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
         T mac[4];
         NodeForce nf;
         if (Forced) {
-            // GetAllForcesForANode (lbm_solver_interface.cpp:132-144): constant force plus node forces
+            // GetAllForcesForANode (lbm_solver_interface.cpp:132-144): constant force plus node forces;
+            // only immersed-boundary stencil nodes (kInfoForce) can hold a node force, the others
+            // skip the FP64 read (adding the 0 it would give changes no bit)
+            const bool node_force = p.force && (!Masked || (info & kInfoForce));
 #pragma unroll
-            for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (p.force ? p.force[(long long)self * 3 + a] : 0.);
+            for (int a = 0; a < 3; ++a) nf.F[a] = p.const_force[a] + (node_force ? p.force[(long long)self * 3 + a] : 0.);
         }
         if constexpr (St::kDeviation) {
             // Smagorinsky constant C: the level's, or 18 c of the learned closure's last evaluation
@@ -986,35 +990,63 @@ __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>:
 }
 
 // ---------------------------------------------------------------- several levels in one launch
+// Division of 31-bit unsigned integers by a fixed divisor through one widening multiply and a
+// shift (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, the round-up method): with l = ceil(log2 d) and m = floor(2^(31 + l) / d) + 1,
+// floor(n / d) = floor(n m / 2^(31 + l)) for every 0 <= n < 2^31; m < 2^32 for d >= 2.
+struct FastDiv {
+    uint32_t d = 1, m = 0, shift = 0;
+    ZL_HD static FastDiv make(uint32_t divisor) {
+        FastDiv f;
+        f.d = divisor;
+        if (divisor <= 1) return f;
+        uint32_t l = 0;
+        while ((1ull << l) < divisor) ++l;
+        f.shift = 31 + l;
+        f.m = (uint32_t)((1ull << f.shift) / divisor + 1);
+        return f;
+    }
+    ZL_HD uint32_t div(uint32_t n) const {
+        return d <= 1 ? n : (uint32_t)(((unsigned long long)n * m) >> shift);
+    }
+};
+
 // Levels whose steps follow one another with no transfer between them are independent: one
 // persistent launch sweeps all their nodes.  Node i of the batch belongs to the level whose
-// [first[l], first[l + 1]) range holds it and is the (i - first[l])-th node of that box, x fastest.
+// [first[l], first[l + 1]) range holds it and is the (i - first[l])-th cell of that box, x fastest;
+// each level's range starts at a multiple of the block size, so a block's level is uniform.
 // Every level of a multi-level context keeps its info array, so the masked, bounded variant
 // (correct for any level) is used throughout; the layout phase is per level.
 constexpr int kBatchMax = 8;
+constexpr int kBatchThreads = 256;
 struct LevelBatch {
     int count;
     int odd[kBatchMax];
     long long first[kBatchMax + 1];
+    FastDiv nx[kBatchMax], ny[kBatchMax];  // box extents n0 and n1 of each level
     void* f[kBatchMax];
     LevelGeom geo[kBatchMax];
     const StepParams* params[kBatchMax];  // device copies of the levels' parameters
 };
 
 template <class L, class S, int Coll, int Ext>
-__global__ void __launch_bounds__(256, 3) aa_batch_kernel(LevelBatch b) {
+__global__ void __launch_bounds__(kBatchThreads, 3) aa_batch_kernel(LevelBatch b) {
     const long long total = b.first[b.count];
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
-         i += (long long)gridDim.x * blockDim.x) {
-        int l = 0;
-        while (l + 1 < b.count && i >= b.first[l + 1]) ++l;
+    for (long long base = (long long)blockIdx.x * kBatchThreads; base < total;
+         base += (long long)gridDim.x * kBatchThreads) {
+        int l = 0;  // uniform across the block
+        while (l + 1 < b.count && base >= b.first[l + 1]) ++l;
         const LevelGeom& geo = b.geo[l];
-        const long long k = i - b.first[l];
+        const long long k64 = base + threadIdx.x - b.first[l];
+        const long long cells = (long long)geo.n[0] * geo.n[1] * geo.n[2];
+        if (k64 >= cells) continue;  // padding between two levels' ranges
+        const uint32_t k = (uint32_t)k64;  // a level box holds fewer than 2^31 cells
+        const uint32_t r = b.nx[l].div(k);
+        const uint32_t z = b.ny[l].div(r);
         Coord c;
-        c.x[0] = (int)(k % geo.n[0]);
-        const long long r = k / geo.n[0];
-        c.x[1] = (int)(r % geo.n[1]);
-        c.x[2] = (int)(r / geo.n[1]);
+        c.x[0] = (int)(k - r * (uint32_t)geo.n[0]);
+        c.x[1] = (int)(r - z * (uint32_t)geo.n[1]);
+        c.x[2] = (int)z;
         S* f = static_cast<S*>(b.f[l]);
         if (b.odd[l]) aa_node<L, S, Coll, true, true, true, Ext>(f, geo, *b.params[l], c);
         else aa_node<L, S, Coll, false, true, true, Ext>(f, geo, *b.params[l], c);

@@ -26,6 +26,10 @@ struct DeviceBuffer {
         ptr = nullptr;
         bytes = 0;
     }
+    void swap(DeviceBuffer& o) {
+        std::swap(ptr, o.ptr);
+        std::swap(bytes, o.bytes);
+    }
 };
 
 struct Level {
@@ -45,6 +49,8 @@ struct Level {
     long long nodes = 0;
     long long steps = 0;
     std::vector<uint64_t> codes;  // sorted node codes (kept for multi-level set-ups)
+    DeviceBuffer node_codes;      // the codes of zl_set_level_nodes in the caller's order (device)
+    long long n_node_codes = 0;
     // coarse/fine transfer with the next coarser level (this level is the fine side)
     DeviceBuffer macro;                                   // rho, u of transfer sources
     DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w;
@@ -515,6 +521,13 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     }
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if ((rc = sync_params(ctx, level))) return rc;
+    // the node list stays on the device for exchanges that pass no codes
+    L.node_codes.release();
+    L.n_node_codes = 0;
+    if (codes) {
+        L.node_codes.swap(dcodes);
+        L.n_node_codes = n;
+    }
     L.active = true;
     return ZL_OK;
 }
@@ -547,21 +560,30 @@ static int exchange(zl_ctx* ctx, int level, const uint64_t* codes, double* f_hos
                     bool write) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
-    if (n < 0 || (n > 0 && !codes)) return fail(ctx, ZL_EINVAL, "bad node list");
+    if (n < 0) return fail(ctx, ZL_EINVAL, "bad node count");
     if (n == 0) return ZL_OK;
     ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
     Level& L = ctx->levels[level];
     const int q = ctx->q, dims = ctx->dims;
-    DeviceBuffer& dcodes = ctx->stage_codes;
     DeviceBuffer& dbuf = ctx->stage_data;
     DeviceBuffer& dmac = ctx->stage_mac;
-    if ((rc = upload_codes(ctx, codes, n, dcodes))) return rc;
+    // no codes: the level's own node list (zl_set_level_nodes order), already on the device
+    const uint64_t* dcodes = nullptr;
+    if (codes) {
+        if ((rc = upload_codes(ctx, codes, n, ctx->stage_codes))) return rc;
+        dcodes = (const uint64_t*)ctx->stage_codes.ptr;
+    } else {
+        if (n != L.n_node_codes)
+            return fail(ctx, ZL_EINVAL, "level %d: without codes, n must be the %lld nodes given to zl_set_level_nodes",
+                        level, L.n_node_codes);
+        dcodes = (const uint64_t*)L.node_codes.ptr;
+    }
     if ((rc = reset_flag(ctx))) return rc;
     if (write) {
         if ((rc = reserve(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
         ZL_CUDA(ctx, cudaMemcpyAsync(dbuf.ptr, f_host, (size_t)n * q * 8, cudaMemcpyHostToDevice, ctx->stream));
         ZL_CUDA(ctx, ctx->ops->scatter(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
-                                       (const uint64_t*)dcodes.ptr, (const double*)dbuf.ptr, n,
+                                       dcodes, (const double*)dbuf.ptr, n,
                                        (int*)ctx->scratch_flag.ptr, ctx->stream));
     } else {
         if (f_host && (rc = reserve(ctx, dbuf, (size_t)n * q * sizeof(double)))) return rc;
@@ -569,7 +591,7 @@ static int exchange(zl_ctx* ctx, int level, const uint64_t* codes, double* f_hos
         double* drho = rho ? (double*)dmac.ptr : nullptr;
         double* du = rho ? drho + n : nullptr;
         ZL_CUDA(ctx, ctx->ops->gather(dims, L.f.ptr, L.geo, L.params, L.map, L.even_layout,
-                                      (const uint64_t*)dcodes.ptr, f_host ? (double*)dbuf.ptr : nullptr, drho, du, n,
+                                      dcodes, f_host ? (double*)dbuf.ptr : nullptr, drho, du, n,
                                       (int*)ctx->scratch_flag.ptr, ctx->stream));
         if (f_host)
             ZL_CUDA(ctx, cudaMemcpyAsync(f_host, dbuf.ptr, (size_t)n * q * 8, cudaMemcpyDeviceToHost, ctx->stream));
@@ -733,7 +755,11 @@ static int step_group(zl_ctx* ctx, const std::vector<int>& group) {
         b.f[i] = L.f.ptr;
         b.geo[i] = L.geo;
         b.params[i] = (const StepParams*)ctx->params_dev.ptr + l;
-        b.first[i + 1] = b.first[i] + (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2];
+        b.nx[i] = FastDiv::make((uint32_t)L.geo.n[0]);
+        b.ny[i] = FastDiv::make((uint32_t)L.geo.n[1]);
+        // each level's range starts on a block boundary (a block's level is uniform)
+        const long long cells = (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2];
+        b.first[i + 1] = b.first[i] + (cells + kBatchThreads - 1) / kBatchThreads * kBatchThreads;
     }
     const int ext = (ctx->cfg.forcing ? kExtForce : 0) | (ctx->cfg.les ? kExtLes : 0);
     ZL_CUDA(ctx, ctx->ops->batch(ctx->dims, ctx->cfg.collision, ext, b, ctx->stream));
@@ -878,6 +904,17 @@ int zl_set_block(zl_ctx* ctx, int level, int x, int y) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
     Level& L = ctx->levels[level];
+    static_assert(ZL_BLOCK_ROW == kRowKernelBlockX, "row-kernel marker");
+    if (x == ZL_BLOCK_ROW) {
+        if (y != 1 && y != 2 && y != 4) return fail(ctx, ZL_EINVAL, "row kernel: %d rows per block", y);
+        if (!row_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes, L.geo))
+            return fail(ctx, ZL_EINVAL,
+                        "the row kernel needs a full periodic D3Q19 box in FP16/BF16 storage with 128 or 256 nodes per row");
+        L.geo.block[0] = x;
+        L.geo.block[1] = y;
+        ++ctx->generation;
+        return ZL_OK;
+    }
     const int ax = std::abs(x);
     if (ax < 32 || ax % 32 || y < 1 || ax * y > 256) return fail(ctx, ZL_EINVAL, "block shape %d x %d", x, y);
     if (x < 0 && !pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes))
@@ -897,10 +934,13 @@ int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
     DeviceBuffer saved;
     if ((rc = alloc(ctx, saved, L.f.bytes))) return rc;
     ZL_CUDA(ctx, cudaMemcpyAsync(saved.ptr, L.f.ptr, L.f.bytes, cudaMemcpyDeviceToDevice, ctx->stream));
-    // negative x: two nodes per thread (full periodic D3Q19 boxes in reduced storage only)
+    // negative x: two nodes per thread (full periodic D3Q19 boxes in reduced storage only);
+    // ZL_BLOCK_ROW: one warp per row (FP16/BF16 boxes with 128- or 256-node rows)
     const int shapes[][2] = {{256, 1}, {128, 2}, {128, 1}, {64, 4}, {64, 2}, {32, 8}, {32, 4},
-                             {-128, 1}, {-64, 2}, {-256, 1}, {-64, 1}};
+                             {-128, 1}, {-64, 2}, {-256, 1}, {-64, 1},
+                             {ZL_BLOCK_ROW, 4}, {ZL_BLOCK_ROW, 2}, {ZL_BLOCK_ROW, 1}};
     const bool pairs = pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes);
+    const bool rows = row_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes, L.geo);
     cudaEvent_t t0, t1;
     ZL_CUDA(ctx, cudaEventCreate(&t0));
     ZL_CUDA(ctx, cudaEventCreate(&t1));
@@ -911,8 +951,12 @@ int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
         LevelGeom g = L.geo;
         g.block[0] = shapes[i][0];
         g.block[1] = shapes[i][1];
-        if (g.block[0] < 0 && !pairs) continue;
-        if (std::abs(g.block[0]) > 2 * std::max(32, g.n[0])) continue;
+        if (g.block[0] == ZL_BLOCK_ROW) {
+            if (!rows) continue;
+        } else {
+            if (g.block[0] < 0 && !pairs) continue;
+            if (std::abs(g.block[0]) > 2 * std::max(32, g.n[0])) continue;
+        }
         const bool odd0 = L.even_layout == 1;
         for (int warm = 0; warm < 2; ++warm)
             ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, odd0 != (warm & 1), L.bnd,
@@ -1255,6 +1299,13 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         if ((rc = alloc(ctx, L.ib_nodes, (size_t)std::max(nodes, 1) * 4))) return rc;
         ZL_CUDA(ctx, cudaMemcpyAsync(L.ib_nodes.ptr, sel.ptr, (size_t)nodes * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        // the step reads node forces only where kInfoForce is set (forces elsewhere stay 0); the
+        // bit is never cleared, released nodes keep it with a zero force
+        if (L.info.ptr && nodes > 0) {
+            or_bits_kernel<<<(nodes + 127) / 128, 128, 0, ctx->stream>>>((uint32_t*)L.info.ptr, (const int*)L.ib_nodes.ptr,
+                                                                          nodes, kInfoForce);
+            ZL_CUDA(ctx, cudaGetLastError());
+        }
         ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         L.n_ib_nodes = nodes;
     }
@@ -1266,6 +1317,9 @@ int zl_ib_set_delta(zl_ctx* ctx, int level, int width) {
     int rc = check_level(ctx, level, false);
     if (rc) return rc;
     if (width != ZL_IB_DELTA_4 && width != ZL_IB_DELTA_3) return fail(ctx, ZL_EINVAL, "stencil width %d", width);
+    // the level's stencil-node list (and the cells that read node forces) follow the width
+    if (ctx->levels[level].n_vertices > 0 && ctx->levels[level].ib_width != width)
+        return fail(ctx, ZL_ESTATE, "level %d: set the delta kernel before the vertices", level);
     ctx->levels[level].ib_width = width;
     ++ctx->generation;
     return ZL_OK;

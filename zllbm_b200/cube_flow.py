@@ -5,10 +5,13 @@ Re = 1000 on the cube edge, FP32 storage; the cube is an immersed boundary (dire
 surface vertices on the finest level).  All level steps run as batched launches replayed from a
 CUDA graph.
 
-    python -m zllbm_b200.cube_flow --topology cube_topology.npz [--steps 64] [--warmup 4]
+    python -m zllbm_b200.cube_flow [--topology cube_topology.npz] [--steps 64] [--warmup 4]
 
 The node sets and interface layers come from the host's grid builder: the reference's own
-(``oracle/make_body_topology.py`` writes them from its AmrManager::SetupMesh).  Throughput counts
+(``oracle/make_body_topology.py`` writes them from its AmrManager::SetupMesh).  The default,
+``zllbm_b200/topologies/cube_256x128x128_l2.npz``, is that builder's grid for this case
+(``--n 256,128,128 --levels 2 --cube 80,64,64,16 --ext 6 --inner 16``) in the packed form of
+``zllbm_b200.topology_pack``.  Throughput counts
 every node update the reference performs: the sum over levels of nodes x 2^level per coarse
 step.
 """
@@ -16,11 +19,15 @@ from __future__ import annotations
 
 import argparse
 import json
+import os
 import time
 
 import numpy as np
 
 import zllbm_b200 as zl
+from zllbm_b200.topology_pack import load_topology
+
+DEFAULT_TOPOLOGY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "topologies", "cube_256x128x128_l2.npz")
 
 U_IN = 0.05
 RE = 1000.0
@@ -47,7 +54,7 @@ def cube_vertices(center, edge: float, h: float) -> tuple[np.ndarray, np.ndarray
 
 
 def build(topology: str, storage: int = zl.STORAGE_F32):
-    z = np.load(topology)
+    z = load_topology(topology)
     meta = json.loads(str(z["meta"]))
     levels = meta["levels"]
     n = meta["n"]
@@ -107,7 +114,7 @@ def run(topology: str, steps: int = 64, warmup: int = 4, graph: bool = True, bat
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--topology", required=True)
+    ap.add_argument("--topology", default=DEFAULT_TOPOLOGY)
     ap.add_argument("--steps", type=int, default=64)
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--graph", type=int, default=1)

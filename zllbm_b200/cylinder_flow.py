@@ -6,22 +6,28 @@ finest level (direct forcing with the reference's four-point delta kernel).  All
 as batched launches replayed from a CUDA graph; drag and lift are the FP64 sums of the vertex
 forces.
 
-    python -m zllbm_b200.cylinder_flow --topology cylinder_topology.npz [--steps 400] [--warmup 8]
+    python -m zllbm_b200.cylinder_flow [--topology cylinder_topology.npz] [--steps 400] [--warmup 8]
 
 The node sets and interface layers come from the host's grid builder: the reference's own
-(``oracle/make_body_topology.py --n 1024,512 --levels 3 --circle 256,256,2.5``).  Throughput counts
+(``oracle/make_body_topology.py --n 1024,512 --levels 3 --circle 256,256,2.5 --ext 8 --inner 8``);
+the default, ``zllbm_b200/topologies/cylinder_1024x512_l3.npz``, is that grid in the packed form
+of ``zllbm_b200.topology_pack``.  Throughput counts
 every node update the reference performs: the sum over levels of nodes x 2^level per coarse step.
 """
 from __future__ import annotations
 
 import argparse
 import json
+import os
 import math
 import time
 
 import numpy as np
 
 import zllbm_b200 as zl
+from zllbm_b200.topology_pack import load_topology
+
+DEFAULT_TOPOLOGY = os.path.join(os.path.dirname(os.path.abspath(__file__)), "topologies", "cylinder_1024x512_l3.npz")
 
 U_IN = 0.04
 RE = 200.0
@@ -29,7 +35,7 @@ VERTICES = 400
 
 
 def build(topology: str, storage: int = zl.STORAGE_F32):
-    z = np.load(topology)
+    z = load_topology(topology)
     meta = json.loads(str(z["meta"]))
     levels = meta["levels"]
     n = meta["n"]
@@ -92,7 +98,7 @@ def run(topology: str, steps: int = 400, warmup: int = 8, graph: bool = True, ba
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--topology", required=True)
+    ap.add_argument("--topology", default=DEFAULT_TOPOLOGY)
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--graph", type=int, default=1)

@@ -3,12 +3,15 @@ tau = 0.55): the same run in FP64, FP32, FP16-deviation and BF16-deviation stora
 velocity's relative L2 error against the FP64 run and the kinetic-energy decay at checkpoints.
 
     python -m zllbm_b200.tgv_accuracy [--cells 256] [--steps 5000] [--checkpoints 5] [--out file.json]
+                                      [--storages f32,f16,bf16]
 
 FP64 storage is the device path that is bit-exact to the reference's own solver, so it is the
 FP64 oracle of the comparison.  Every run starts from feq(rho, u) of the analytic TGV fields
 (pressure from the TGV formula, rho = 1 + 3 p).  Kinetic energy is also compared with the
 linear viscous decay exp(-2 nu |k|^2 t), |k|^2 = 3 (2 pi / N)^2 (the u0 = 0.05 vortex is nearly
-linear at these Reynolds numbers).
+linear at these Reynolds numbers).  Each error is also split into an amplitude part (the
+projection on the FP64 field, a = <u, u64> / <u64, u64>: a - 1 is a decay-rate bias) and the part
+orthogonal to it (|u - a u64| / |u64|: noise and shape errors).
 """
 from __future__ import annotations
 
@@ -62,7 +65,8 @@ def run_storage(storage: str, n: int, steps: int, checkpoints: int, log=print):
     return out, mlups
 
 
-def run(n: int = 256, steps: int = 5000, checkpoints: int = 5, log=print) -> dict:
+def run(n: int = 256, steps: int = 5000, checkpoints: int = 5, log=print,
+        storages: tuple = ("f32", "f16", "bf16")) -> dict:
     import torch
     nu = (TAU - 0.5) / 3.0
     k2 = 3.0 * (2.0 * math.pi / n) ** 2
@@ -75,14 +79,20 @@ def run(n: int = 256, steps: int = 5000, checkpoints: int = 5, log=print) -> dic
     result["kinetic_energy_f64"] = ke_ref
     result["kinetic_energy_linear_decay"] = [e0 * math.exp(-2.0 * nu * k2 * s) for s, _ in ref]
     result["storages"]["f64"] = {"mlups_with_readback": mlups64}
-    for storage in ("f32", "f16", "bf16"):
+    for storage in storages:
         fields, mlups = run_storage(storage, n, steps, checkpoints, log)
-        errs, kes = [], []
+        errs, kes, amps, perps = [], [], [], []
         for (s, u), (_, u64) in zip(fields, ref):
-            diff = (u.double() - u64.double()).norm() / u64.double().norm()
+            ud, rd = u.double(), u64.double()
+            nr = rd.norm()
+            diff = (ud - rd).norm() / nr
+            a = float((ud * rd).sum() / (nr * nr))
             errs.append(float(diff))
-            kes.append(float(0.5 * (u.double() ** 2).sum(1).mean()))
-        result["storages"][storage] = {"velocity_rel_l2_vs_f64": errs, "kinetic_energy": kes,
+            amps.append(a - 1.0)
+            perps.append(float((ud - a * rd).norm() / nr))
+            kes.append(float(0.5 * (ud ** 2).sum(1).mean()))
+        result["storages"][storage] = {"velocity_rel_l2_vs_f64": errs, "amplitude_minus_1": amps,
+                                       "orthogonal_rel_l2": perps, "kinetic_energy": kes,
                                        "kinetic_energy_rel_diff_vs_f64": [k / r - 1.0 for k, r in zip(kes, ke_ref)],
                                        "mlups_with_readback": mlups}
         log(f"{storage}: velocity rel L2 vs FP64 at checkpoints {['%.2e' % e for e in errs]}")
@@ -97,8 +107,9 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--checkpoints", type=int, default=5)
     ap.add_argument("--out", default=None)
+    ap.add_argument("--storages", default="f32,f16,bf16")
     a = ap.parse_args(argv)
-    res = run(a.cells, a.steps, a.checkpoints)
+    res = run(a.cells, a.steps, a.checkpoints, storages=tuple(a.storages.split(",")))
     text = json.dumps(res, indent=1)
     if a.out:
         with open(a.out, "w") as fh:
