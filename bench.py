@@ -288,12 +288,17 @@ def closure_block():
     cost = res.mlups["cost"]
     return {
         "workload": "decaying HIT (seeded random-phase modes, k0=4, u_rms=0.04): fine D3Q19 SRT 256^3 box-filtered "
-                    "by 4 to 64^3, 2000 coarse steps; trained and calibrated on one realization, scored on another",
+                    "by 4 to 64^3, 2000 coarse steps; trained and calibrated on one realization, scored on three "
+                    "others (mean, spread)",
         "error": "RMS over shells and 8 checkpoints of log(E_LES / E_filtered_fine), lower is better",
+        "test_realizations": len(e["smagorinsky"]["per_realization"]),
         "smagorinsky_cs0.1": e["smagorinsky"]["error"],
         "smagorinsky_calibrated": e["smagorinsky_calibrated"]["error"],
         "learned_calibrated": e["learned_calibrated"]["error"],
         "learned_calibrated_every16": e["learned_calibrated_every16"]["error"],
+        "error_std": {k: e[k]["error_std"] for k in ("smagorinsky", "smagorinsky_calibrated", "learned_calibrated",
+                                                       "learned_calibrated_every16")},
+        "learned_minus_smagorinsky_calibrated": e["learned_minus_smagorinsky_calibrated"],
         "alpha": res.training["alpha"], "cs_calibrated": res.training["calibration"]["cs_best"],
         "held_out_mse": {"network": res.training["val_loss"], "smagorinsky_y1": res.training["val_loss_smagorinsky_y1"],
                          "best_constant": res.training["val_loss_best_constant"]},
@@ -302,6 +307,34 @@ def closure_block():
         "cost_fraction_every_step": cost["learned_cost_fraction"],
         "seconds": time.perf_counter() - t0,
     }
+
+
+def kernel_name(block, storage: str) -> str:
+    """The step kernel the (autotuned) block shape selects."""
+    import zllbm_b200 as zl
+    if block and block[0] == zl.BLOCK_ROW:
+        return f"aa_row_kernel<{storage}, {COLLISION.upper()}> (one warp per x-row)"
+    if block and block[0] < 0:
+        return f"aa_pair_kernel<{storage}, {COLLISION.upper()}> (two nodes per thread)"
+    return f"aa_step_kernel<D3Q19, {storage}, {COLLISION.upper()}>"
+
+
+def multilevel_block(steps: int, warmup: int, peak: float):
+    """The multi-level configurations on the reference-built grids (packed under
+    zllbm_b200/topologies/): the cube flow (D3Q19 SRT + Smagorinsky + immersed-boundary cube,
+    levels 0..2) and the cylinder flow (D2Q9 MRT + immersed-boundary cylinder, levels 0..3), FP32,
+    batched level steps replayed from a CUDA graph.  MLUPS count every node update of every level
+    (nodes x 2^level per coarse step); the HBM figure is those updates' algorithmic bytes
+    (2 Q sizeof(float) each) over the event time."""
+    from zllbm_b200 import cube_flow, cylinder_flow
+    out = {}
+    for name, mod, q, k in (("cube_flow", cube_flow, 19, steps), ("cylinder_flow", cylinder_flow, 9, 4 * steps)):
+        res = mod.run(mod.DEFAULT_TOPOLOGY, steps=k, warmup=warmup, log=lambda m: None)
+        gbs = res["mlups"] * 1e6 * 2 * q * 4 / 1e9
+        out[name] = {"workload": res["workload"], "mlups": res["mlups"], "ms_per_coarse_step": res["ms_per_coarse_step"],
+                     "coarse_steps": k, "nodes_per_level": res["nodes_per_level"],
+                     "hbm_gbs_algorithmic": gbs, "frac": gbs / peak, "finite": res["finite"]}
+    return out
 
 
 def run_ours(args):
@@ -350,10 +383,15 @@ def run_ours(args):
     # other storage precisions of the same workload, kernel time only (reported alongside)
     variants = {}
     if args.variants and rank == 0:
-        for name in ("f16", "bf16", "f32"):
+        # 16-bit storages with the default stochastic rounding and ("rn") round to nearest
+        for name in ("f16", "bf16", "f32", "f16rn", "bf16rn"):
             if name == args.storage:
                 continue
-            with zl.Context(solver_config(zl.STORAGE_NAMES[name], local)) as c2:
+            rn = name.endswith("rn")
+            base = name[:-2] if rn else name
+            vcfg = solver_config(zl.STORAGE_NAMES[base], local)
+            vcfg.storage_rounding = zl.ROUND_NEAREST if rn else zl.ROUND_STOCHASTIC
+            with zl.Context(vcfg) as c2:
                 c2.set_level_nodes(0, codes)
                 c2.set_populations(0, codes, f0)
                 vblock = c2.autotune(0) if args.tune else None
@@ -362,40 +400,43 @@ def run_ours(args):
                 c2.set_graph(args.graph)
                 c2.advance(args.warmup)
                 vms = time_steps(c2, args.steps, args.graph)
-                b = nodes * 2 * 19 * STORAGE_BYTES[name]
+                b = nodes * 2 * 19 * STORAGE_BYTES[base]
                 variants[name] = {"mlups": nodes * args.steps / (vms / 1e3) / 1e6,
                                   "ms_per_step": vms / args.steps,
                                   "hbm_gbs": b / (vms / args.steps / 1e3) / 1e9,
                                   "frac": b / (vms / args.steps / 1e3) / 1e9 / peak,
-                                  "block": vblock}
+                                  "block": vblock, "kernel": kernel_name(vblock, name),
+                                  "rounding": "nearest" if rn else ("stochastic" if base in ("f16", "bf16") else None)}
     # end to end through the C ABI with host buffers
     e2e = None
     if not args.no_e2e:
-        codes_h = torch.from_numpy(codes).pin_memory()
         f_h = torch.from_numpy(f0).pin_memory()
         rho_h = torch.empty(codes.size, dtype=torch.float64).pin_memory()
         u_h = torch.empty((codes.size, 3), dtype=torch.float64).pin_memory()
         lib = ctx.lib
         import ctypes
-        u64p, dp = ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_double)
-        cp = ctypes.cast(codes_h.data_ptr(), u64p)
+        dp = ctypes.POINTER(ctypes.c_double)
+        # the level's node list was handed over once (zl_set_level_nodes); exchanges without codes
+        # use it in that order, so only populations and fields cross PCIe
         barrier(dist)
         ctx.synchronize()
         t0 = time.perf_counter()
-        ctx._check(lib.zl_set_populations(ctx.handle, 0, cp, ctypes.cast(f_h.data_ptr(), dp), codes.size))
+        ctx._check(lib.zl_set_populations(ctx.handle, 0, None, ctypes.cast(f_h.data_ptr(), dp), codes.size))
         ctx._check(lib.zl_advance(ctx.handle, args.steps))
-        ctx._check(lib.zl_get_macros(ctx.handle, 0, cp, ctypes.cast(rho_h.data_ptr(), dp),
+        ctx._check(lib.zl_get_macros(ctx.handle, 0, None, ctypes.cast(rho_h.data_ptr(), dp),
                                      ctypes.cast(u_h.data_ptr(), dp), codes.size))
         ctx.synchronize()
         t_e2e = max_over_ranks(dist, time.perf_counter() - t0)
-        h2d = codes.nbytes * 2 + f0.nbytes
+        h2d = f0.nbytes
         d2h = rho_h.numel() * 8 + u_h.numel() * 8
         e2e = {"value": whole_job_mlups(world, nodes, args.steps, t_e2e), "unit": "MLUPS",
                "h2d_bytes_per_step": h2d / args.steps, "d2h_bytes_per_step": d2h / args.steps,
                "seconds": t_e2e,
-               "includes": "H2D of codes + initial populations (pinned), K steps, D2H of rho and u"}
+               "includes": "H2D of the initial populations (pinned; node codes handed over once at set-up), "
+                           "K steps, D2H of rho and u"}
     ctx.close()
 
+    multilevel = multilevel_block(max(16, args.steps), args.warmup, peak) if rank == 0 and args.multilevel else None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_sample(processes=1)
@@ -416,9 +457,7 @@ def run_ours(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "peak_kind": peak_kind, "algorithmic_bytes_per_launch": alg_bytes,
-                         "kernel": (f"aa_pair_kernel<{args.storage}, {COLLISION.upper()}> (two nodes per thread)"
-                                    if block and block[0] < 0 else
-                                    f"aa_step_kernel<D3Q19, {args.storage}, {COLLISION.upper()}>")},
+                         "kernel": kernel_name(block, args.storage)},
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": args.steps,
@@ -428,6 +467,8 @@ def run_ours(args):
         }
         if variants:
             out["storage_variants"] = variants
+        if multilevel:
+            out["multilevel"] = multilevel
         if closure:
             out["closure"] = closure
         print(json.dumps(out), flush=True)
@@ -451,6 +492,8 @@ def main():
     ap.add_argument("--tune", type=int, default=1, help="autotune the step kernel's block shape")
     ap.add_argument("--graph", type=int, default=1, help="replay steps as a captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--multilevel", type=int, default=1,
+                    help="multi-level cube-flow and cylinder-flow block (reference-built grids)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

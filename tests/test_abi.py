@@ -17,7 +17,7 @@ def test_library_exports_every_header_symbol():
 
 
 def test_abi_version():
-    assert zl.load_library().zl_abi_version() == 1
+    assert zl.load_library().zl_abi_version() == zl.ABI_VERSION == 2
 
 
 @pytest.mark.parametrize("mutate", [
@@ -95,4 +95,4 @@ def test_header_is_plain_c_and_links(tmp_path, compiler, std):
     subprocess.run([compiler, std, "-Wall", "-Werror", "-I", os.path.join(root, "include"), str(src), "-o", str(exe),
                     "-L", lib_dir, "-lzllbm_b200", f"-Wl,-rpath,{lib_dir}"], check=True)
     out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
-    assert out == ["1", "1", "1"]
+    assert out == ["2", "2", "1"]

@@ -28,7 +28,7 @@ def test_hit_pipeline_small_box_network_beats_smagorinsky_a_priori():
     from zllbm_b200.hit import HitConfig, run
     cfg = HitConfig(fine=128, factor=4, nu_fine=0.002, coarse_steps=400, checkpoints=4, train_snapshots=2,
                     train_steps=300, batch=128 * 64, closure_every=4, calibrate_alpha=(0.8, 1.0),
-                    calibrate_cs=(0.1,))
+                    calibrate_cs=(0.1,), test_realizations=2)
     res = run(cfg, log=lambda m: None)
     tr = res.training
     assert tr["val_loss"] < tr["val_loss_smagorinsky_y1"]
@@ -37,3 +37,7 @@ def test_hit_pipeline_small_box_network_beats_smagorinsky_a_priori():
         assert res.errors[name]["error"] is not None
         assert np.isfinite(res.errors[name]["error"])
         assert res.mlups[name] > 0
+        seeds = [r["seed"] for r in res.errors[name]["per_realization"]]
+        assert seeds == [cfg.seed + 1000, cfg.seed + 2000]
+        assert np.isfinite(res.errors[name]["error_std"])
+    assert len(res.errors["learned_minus_smagorinsky_calibrated"]["per_realization"]) == 2

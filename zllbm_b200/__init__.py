@@ -23,6 +23,8 @@ BC_NONE, BC_BOUNCE_BACK, BC_PERIODIC, BC_NONEQ_EXTRAPOLATION, BC_CONVECTIVE_OUTF
 STORAGE_F64, STORAGE_F32, STORAGE_F16, STORAGE_BF16 = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORAGE_F64, "f32": STORAGE_F32, "f16": STORAGE_F16, "bf16": STORAGE_BF16}
 BLOCK_ROW = 1 << 20  # zl_set_block x: one warp per x-row (ZL_BLOCK_ROW)
+ROUND_STOCHASTIC, ROUND_NEAREST = 0, 1  # zl_config.storage_rounding (stochastic is the default)
+ABI_VERSION = 2
 ERRORS = {-1: "EINVAL", -2: "ETOPOLOGY", -3: "EDEVICE", -4: "ETIMEOUT", -5: "ENAN", -6: "ESTATE",
           -7: "ETOOLARGE"}
 
@@ -55,6 +57,7 @@ class ZlConfig(ctypes.Structure):
         ("les_cs", ctypes.c_double),
         ("dx", ctypes.c_double),
         ("device", ctypes.c_int),
+        ("storage_rounding", ctypes.c_int),
     ]
 
 
@@ -211,6 +214,7 @@ class SolverConfig:
     les_cs: float = 0.0
     dx: float = 0.0
     device: int = 0
+    storage_rounding: int = 0  # ROUND_STOCHASTIC (default) or ROUND_NEAREST (FP16 / BF16 storage)
     extra: dict = field(default_factory=dict)
 
     @property
@@ -241,6 +245,7 @@ class SolverConfig:
         c.les_cs = self.les_cs
         c.dx = self.dx
         c.device = self.device
+        c.storage_rounding = self.storage_rounding
         return c
 
 

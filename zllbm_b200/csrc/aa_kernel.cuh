@@ -75,7 +75,55 @@ struct StepParams {
     double les_c;           // 18 Cs^2
     const float* c_node;    // learned closure: per-cell constant c (C = 18 c), or nullptr
     double conv_u[6];       // convective outflow: convection speed per face
+    // FP16 / BF16 stochastic rounding: two step seeds of the level in device memory (the even
+    // step reads [0] and its first thread writes [1] = [0] + 1, the odd step the other way round,
+    // so no launch reads a word another thread of it writes); nullptr: round to nearest
+    uint32_t* sr_seed;
 };
+
+// ---------------------------------------------------------------- stochastic rounding
+// Random bits for stochastic rounding: a counter-based stream per thread, seeded by the step
+// seed and the thread's node (or node pair, or lane) index through the "lowbias32" integer hash
+// (C. Wellons, 2018, public domain), advanced by a 32-bit linear congruential step (the
+// Numerical Recipes constants) whose output is folded (x ^ x >> 16) so that its low bits are
+// usable.  Deterministic: the same calls give the same bits.
+struct SrBits {
+    uint32_t h;
+    __device__ __forceinline__ static uint32_t mix(uint32_t x) {
+        x ^= x >> 16;
+        x *= 0x7feb352du;
+        x ^= x >> 15;
+        x *= 0x846ca68bu;
+        x ^= x >> 16;
+        return x;
+    }
+    __device__ __forceinline__ SrBits(uint32_t seed, uint32_t stream) : h(mix(mix(seed) ^ stream)) {}
+    __device__ __forceinline__ uint32_t next() {
+        h = h * 1664525u + 1013904223u;
+        return h ^ (h >> 16);
+    }
+};
+
+// The level's step seed for this layout phase, and its advance by the launch's first thread.
+__device__ __forceinline__ uint32_t sr_seed(const StepParams& p, bool odd) {
+    return p.sr_seed ? __ldcg(p.sr_seed + (odd ? 1 : 0)) : 0u;
+}
+__device__ __forceinline__ void sr_advance(const StepParams& p, bool odd, uint32_t seed, bool leader) {
+    if (p.sr_seed && leader) p.sr_seed[odd ? 0 : 1] = seed + 1u;
+}
+
+// FP32 -> FP16 / BF16 pairs with the sm_100 stochastic-rounding conversion (cvt.rs, random bits
+// from rbits); the first operand lands in the upper half, as with cvt.rn
+__device__ __forceinline__ uint32_t cvt_rs_f16x2(float hi, float lo, uint32_t rbits) {
+    uint32_t d;
+    asm("cvt.rs.f16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
+__device__ __forceinline__ uint32_t cvt_rs_bf16x2(float hi, float lo, uint32_t rbits) {
+    uint32_t d;
+    asm("cvt.rs.bf16x2.f32 %0, %1, %2, %3;" : "=r"(d) : "f"(hi), "f"(lo), "r"(rbits));
+    return d;
+}
 
 // Per-node extras handed to the collision.
 struct NodeForce {
@@ -90,6 +138,7 @@ template <> struct Storage<double> {
     static constexpr bool kScaled = false;
     ZL_HD static T load_raw(const double* p) { return *p; }
     ZL_HD static void store_raw(double* p, T v) { *p = v; }
+    ZL_HD static void store_raw_sr(double* p, T v, uint32_t) { *p = v; }
     ZL_HD static T load(const double* p, const StepParams&) { return *p; }
     ZL_HD static void store(double* p, T v, const StepParams&) { *p = v; }
 };
@@ -99,6 +148,7 @@ template <> struct Storage<float> {
     static constexpr bool kScaled = false;
     __device__ __forceinline__ static T load_raw(const float* p) { return __ldg(p); }
     __device__ __forceinline__ static void store_raw(float* p, T v) { *p = v; }
+    __device__ __forceinline__ static void store_raw_sr(float* p, T v, uint32_t) { *p = v; }
     __device__ __forceinline__ static T load(const float* p, const StepParams&) { return __ldg(p); }
     __device__ __forceinline__ static void store(float* p, T v, const StepParams&) { *p = v; }
 };
@@ -112,6 +162,10 @@ template <> struct Storage<__half> {
     static constexpr bool kScaled = true;
     __device__ __forceinline__ static T load_raw(const __half* p) { return __half2float(__ldg(p)); }
     __device__ __forceinline__ static void store_raw(__half* p, T v) { *p = __float2half_rn(v); }
+    __device__ __forceinline__ static void store_raw_sr(__half* p, T v, uint32_t rbits) {
+        const unsigned short h = (unsigned short)(cvt_rs_f16x2(0.f, v, rbits) & 0xffffu);
+        *reinterpret_cast<unsigned short*>(p) = h;
+    }
     __device__ __forceinline__ static T load(const __half* p, const StepParams& sp) {
         return load_raw(p) * sp.inv_scale;
     }
@@ -123,6 +177,10 @@ template <> struct Storage<__nv_bfloat16> {
     static constexpr bool kScaled = true;
     __device__ __forceinline__ static T load_raw(const __nv_bfloat16* p) { return __bfloat162float(__ldg(p)); }
     __device__ __forceinline__ static void store_raw(__nv_bfloat16* p, T v) { *p = __float2bfloat16_rn(v); }
+    __device__ __forceinline__ static void store_raw_sr(__nv_bfloat16* p, T v, uint32_t rbits) {
+        const unsigned short h = (unsigned short)(cvt_rs_bf16x2(0.f, v, rbits) & 0xffffu);
+        *reinterpret_cast<unsigned short*>(p) = h;
+    }
     __device__ __forceinline__ static T load(const __nv_bfloat16* p, const StepParams& sp) {
         return load_raw(p) * sp.inv_scale;
     }
@@ -641,6 +699,9 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
                                             const NodeForce* nf, float les_c = 0.f) {
     using Tb = Tables<L>;
     constexpr int Q = L::kQ;
+    // a node whose force is exactly zero (every node of a forced level outside the immersed-
+    // boundary band, with no constant force) takes the unforced update: the Guo terms vanish
+    if (nf && nf->F[0] == 0. && nf->F[1] == 0. && nf->F[2] == 0.) nf = nullptr;
     if constexpr (L::kQ == 19 && !Les) {
         if (coll == kMrt && !nf) {
             mrt_d3q19_fused(d, out, p, mac);
@@ -866,9 +927,17 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
             m[3] = (double)mac[3];
         }
 
+        if (sizeof(S) == 2 && p.sr_seed) {
+            // stochastic rounding of the 16-bit stores, one random stream per node
+            SrBits rng(sr_seed(p, Odd), (uint32_t)self);
 #pragma unroll
-        for (int q = 0; q < Q; ++q) St::store_raw(write_slot(q), post[q]);
-        if (Bnd || Masked) {
+            for (int q = 0; q < Q; ++q) St::store_raw_sr(write_slot(q), post[q], rng.next());
+        } else {
+#pragma unroll
+            for (int q = 0; q < Q; ++q) St::store_raw(write_slot(q), post[q]);
+        }
+        // a masked node with no missing upstream neighbour (bits 1 .. Q-1 clear) has nothing to patch
+        if ((Bnd || Masked) && (!Masked || (info & ((1u << Q) - 2u)))) {
             const int faces = Bnd ? (Masked ? (int)((info >> kInfoFaceShift) & 63u) : on_faces(geo, c, L::kDims)) : 0;
 #pragma unroll
             for (int q = 1; q < Q; ++q) {
@@ -958,6 +1027,15 @@ __device__ __forceinline__ void aa_node_periodic(S* __restrict__ f, const LevelG
     } else {
         collide_exact<L, Les>(pre, post, p, Coll, mac, Forced ? &nf : nullptr);
     }
+    if (sizeof(S) == 2 && p.sr_seed) {
+        SrBits rng(sr_seed(p, Odd), (uint32_t)(row + x));
+#pragma unroll
+        for (int q = 0; q < Q; ++q) {
+            if (Odd && q != 0) St::store_raw_sr(px[1 + Tb::cx(q)] + off(q, Tb::cy(q), Tb::cz(q)), post[q], rng.next());
+            else St::store_raw_sr(px[1] + off(Tb::opp(q), 0, 0), post[q], rng.next());
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < Q; ++q) {
         if (Odd && q != 0) St::store_raw(px[1 + Tb::cx(q)] + off(q, Tb::cy(q), Tb::cz(q)), post[q]);
@@ -979,6 +1057,8 @@ __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>:
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
     c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
     c.x[2] = blockIdx.z;
+    if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+        sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;
     if constexpr (!Bnd && !Masked) {
         if (c.x[1] > 0 && c.x[1] < geo.n[1] - 1 && (L::kDims == 2 || (c.x[2] > 0 && c.x[2] < geo.n[2] - 1))) {
@@ -1037,6 +1117,8 @@ __global__ void __launch_bounds__(kBatchThreads, 3) aa_batch_kernel(LevelBatch b
         int l = 0;  // uniform across the block
         while (l + 1 < b.count && base >= b.first[l + 1]) ++l;
         const LevelGeom& geo = b.geo[l];
+        if (sizeof(S) == 2 && base == b.first[l] && threadIdx.x == 0)
+            sr_advance(*b.params[l], b.odd[l], sr_seed(*b.params[l], b.odd[l]), true);
         const long long k64 = base + threadIdx.x - b.first[l];
         const long long cells = (long long)geo.n[0] * geo.n[1] * geo.n[2];
         if (k64 >= cells) continue;  // padding between two levels' ranges

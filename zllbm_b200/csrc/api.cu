@@ -66,11 +66,15 @@ struct Level {
     DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
     DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
     DeviceBuffer ib_nodes;   // every cell a vertex stencil touches, once
+    // the stencils resolved when the vertices are set: per (vertex, stencil node) pair its cell and
+    // delta weight; per stencil node the list of its pairs in vertex order (CSR)
+    DeviceBuffer ib_pair_cell, ib_pair_w, ib_csr_pair, ib_csr_start;
     int n_vertices = 0, n_ib_nodes = 0;
     int ib_width = 4;        // immersed-boundary stencil: 4 (reference) or 3 (Roma et al.)
     DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q doubles)
     bool c2f_last_valid = false;
     DeviceBuffer c_node;     // learned closure: c of the last network evaluation per cell
+    DeviceBuffer sr_seed;    // stochastic rounding: the two step seeds (StepParams::sr_seed)
 };
 
 }  // namespace
@@ -230,6 +234,8 @@ int zl_create(const zl_config* config, zl_ctx** out) {
     if (config->max_level < 0 || config->max_level >= ZL_MAX_LEVELS) return ZL_EINVAL;
     if (!(config->viscosity > 0.)) return ZL_EINVAL;
     if (config->les < ZL_LES_OFF || config->les > ZL_LES_LEARNED) return ZL_EINVAL;
+    if (config->storage_rounding != ZL_ROUND_NEAREST && config->storage_rounding != ZL_ROUND_STOCHASTIC)
+        return ZL_EINVAL;
     for (int f = 0; f < 6; ++f)
         if (config->bc_kind[f] < ZL_BC_NONE || config->bc_kind[f] > ZL_BC_CONVECTIVE_OUTFLOW) return ZL_EINVAL;
     const int dims = config->lattice == ZL_D2Q9 ? 2 : 3;
@@ -460,6 +466,14 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     p.scale = ctx->cfg.storage == ZL_STORAGE_F16 || ctx->cfg.storage == ZL_STORAGE_BF16 ? (float)scale : 1.f;
     p.inv_scale = 1.f / p.scale;
     p.scale_d = (double)p.scale;
+    // stochastic rounding of FP16 / BF16 stores: the level's seeds start at 0 with every set-up
+    L.sr_seed.release();
+    if ((ctx->cfg.storage == ZL_STORAGE_F16 || ctx->cfg.storage == ZL_STORAGE_BF16) &&
+        ctx->cfg.storage_rounding == ZL_ROUND_STOCHASTIC) {
+        if ((rc = alloc(ctx, L.sr_seed, 2 * sizeof(uint32_t)))) return rc;
+        ZL_CUDA(ctx, cudaMemset(L.sr_seed.ptr, 0, 2 * sizeof(uint32_t)));
+        p.sr_seed = (uint32_t*)L.sr_seed.ptr;
+    }
     if (ctx->cfg.collision == ZL_MRT && ctx->cfg.storage == ZL_STORAGE_F64) {
         std::vector<double> m(q * q);
         host_mrt_matrix(dims, 1. / p.tau, false, m.data());
@@ -1206,14 +1220,20 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     IbVertices v = ib_view(ctx, L, level);
     ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.params, L.even_layout, (const int*)L.ib_nodes.ptr,
                                     L.n_ib_nodes, (double*)L.force.ptr, (double*)L.ib_vel.ptr, ctx->stream));
-    // one warp per vertex, kIbWarps vertices per block
+    // interpolation: one warp per vertex, kIbWarps vertices per block; spread: one thread per node
     const unsigned blocks = (unsigned)((v.n + kIbWarps - 1) / kIbWarps), threads = 32 * kIbWarps;
+    const unsigned nblocks = (unsigned)((L.n_ib_nodes + 127) / 128);
+    const int* pc = (const int*)L.ib_pair_cell.ptr;
+    const double* pw = (const double*)L.ib_pair_w.ptr;
+    const int *cs = (const int*)L.ib_csr_start.ptr, *cp = (const int*)L.ib_csr_pair.ptr;
     if (ctx->dims == 2) {
-        ib_force_kernel<2><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<2><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+        ib_force_kernel<2><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<2><<<nblocks, 128, 0, ctx->stream>>>(L.params, v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs,
+                                                              cp, pw, (double*)L.force.ptr);
     } else {
-        ib_force_kernel<3><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, v, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<3><<<blocks, threads, 0, ctx->stream>>>(L.geo, L.map, L.params, v, (double*)L.force.ptr);
+        ib_force_kernel<3><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
+        ib_spread_kernel<3><<<nblocks, 128, 0, ctx->stream>>>(L.params, v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs,
+                                                              cp, pw, (double*)L.force.ptr);
     }
     ZL_CUDA(ctx, cudaGetLastError());
     return ZL_OK;
@@ -1299,6 +1319,43 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         if ((rc = alloc(ctx, L.ib_nodes, (size_t)std::max(nodes, 1) * 4))) return rc;
         ZL_CUDA(ctx, cudaMemcpyAsync(L.ib_nodes.ptr, sel.ptr, (size_t)nodes * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+        // the stencils resolved once: every (vertex, stencil node) pair's cell and delta weight, and
+        // each stencil node's pairs in vertex order (stable sort on the node's list index)
+        const long long pairs = (long long)n * K;
+        if (pairs >= 0x7fffffffll) return fail(ctx, ZL_ETOOLARGE, "level %d: too many vertex-node pairs", level);
+        {
+            DeviceBuffer node_of_cell, key, key_sorted, id, stmp;
+            if ((rc = alloc(ctx, node_of_cell, (size_t)cells * 4)) || (rc = alloc(ctx, key, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, key_sorted, (size_t)pairs * 4)) || (rc = alloc(ctx, id, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, L.ib_pair_cell, (size_t)pairs * 4)) || (rc = alloc(ctx, L.ib_pair_w, (size_t)pairs * 8)) ||
+                (rc = alloc(ctx, L.ib_csr_pair, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, L.ib_csr_start, (size_t)(nodes + 1) * 4)))
+                return rc;
+            ib_index_nodes_kernel<<<(nodes + 127) / 128, 128, 0, ctx->stream>>>((const int*)L.ib_nodes.ptr, nodes,
+                                                                               (int*)node_of_cell.ptr);
+            const unsigned pblocks = (unsigned)((pairs + 127) / 128);
+            if (ctx->dims == 2)
+                ib_pairs_kernel<2><<<pblocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const int*)node_of_cell.ptr,
+                                                                    (int*)L.ib_pair_cell.ptr, (double*)L.ib_pair_w.ptr,
+                                                                    (int*)key.ptr, (int*)id.ptr);
+            else
+                ib_pairs_kernel<3><<<pblocks, 128, 0, ctx->stream>>>(L.geo, L.map, v, (const int*)node_of_cell.ptr,
+                                                                    (int*)L.ib_pair_cell.ptr, (double*)L.ib_pair_w.ptr,
+                                                                    (int*)key.ptr, (int*)id.ptr);
+            ZL_CUDA(ctx, cudaGetLastError());
+            int bits = 1;
+            while ((1ll << bits) < (long long)nodes) ++bits;
+            size_t sbytes = 0;
+            ZL_CUDA(ctx, sort_pairs_by_key((const int*)key.ptr, (int*)key_sorted.ptr, (const int*)id.ptr,
+                                           (int*)L.ib_csr_pair.ptr, (int)pairs, bits, nullptr, &sbytes, ctx->stream));
+            if ((rc = alloc(ctx, stmp, std::max<size_t>(sbytes, 1)))) return rc;
+            ZL_CUDA(ctx, sort_pairs_by_key((const int*)key.ptr, (int*)key_sorted.ptr, (const int*)id.ptr,
+                                           (int*)L.ib_csr_pair.ptr, (int)pairs, bits, stmp.ptr, &sbytes, ctx->stream));
+            ib_csr_start_kernel<<<(unsigned)((pairs + 1 + 127) / 128), 128, 0, ctx->stream>>>(
+                (const int*)key_sorted.ptr, pairs, (int*)L.ib_csr_start.ptr, nodes);
+            ZL_CUDA(ctx, cudaGetLastError());
+            ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        }
         // the step reads node forces only where kInfoForce is set (forces elsewhere stay 0); the
         // bit is never cleared, released nodes keep it with a zero force
         if (L.info.ptr && nodes > 0) {

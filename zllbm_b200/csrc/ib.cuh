@@ -7,10 +7,13 @@
 //   2. every vertex interpolates the node velocities with the delta kernel and sets its force
 //      F = 2 (U_b - u) (:183-184, :318-320);
 //   3. every vertex spreads F delta area / (dt dx^(d-1)) into the node forces (:187-199, :322-339).
-// Launches 2 and 3 give each vertex a warp: the block's vertex records are staged in shared
-// memory, lanes take the stencil nodes, and the interpolation sums are warp-shuffle reductions;
-// the spread adds into the nodes with FP64 atomics.  Summation orders differ from the reference's
-// (an unordered_map walk and a sequential stencil loop); sums agree to rounding.
+// The stencils of a vertex set are resolved once, when the vertices are set (ib_pairs_kernel):
+// every (vertex, stencil node) pair gets its cell and FP64 delta weight, and every stencil node
+// the list of its pairs in vertex order (a CSR built by a stable radix sort).  Launch 2 gives each
+// vertex a warp that reads its pairs and sums with warp-shuffle reductions; launch 3 gives each
+// stencil node a thread that sums the shares of its vertices in vertex order, so the spread needs
+// no atomics and is deterministic.  Summation orders differ from the reference's (an unordered_map
+// walk and a sequential stencil loop); sums agree to rounding.
 //
 // Stencils: width 4 is the reference's StencilDisTwo (immersed_boundary.cpp:365-384); width 3 is
 // the three-point kernel of Roma, Peskin and Berger (J. Comput. Phys. 153, 1999), which the
@@ -200,84 +203,48 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepPara
 
 constexpr int kIbWarps = 4;  // vertices (warps) per block of the interpolation and spread kernels
 
-// This block's vertex records (coordinate, velocity, area) in shared memory.
-struct IbStage {
-    double coord[kIbWarps][3];
-    double vel[kIbWarps][3];
-    double area[kIbWarps];
-};
-
-__device__ __forceinline__ void ib_stage(const IbVertices& v, IbStage& s) {
-    const int base = blockIdx.x * kIbWarps;
-    for (int e = threadIdx.x; e < kIbWarps * 7; e += blockDim.x) {
-        const int w = e / 7, f = e % 7, i = base + w;
-        if (i >= v.n) continue;
-        if (f < 3) s.coord[w][f] = v.coord[i * 3 + f];
-        else if (f < 6) s.vel[w][f - 3] = v.vel[i * 3 + f - 3];
-        else s.area[w] = v.area[i];
-    }
-    __syncthreads();
-}
-
 __device__ __forceinline__ double warp_sum_d(double x) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
     return x;
 }
 
-// The warp's vertex: its stencil origin and the 1-D delta weights of each axis, computed once
-// (lanes 0 .. D * width - 1) instead of once per stencil node; a stencil node's weight is their
-// product in axis order, as ib_stencil_node forms it.
-struct IbWarpStencil {
-    double w[kIbWarps][3][4];
-};
-
+// Every (vertex i, stencil node k) pair, k over width^D nodes x fastest: the node's cell, its
+// index in the level's stencil-node list (the sort key of the CSR) and the delta weight, formed as
+// ib_stencil_node forms it (the 1-D weights multiplied in axis order).  Runs when the vertices are set.
 template <int D>
-__device__ __forceinline__ void ib_warp_weights(const IbVertices& v, const double* dis, IbWarpStencil& ws, int w,
-                                                int lane) {
-    if (lane < D * v.width) {
-        const int a = lane / v.width, o = lane % v.width;
-        ws.w[w][a][o] = ib_weight(v, dis[a], o);
-    }
-    __syncwarp();
+__global__ void ib_pairs_kernel(LevelGeom geo, LevelMap m, IbVertices v, const int* __restrict__ node_of_cell,
+                                int* __restrict__ pair_cell, double* __restrict__ pair_w, int* __restrict__ pair_node,
+                                int* __restrict__ pair_id) {
+    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)v.n * K) return;
+    const int i = (int)(t / K), k = (int)(t % K);
+    long long first[3], nid[3];
+    double dis[3];
+    ib_reference(v, v.coord + i * 3, D, first, dis);
+    const double w = ib_stencil_node(v, D, first, dis, k, nid);
+    const long long cell = ib_cell(geo, m, nid, D);  // present: checked by ib_mark_kernel
+    pair_cell[t] = (int)cell;
+    pair_w[t] = w;
+    pair_node[t] = node_of_cell[cell];
+    pair_id[t] = (int)t;
 }
 
+// Launch 2: a warp per vertex interpolates the node velocities through its pairs.
 template <int D>
-__device__ __forceinline__ double ib_node_weight(const IbVertices& v, const IbWarpStencil& ws, int w,
-                                                 const long long* first, int k, long long* nid) {
-    const int n = v.width;
-    const int o[3] = {k % n, (k / n) % n, k / (n * n)};
-    double weight = 1.;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        if (a < D) {
-            nid[a] = first[a] + o[a];
-            weight *= ws.w[w][a][o[a]];
-        } else {
-            nid[a] = 0;
-        }
-    }
-    return weight;
-}
-
-template <int D>
-__global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(LevelGeom geo, LevelMap m, IbVertices v,
+__global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(IbVertices v, const int* __restrict__ pair_cell,
+                                                                 const double* __restrict__ pair_w,
                                                                  const double* __restrict__ node_vel) {
-    __shared__ IbStage s;
-    __shared__ IbWarpStencil ws;
-    ib_stage(v, s);
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int i = blockIdx.x * kIbWarps + w;
     if (i >= v.n) return;
-    long long first[3], nid[3];
-    double dis[3];
-    ib_reference(v, s.coord[w], D, first, dis);
-    ib_warp_weights<D>(v, dis, ws, w, lane);
     const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    const long long base = (long long)i * K;
     double ur = 0., vr = 0., wr = 0.;
     for (int k = lane; k < K; k += 32) {
-        const double delta = ib_node_weight<D>(v, ws, w, first, k, nid);
-        const long long cell = ib_cell(geo, m, nid, D);
+        const long long cell = __ldg(pair_cell + base + k);
+        const double delta = __ldg(pair_w + base + k);
         ur += node_vel[cell * 3] * delta;
         vr += node_vel[cell * 3 + 1] * delta;
         if (D == 3) wr += node_vel[cell * 3 + 2] * delta;
@@ -286,34 +253,49 @@ __global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(LevelGeom geo, 
     vr = warp_sum_d(vr);
     if (D == 3) wr = warp_sum_d(wr);
     if (lane == 0) {
-        v.force[i * 3] = 2. * (s.vel[w][0] - ur);
-        v.force[i * 3 + 1] = 2. * (s.vel[w][1] - vr);
-        v.force[i * 3 + 2] = D == 3 ? 2. * (s.vel[w][2] - wr) : 0.;
+        v.force[i * 3] = 2. * (v.vel[i * 3] - ur);
+        v.force[i * 3 + 1] = 2. * (v.vel[i * 3 + 1] - vr);
+        v.force[i * 3 + 2] = D == 3 ? 2. * (v.vel[i * 3 + 2] - wr) : 0.;
     }
 }
 
+// Launch 3: a thread per stencil node sums F delta area / (dt dx^(d-1)) over its pairs, in vertex
+// order, and writes the node force (launch 1 zeroed it; no other pass adds to it).
 template <int D>
-__global__ void __launch_bounds__(32 * kIbWarps) ib_spread_kernel(LevelGeom geo, LevelMap m, StepParams p,
-                                                                  IbVertices v, double* __restrict__ node_force) {
-    __shared__ IbStage s;
-    __shared__ IbWarpStencil ws;
-    ib_stage(v, s);
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kIbWarps + w;
-    if (i >= v.n) return;
-    long long first[3], nid[3];
-    double dis[3];
-    ib_reference(v, s.coord[w], D, first, dis);
-    ib_warp_weights<D>(v, dis, ws, w, lane);
-    const double area = D == 3 ? s.area[w] / p.dt / v.dx / v.dx : s.area[w] / p.dt / v.dx;
-    const double F[3] = {v.force[i * 3], v.force[i * 3 + 1], v.force[i * 3 + 2]};
+__global__ void ib_spread_kernel(StepParams p, IbVertices v, const int* __restrict__ nodes, int n_nodes,
+                                 const int* __restrict__ csr_start, const int* __restrict__ csr_pair,
+                                 const double* __restrict__ pair_w, double* __restrict__ node_force) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n_nodes) return;
     const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
-    for (int k = lane; k < K; k += 32) {
-        const double delta = ib_node_weight<D>(v, ws, w, first, k, nid);
-        const long long cell = ib_cell(geo, m, nid, D);
-        const double dt = delta * area;
-        for (int a = 0; a < D; ++a) atomicAdd(node_force + cell * 3 + a, F[a] * dt);
+    double F[3] = {0., 0., 0.};
+    for (int s = csr_start[j]; s < csr_start[j + 1]; ++s) {
+        const int pr = csr_pair[s];
+        const int i = pr / K;
+        const double area = D == 3 ? v.area[i] / p.dt / v.dx / v.dx : v.area[i] / p.dt / v.dx;
+        const double dt = pair_w[pr] * area;
+        for (int a = 0; a < D; ++a) F[a] += v.force[i * 3 + a] * dt;
     }
+    const long long cell = nodes[j];
+    for (int a = 0; a < D; ++a) node_force[cell * 3 + a] = F[a];
+}
+
+// CSR row starts of the sorted pair keys (every stencil node owns at least one pair).
+static __global__ void ib_csr_start_kernel(const int* __restrict__ sorted_node, long long pairs,
+                                           int* __restrict__ start, int n_nodes) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t > pairs) return;
+    if (t == pairs) {
+        start[n_nodes] = (int)pairs;
+        return;
+    }
+    if (t == 0 || sorted_node[t] != sorted_node[t - 1]) start[sorted_node[t]] = (int)t;
+}
+
+// node_of_cell[nodes[j]] = j over the level's stencil-node list.
+static __global__ void ib_index_nodes_kernel(const int* __restrict__ nodes, int n_nodes, int* __restrict__ node_of_cell) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j < n_nodes) node_of_cell[nodes[j]] = j;
 }
 
 // Sum over vertices of F area / dx_background^(d-1) in vertex order (WriteTimeHisLagrangianForce,

@@ -267,6 +267,8 @@ __global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParam
 // arrays, in the reference's loop order (z outer, x inner, grid/grid_interpolation.cpp:485-517).
 // Every distinct source node is evaluated once per transfer (c2f_sources_kernel) into the
 // table g; the targets then form their weighted sums from the table.
+constexpr int kC2fThreads = 128;  // explosion kernel: 4 targets (warps) per block
+
 struct C2FStencil {
     const int* target;        // fine cell of every target node
     const int* offset;        // n_targets + 1
@@ -333,36 +335,44 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
 // targets get 0.5 (prev + value) instead, the time interpolation between the last transfer and
 // the coarse level's current state (no counterpart in the reference, whose explosion is spatial
 // only); store = 0 only saves.
+// One warp per target: lane q (< Q) sums population q over the target's sources in table order
+// (so FP64 keeps its summation order); the source rows are read coalesced, and the rows' indices
+// and weights are fetched 32 at a time and broadcast by shuffle.
 template <class L, class S>
-__global__ void c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even, StepParams fp, C2FStencil st,
-                           double* __restrict__ save, const double* __restrict__ prev, int store) {
+__global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
+                                                         StepParams fp, C2FStencil st, double* __restrict__ save,
+                                                         const double* __restrict__ prev, int store) {
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= st.n_targets) return;
+    const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= st.n_targets) return;  // whole warp
     const T* __restrict__ g = static_cast<const T*>(st.g);
-    T acc[Q];
-#pragma unroll
-    for (int q = 0; q < Q; ++q) acc[q] = (T)0;
-    for (int k = st.offset[t]; k < st.offset[t + 1]; ++k) {
-        const T w = (T)st.weight[k];
-        const T* gk = g + (long long)st.src[k] * Q;
-#pragma unroll
-        for (int q = 0; q < Q; ++q) acc[q] = acc[q] + w * gk[q];
+    const bool active = lane < Q;
+    const int q = active ? lane : 0;
+    T acc = (T)0;
+    const int k0 = st.offset[t], k1 = st.offset[t + 1];
+    for (int kb = k0; kb < k1; kb += 32) {
+        int src = 0;
+        double wd = 0.;
+        if (kb + lane < k1) {
+            src = st.src[kb + lane];
+            wd = st.weight[kb + lane];
+        }
+        const int m = k1 - kb < 32 ? k1 - kb : 32;
+        for (int j = 0; j < m; ++j) {
+            const int sj = __shfl_sync(0xffffffffu, src, j);
+            const T w = (T)__shfl_sync(0xffffffffu, wd, j);
+            acc = acc + w * g[(long long)sj * Q + q];
+        }
     }
-    if (save) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) save[(long long)t * Q + q] = (double)acc[q];
-    }
+    if (!active) return;
+    if (save) save[(long long)t * Q + q] = (double)acc;
     if (!store) return;
-    if (prev) {
-#pragma unroll
-        for (int q = 0; q < Q; ++q) acc[q] = (T)0.5 * ((T)prev[(long long)t * Q + q] + acc[q]);
-    }
+    if (prev) acc = (T)0.5 * ((T)prev[(long long)t * Q + q] + acc);
     const Coord c = cell_coord(fgeo, st.target[t]);
-#pragma unroll
-    for (int q = 0; q < Q; ++q) St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), acc[q], fp);
+    St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), acc, fp);
 }
 
 // Coalescence (TransferInfoToCoarseGrid, lbm_grid_interface.cpp:524-564): a coarse node of the

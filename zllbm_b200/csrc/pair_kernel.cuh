@@ -24,6 +24,7 @@ template <class S> struct PairIO;
 template <> struct PairIO<float> {
     __device__ __forceinline__ static F2 load(const float* p) { return {__ldg(reinterpret_cast<const float2*>(p))}; }
     __device__ __forceinline__ static void store(float* p, F2 v) { *reinterpret_cast<float2*>(p) = v.v; }
+    __device__ __forceinline__ static void store_sr(float* p, F2 v, uint32_t) { store(p, v); }
 };
 template <> struct PairIO<__half> {
     __device__ __forceinline__ static F2 load(const __half* p) {
@@ -32,6 +33,9 @@ template <> struct PairIO<__half> {
     __device__ __forceinline__ static void store(__half* p, F2 v) {
         *reinterpret_cast<__half2*>(p) = __float22half2_rn(v.v);
     }
+    __device__ __forceinline__ static void store_sr(__half* p, F2 v, uint32_t rbits) {
+        *reinterpret_cast<uint32_t*>(p) = cvt_rs_f16x2(v.v.y, v.v.x, rbits);
+    }
 };
 template <> struct PairIO<__nv_bfloat16> {
     __device__ __forceinline__ static F2 load(const __nv_bfloat16* p) {
@@ -39,6 +43,9 @@ template <> struct PairIO<__nv_bfloat16> {
     }
     __device__ __forceinline__ static void store(__nv_bfloat16* p, F2 v) {
         *reinterpret_cast<__nv_bfloat162*>(p) = __float22bfloat162_rn(v.v);
+    }
+    __device__ __forceinline__ static void store_sr(__nv_bfloat16* p, F2 v, uint32_t rbits) {
+        *reinterpret_cast<uint32_t*>(p) = cvt_rs_bf16x2(v.v.y, v.v.x, rbits);
     }
 };
 
@@ -151,6 +158,8 @@ __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, Leve
     using IO = PairIO<S>;
     const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
     const int y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
+        sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (x0 >= geo.n[0] || y >= geo.n[1]) return;
     if (!(y > 0 && y < geo.n[1] - 1 && z > 0 && z < geo.n[2] - 1)) {
         Coord c;
@@ -183,6 +192,24 @@ __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, Leve
         }
     }
     fused_pair<Coll == kMrt>(pre, post, p);
+    if (sizeof(S) == 2 && p.sr_seed) {
+        // stochastic rounding of the 16-bit stores, one random stream per node pair
+        SrBits rng(sr_seed(p, Odd), (uint32_t)((row + x0) >> 1));
+#pragma unroll
+        for (int q = 0; q < 19; ++q) {
+            const uint32_t r = rng.next();
+            if (!Odd || q == 0) {
+                IO::store_sr(pc[1] + off(Tb::opp(q), 0, 0), post[q], r);
+            } else if (Tb::cx(q) == 0) {
+                IO::store_sr(pc[1] + off(q, Tb::cy(q), Tb::cz(q)), post[q], r);
+            } else {
+                const long long o = off(q, Tb::cy(q), Tb::cz(q));
+                St::store_raw_sr(pc[1 + Tb::cx(q)] + o, post[q].v.x, r);
+                St::store_raw_sr(pc[2 + Tb::cx(q)] + o, post[q].v.y, r ^ 0x9e3779b9u);
+            }
+        }
+        return;
+    }
 #pragma unroll
     for (int q = 0; q < 19; ++q) {
         if (!Odd || q == 0) {

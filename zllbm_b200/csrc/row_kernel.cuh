@@ -30,6 +30,7 @@ template <> struct HalfPairIO<__half> {
         memcpy(&w, &h, 4);
         return w;
     }
+    __device__ __forceinline__ static uint32_t pack_sr(F2 v, uint32_t rbits) { return cvt_rs_f16x2(v.v.y, v.v.x, rbits); }
 };
 template <> struct HalfPairIO<__nv_bfloat16> {
     __device__ __forceinline__ static F2 unpack(uint32_t w) {
@@ -43,6 +44,7 @@ template <> struct HalfPairIO<__nv_bfloat16> {
         memcpy(&w, &h, 4);
         return w;
     }
+    __device__ __forceinline__ static uint32_t pack_sr(F2 v, uint32_t rbits) { return cvt_rs_bf16x2(v.v.y, v.v.x, rbits); }
 };
 
 // V 16-bit values of one plane as V / 2 32-bit words (element 2k in the low half of word k).
@@ -105,6 +107,7 @@ __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, Level
     const int lane = threadIdx.x & 31;
     const int y = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     const int z = blockIdx.y;
+    if ((blockIdx.x | blockIdx.y | threadIdx.x) == 0) sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (y >= geo.n[1]) return;  // whole warp: every shuffle below has all 32 lanes
     const int n1 = geo.n[1], n2 = geo.n[2];
     // element offsets of the rows (y + dy, z + dz), wrapped, plus this lane's first node
@@ -133,14 +136,22 @@ __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, Level
             else v[q] = r;
         }
     }
+    // stochastic rounding (p.sr_seed): one random stream per lane
+    const bool sr = p.sr_seed != nullptr;
+    SrBits rng(sr ? sr_seed(p, Odd) : 0u, (uint32_t)((geo.n[1] * z + y) * 32 + lane));
 #pragma unroll
     for (int k = 0; k < K; ++k) {
         F2 pre[19], post[19];
 #pragma unroll
         for (int q = 0; q < 19; ++q) pre[q] = IO::unpack(v[q].w[k]);
         fused_pair<Coll == kMrt>(pre, post, p);
+        if (sr) {
 #pragma unroll
-        for (int q = 0; q < 19; ++q) v[q].w[k] = IO::pack(post[q]);
+            for (int q = 0; q < 19; ++q) v[q].w[k] = IO::pack_sr(post[q], rng.next());
+        } else {
+#pragma unroll
+            for (int q = 0; q < 19; ++q) v[q].w[k] = IO::pack(post[q]);
+        }
     }
 #pragma unroll
     for (int q = 0; q < 19; ++q) {

@@ -242,4 +242,9 @@ cudaError_t select_marked(const uint32_t* mark, int n, int* out, int* count, voi
     return cub::DeviceSelect::Flagged(tmp, *tmp_bytes, thrust::counting_iterator<int>(0), mark, out, count, n, s);
 }
 
+cudaError_t sort_pairs_by_key(const int* keys_in, int* keys_out, const int* vals_in, int* vals_out, int n, int key_bits,
+                              void* tmp, size_t* tmp_bytes, cudaStream_t s) {
+    return cub::DeviceRadixSort::SortPairs(tmp, *tmp_bytes, keys_in, keys_out, vals_in, vals_out, n, 0, key_bits, s);
+}
+
 }  // namespace zl

@@ -19,6 +19,9 @@ cudaError_t launch_fill(int storage, void* f, long long stride, int q, const Ste
 cudaError_t launch_morton_neighbors(const uint64_t* codes, long long n, int dims, uint64_t* out, cudaStream_t s);
 cudaError_t launch_upstream_index(int dims, const uint64_t* sorted, const long long* order, long long n,
                                   long long* out, cudaStream_t s);
+// Stable radix sort of (key, value) pairs on the low key_bits bits of the keys (null tmp: size query).
+cudaError_t sort_pairs_by_key(const int* keys_in, int* keys_out, const int* vals_in, int* vals_out, int n, int key_bits,
+                              void* tmp, size_t* tmp_bytes, cudaStream_t s);
 cudaError_t select_marked(const uint32_t* mark, int n, int* out, int* count, void* tmp, size_t* tmp_bytes,
                           cudaStream_t s);
 

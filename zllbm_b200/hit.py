@@ -73,13 +73,13 @@ def spectrum_error(e_model: np.ndarray, e_ref: np.ndarray, k_max: int) -> float:
 
 
 def box_context(n: int, tau: float, storage: int = zl.STORAGE_F32, les: int = zl.LES_OFF, cs: float = 0.0,
-                collision: int = zl.SRT, device: int = 0) -> zl.Context:
+                collision: int = zl.SRT, device: int = 0, rounding: int = zl.ROUND_STOCHASTIC) -> zl.Context:
     """A full periodic n^3 box level issuing on torch's current stream (so that torch work on the
     fields and the library's kernels stay ordered; that stream must not be the legacy default one)."""
     import torch
     cfg = zl.SolverConfig(lattice=zl.D3Q19, collision=collision, storage=storage, viscosity=(tau - 0.5) / 3.0,
                           bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(0, 0, 0), domain_max=(n, n, n), les=les,
-                          les_cs=cs, device=device)
+                          les_cs=cs, device=device, storage_rounding=rounding)
     ctx = zl.Context(cfg)
     ctx.set_stream(torch.cuda.current_stream().cuda_stream or None)
     ctx.set_level_box(0, (0, 0, 0), (n, n, n))
@@ -101,8 +101,11 @@ class HitConfig:
     batch: int = 128 * 148 * 2
     lr: float = 2e-3           # cosine-decayed to lr / 20
     closure_every: int = 8     # the amortised variant evaluates the network on every k-th step
-    calibrate_alpha: tuple = (0.2, 0.3, 0.4, 0.5, 0.6, 0.8, 1.0)      # network output scales tried
-    calibrate_cs: tuple = (0.05, 0.06, 0.07, 0.08, 0.09, 0.1, 0.12)   # Smagorinsky constants tried
+    # network output scales and Smagorinsky constants tried by the calibration (both searches
+    # reach well below the optima seen so far, alpha 0.3 - 0.5 and Cs 0.06 - 0.08)
+    calibrate_alpha: tuple = (0.05, 0.1, 0.15, 0.2, 0.25, 0.3, 0.4, 0.5, 0.6, 0.8, 1.0)
+    calibrate_cs: tuple = (0.02, 0.03, 0.04, 0.05, 0.06, 0.07, 0.08, 0.09, 0.1, 0.12)
+    test_realizations: int = 3  # independent test fields (seeds seed + 1000 k, k = 1 ..)
     storage: int = zl.STORAGE_F32
     fine_storage: int = zl.STORAGE_F32
     cs: float = 0.1
@@ -370,9 +373,9 @@ def coarse_run(cfg: HitConfig, ref: FineReference, ck_times, les: int, cs: float
 def _run(cfg: HitConfig, log=print) -> HitResult:
     """Training realization (seed): fine run, training pairs, network training, and a one-number
     calibration of the network output scale (and, for a fair comparison, of the Smagorinsky
-    constant) against its filtered spectra.  Test realization (seed + 1000): a fresh fine run
-    against which Smagorinsky (configured and calibrated constant) and the learned closure
-    (raw and calibrated) are scored."""
+    constant) against its filtered spectra.  Test realizations (seeds seed + 1000 k): fresh fine
+    runs against which Smagorinsky (configured and calibrated constant) and the learned closure
+    (raw and calibrated) are scored; errors are the mean over realizations with their spread."""
     import torch
     res = HitResult(config={**cfg.__dict__, "coarse": cfg.coarse, "tau_fine": cfg.tau_fine,
                             "tau_coarse": cfg.tau_coarse})
@@ -408,9 +411,7 @@ def _run(cfg: HitConfig, log=print) -> HitResult:
     del train_ref
     torch.cuda.empty_cache()
 
-    # evaluation on an independent realization
-    test_ref = fine_reference(cfg, cfg.seed + 1000, ck_times, (), log)
-    res.spectra["filtered_fine"] = {str(k): v.tolist() for k, v in test_ref.spectra.items()}
+    # evaluation on independent realizations: every model scored on each, mean and spread reported
     net_cal = scaled_net(net, alpha)
     runs = [("smagorinsky", zl.LES_SMAGORINSKY, cfg.cs, None, 1),
             (f"smagorinsky_calibrated", zl.LES_SMAGORINSKY, cs_best, None, 1),
@@ -418,13 +419,35 @@ def _run(cfg: HitConfig, log=print) -> HitResult:
             ("learned_calibrated", zl.LES_LEARNED, cfg.cs, net_cal, 1),
             (f"learned_calibrated_every{cfg.closure_every}", zl.LES_LEARNED, cfg.cs, net_cal, cfg.closure_every)]
     res.training["coarse_predicted_y"] = {}
-    for name, les, cs, n_, k in runs:
-        r = coarse_run(cfg, test_ref, ck_times, les, cs, n_, k, diagnose=n_ is not None)
-        res.spectra[name] = r.pop("spectra")
-        res.training["coarse_predicted_y"][name] = r.pop("predicted_y")
-        res.mlups[name] = r.pop("mlups")
-        res.errors[name] = r
-        log(f"{name}: spectrum error {r['error']} (k <= n/4: {r['error_k_le_n/4']}), {res.mlups[name]} MLUPS")
+    per = {name: [] for name, *_ in runs}
+    for t in range(max(1, cfg.test_realizations)):
+        seed = cfg.seed + 1000 * (t + 1)
+        test_ref = fine_reference(cfg, seed, ck_times, (), log)
+        if t == 0:
+            res.spectra["filtered_fine"] = {str(k): v.tolist() for k, v in test_ref.spectra.items()}
+        for name, les, cs, n_, k in runs:
+            r = coarse_run(cfg, test_ref, ck_times, les, cs, n_, k, diagnose=n_ is not None and t == 0)
+            spectra, pred, mlups = r.pop("spectra"), r.pop("predicted_y"), r.pop("mlups")
+            if t == 0:
+                res.spectra[name] = spectra
+                res.training["coarse_predicted_y"][name] = pred
+                res.mlups[name] = mlups
+            per[name].append({"seed": seed, **r})
+            log(f"{name} (seed {seed}): spectrum error {r['error']} (k <= n/4: {r['error_k_le_n/4']})")
+        del test_ref
+        torch.cuda.empty_cache()
+    for name, rs in per.items():
+        # a run without a finite spectrum (unstable) scores infinity
+        errs = np.array([np.inf if r["error"] is None else r["error"] for r in rs], dtype=np.float64)
+        low = np.array([np.inf if r["error_k_le_n/4"] is None else r["error_k_le_n/4"] for r in rs], dtype=np.float64)
+        res.errors[name] = {"error": float(errs.mean()), "error_std": float(errs.std(ddof=1)) if errs.size > 1 else 0.0,
+                            "error_k_le_n/4": float(low.mean()), "per_realization": rs}
+    # the learned closure against Smagorinsky calibrated the same way, realization by realization
+    diff = np.array([(np.inf if a["error"] is None else a["error"]) - (np.inf if b["error"] is None else b["error"])
+                     for a, b in zip(per["learned_calibrated"], per["smagorinsky_calibrated"])])
+    res.errors["learned_minus_smagorinsky_calibrated"] = {"mean": float(diff.mean()),
+                                                          "std": float(diff.std(ddof=1)) if diff.size > 1 else 0.0,
+                                                          "per_realization": diff.tolist()}
     res.mlups["cost"] = closure_cost(net_cal, max(256, nc), cfg.tau_coarse, (1, 8, 16, cfg.closure_every))
     log(f"closure cost on {max(256, nc)}^3: {res.mlups['cost']}")
     res.training["net"] = net.flat().tolist()
@@ -446,12 +469,13 @@ def main(argv=None):
     ap.add_argument("--every", type=int, default=8)
 
     ap.add_argument("--seed", type=int, default=20261203)
+    ap.add_argument("--test-realizations", type=int, default=3)
     ap.add_argument("--fine-storage", default="f32")
     ap.add_argument("--out", default=None)
     a = ap.parse_args(argv)
     cfg = HitConfig(fine=a.fine, factor=a.factor, nu_fine=a.nu, coarse_steps=a.coarse_steps,
                     checkpoints=a.checkpoints, train_snapshots=a.snapshots, train_steps=a.train_steps,
-                    closure_every=a.every, seed=a.seed,
+                    closure_every=a.every, seed=a.seed, test_realizations=a.test_realizations,
 
                     fine_storage=zl.STORAGE_NAMES[a.fine_storage])
     res = run(cfg, log=lambda m: print(m, flush=True))

@@ -3,7 +3,7 @@ tau = 0.55): the same run in FP64, FP32, FP16-deviation and BF16-deviation stora
 velocity's relative L2 error against the FP64 run and the kinetic-energy decay at checkpoints.
 
     python -m zllbm_b200.tgv_accuracy [--cells 256] [--steps 5000] [--checkpoints 5] [--out file.json]
-                                      [--storages f32,f16,bf16]
+                                      [--storages f32,f16,f16rn,bf16,bf16rn]
 
 FP64 storage is the device path that is bit-exact to the reference's own solver, so it is the
 FP64 oracle of the comparison.  Every run starts from feq(rho, u) of the analytic TGV fields
@@ -11,7 +11,9 @@ FP64 oracle of the comparison.  Every run starts from feq(rho, u) of the analyti
 linear viscous decay exp(-2 nu |k|^2 t), |k|^2 = 3 (2 pi / N)^2 (the u0 = 0.05 vortex is nearly
 linear at these Reynolds numbers).  Each error is also split into an amplitude part (the
 projection on the FP64 field, a = <u, u64> / <u64, u64>: a - 1 is a decay-rate bias) and the part
-orthogonal to it (|u - a u64| / |u64|: noise and shape errors).
+orthogonal to it (|u - a u64| / |u64|: noise and shape errors).  FP16 / BF16 store with the
+library's default stochastic rounding; a name ending in "rn" (f16rn, bf16rn) rounds to nearest.  The 16-bit runs take the
+benchmark's kernel where it applies (one warp per x-row for 128- and 256-node rows).
 """
 from __future__ import annotations
 
@@ -44,8 +46,13 @@ def run_storage(storage: str, n: int, steps: int, checkpoints: int, log=print):
     from zllbm_b200.hit import box_context
     every = steps // checkpoints
     out = []
+    rn = storage.endswith("rn")
+    base = storage[:-2] if rn else storage
     with torch.cuda.stream(torch.cuda.Stream()):
-        ctx = box_context(n, TAU, storage=zl.STORAGE_NAMES[storage], collision=zl.MRT)
+        ctx = box_context(n, TAU, storage=zl.STORAGE_NAMES[base], collision=zl.MRT,
+                          rounding=zl.ROUND_NEAREST if rn else zl.ROUND_STOCHASTIC)
+        if zl.STORAGE_NAMES[base] in (zl.STORAGE_F16, zl.STORAGE_BF16) and n in (128, 256):
+            ctx.set_block(0, zl.BLOCK_ROW, 1)
         rho, u = tgv_fields(n)
         ctx.set_equilibrium_dense(0, rho.data_ptr(), u.data_ptr())
         ctx.synchronize()
@@ -66,7 +73,7 @@ def run_storage(storage: str, n: int, steps: int, checkpoints: int, log=print):
 
 
 def run(n: int = 256, steps: int = 5000, checkpoints: int = 5, log=print,
-        storages: tuple = ("f32", "f16", "bf16")) -> dict:
+        storages: tuple = ("f32", "f16", "f16rn", "bf16", "bf16rn")) -> dict:
     import torch
     nu = (TAU - 0.5) / 3.0
     k2 = 3.0 * (2.0 * math.pi / n) ** 2
@@ -107,7 +114,7 @@ def main(argv=None):
     ap.add_argument("--steps", type=int, default=5000)
     ap.add_argument("--checkpoints", type=int, default=5)
     ap.add_argument("--out", default=None)
-    ap.add_argument("--storages", default="f32,f16,bf16")
+    ap.add_argument("--storages", default="f32,f16,f16rn,bf16,bf16rn")
     a = ap.parse_args(argv)
     res = run(a.cells, a.steps, a.checkpoints, storages=tuple(a.storages.split(",")))
     text = json.dumps(res, indent=1)
