@@ -554,6 +554,86 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
     for (int q = 0; q < 19; ++q) out[q] = fmaf(-omega, n[q], d[q]) - c[q];
 }
 
+// D3Q19 SRT without forcing, optionally with Smagorinsky, in one pass over the deviations d
+// (scaled units): the pair sums / differences of opposite directions give the density, momentum
+// and second moments; the non-equilibrium stress of the reference's second-order equilibrium
+// (lbm_solver_interface.cpp:374-435) is then Pi_ab = sum_q c_a c_b d_q - drho / 3 delta_ab - G u_a u_b
+// (G = scale rho), its diagonal sums S1 + Sxy + Sxz (x), ... and its off-diagonal S4 - S5 (xy),
+// S6 - S7 (xz), S8 - S9 (yz).  Smagorinsky: tau = tau0 + (sqrt(tau0^2 + C sqrt(2 Pi:Pi)) - tau0) / 2
+// (lbm_les_smagorinsky.cpp:22-94 with the increment added to tau0).  The update
+// f*_q = (1 - omega) d_q + omega feq_q is formed per opposite pair from its sum and difference:
+// feq_q = w (B + 4.5 G (c.u)^2) + 3 w (c.j), B = drho - 1.5 G u^2.
+__device__ __forceinline__ void srt_d3q19_fused(const float* d, float* out, const StepParams& p, float* mac,
+                                                bool les, float les_c) {
+    const float S1 = d[1] + d[2], D1 = d[1] - d[2];
+    const float S2 = d[3] + d[4], D2 = d[3] - d[4];
+    const float S3 = d[5] + d[6], D3 = d[5] - d[6];
+    const float S4 = d[7] + d[10], D4 = d[7] - d[10];
+    const float S5 = d[8] + d[9], D5 = d[8] - d[9];
+    const float S6 = d[11] + d[14], D6 = d[11] - d[14];
+    const float S7 = d[12] + d[13], D7 = d[12] - d[13];
+    const float S8 = d[15] + d[18], D8 = d[15] - d[18];
+    const float S9 = d[16] + d[17], D9 = d[16] - d[17];
+    const float Sxy = S4 + S5, Sxz = S6 + S7, Syz = S8 + S9;
+    const float drho = ((d[0] + S1) + (S2 + S3)) + ((Sxy + Sxz) + Syz);
+    const float jx = D1 + (D4 - D5) + (D6 - D7);
+    const float jy = D2 + (D4 + D5) + (D8 - D9);
+    const float jz = D3 + (D6 + D7) + (D8 + D9);
+    const float rho = fmaf(drho, p.inv_scale, 1.f);
+    const float k = __fdividef(p.inv_scale, rho);  // fast reciprocal, two ulps (rho is close to 1)
+    const float ux = jx * k, uy = jy * k, uz = jz * k;
+    mac[0] = rho;
+    mac[1] = ux;
+    mac[2] = uy;
+    mac[3] = uz;
+    const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
+    const float G = p.scale * rho;
+    float omega = p.omega32;
+    if (les) {
+        const float t = drho * (1.f / 3.f);
+        const float pxx = fmaf(-G, ux2, (S1 + Sxy + Sxz) - t);
+        const float pyy = fmaf(-G, uy2, (S2 + Sxy + Syz) - t);
+        const float pzz = fmaf(-G, uz2, (S3 + Sxz + Syz) - t);
+        const float pxy = fmaf(-G, ux * uy, S4 - S5);
+        const float pxz = fmaf(-G, ux * uz, S6 - S7);
+        const float pyz = fmaf(-G, uy * uz, S8 - S9);
+        const float is2 = p.inv_scale * p.inv_scale;
+        const float pi2 = is2 * (pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz));
+        const float tau0 = (float)p.tau;
+        const float tau = tau0 + 0.5f * (sqrtf(tau0 * tau0 + les_c * sqrtf(2.f * pi2)) - tau0);
+        omega = 1.f / tau;
+    }
+    const float B = fmaf(-1.5f * G, ux2 + uy2 + uz2, drho);
+    const float h = 0.5f * (1.f - omega);
+    const float ow0 = omega * (1.f / 3.f), ow1 = omega * (1.f / 18.f), ow2 = omega * (1.f / 36.f);
+    const float K1 = 4.5f * ow1 * G, L1 = ow1 * B, o1 = 3.f * ow1;
+    const float K2 = 4.5f * ow2 * G, L2 = ow2 * B, o2 = 3.f * ow2;
+    out[0] = fmaf(1.f - omega, d[0], ow0 * B);
+    auto pair = [&](int q, int o, float S, float D, float even, float odd) {
+        const float e = fmaf(h, S, even), od = fmaf(h, D, odd);
+        out[q] = e + od;
+        out[o] = e - od;
+    };
+    pair(1, 2, S1, D1, fmaf(K1, ux2, L1), o1 * jx);
+    pair(3, 4, S2, D2, fmaf(K1, uy2, L1), o1 * jy);
+    pair(5, 6, S3, D3, fmaf(K1, uz2, L1), o1 * jz);
+    {
+        const float a = ux + uy, b = uy - ux;
+        pair(7, 10, S4, D4, fmaf(K2, a * a, L2), o2 * (jx + jy));
+        pair(8, 9, S5, D5, fmaf(K2, b * b, L2), o2 * (jy - jx));
+    }
+    {
+        const float a = ux + uz, b = uz - ux;
+        pair(11, 14, S6, D6, fmaf(K2, a * a, L2), o2 * (jx + jz));
+        pair(12, 13, S7, D7, fmaf(K2, b * b, L2), o2 * (jz - jx));
+    }
+    {
+        const float a = uy + uz, b = uz - uy;
+        pair(15, 18, S8, D8, fmaf(K2, a * a, L2), o2 * (jy + jz));
+        pair(16, 17, S9, D9, fmaf(K2, b * b, L2), o2 * (jz - jy));
+    }
+}
+
 // D3Q19 MRT without forcing or LES, in one pass over the deviations d (scaled units).
 //
 // The same update as feq_neq_dev + mrt_d3q19_dev, f* = f - omega neq - sum_k lambda_k m_k M_k,
@@ -702,9 +782,13 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
     // a node whose force is exactly zero (every node of a forced level outside the immersed-
     // boundary band, with no constant force) takes the unforced update: the Guo terms vanish
     if (nf && nf->F[0] == 0. && nf->F[1] == 0. && nf->F[2] == 0.) nf = nullptr;
-    if constexpr (L::kQ == 19 && !Les) {
-        if (coll == kMrt && !nf) {
+    if constexpr (L::kQ == 19) {
+        if (coll == kMrt && !nf && !Les) {
             mrt_d3q19_fused(d, out, p, mac);
+            return;
+        }
+        if (coll == kSrt && !nf) {
+            srt_d3q19_fused(d, out, p, mac, Les, les_c);
             return;
         }
     }

@@ -267,14 +267,37 @@ __global__ void ib_spread_kernel(StepParams p, IbVertices v, const int* __restri
                                  const double* __restrict__ pair_w, double* __restrict__ node_force) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_nodes) return;
-    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    const FastDiv K = FastDiv::make(D == 3 ? v.width * v.width * v.width : v.width * v.width);
     double F[3] = {0., 0., 0.};
-    for (int s = csr_start[j]; s < csr_start[j + 1]; ++s) {
-        const int pr = csr_pair[s];
-        const int i = pr / K;
+    auto add = [&](double w, int i, const double* f) {
         const double area = D == 3 ? v.area[i] / p.dt / v.dx / v.dx : v.area[i] / p.dt / v.dx;
-        const double dt = pair_w[pr] * area;
-        for (int a = 0; a < D; ++a) F[a] += v.force[i * 3 + a] * dt;
+        const double dt = w * area;
+        for (int a = 0; a < D; ++a) F[a] += f[a] * dt;
+    };
+    const int s1 = csr_start[j + 1];
+    int s = csr_start[j];
+    // four pairs per round: their loads are issued before the sums (kept in pair order)
+    for (; s + 4 <= s1; s += 4) {
+        int i4[4];
+        double w4[4], f4[4][3];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int pr = __ldg(csr_pair + s + e);
+            i4[e] = (int)K.div((uint32_t)pr);
+            w4[e] = __ldg(pair_w + pr);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+#pragma unroll
+            for (int a = 0; a < D; ++a) f4[e][a] = v.force[i4[e] * 3 + a];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) add(w4[e], i4[e], f4[e]);
+    }
+    for (; s < s1; ++s) {
+        const int pr = __ldg(csr_pair + s);
+        const int i = (int)K.div((uint32_t)pr);
+        const double f1[3] = {v.force[i * 3], v.force[i * 3 + 1], D == 3 ? v.force[i * 3 + 2] : 0.};
+        add(__ldg(pair_w + pr), i, f1);
     }
     const long long cell = nodes[j];
     for (int a = 0; a < D; ++a) node_force[cell * 3 + a] = F[a];

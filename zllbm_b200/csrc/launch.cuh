@@ -200,13 +200,14 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
                         const int* coarse_cell, const int* fine_cell, int n, const double* fine_macro,           \
                         double tau_ratio, cudaStream_t s) {                                                      \
         if (n <= 0) return cudaSuccess;                                                                          \
-        const unsigned blocks = (unsigned)((n + 127) / 128);                                                     \
+        /* a few thousand targets: one-warp blocks spread them over every SM */                                  \
+        const unsigned blocks = (unsigned)((n + 31) / 32);                                                       \
         if (dims == 2)                                                                                           \
-            f2c_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp, \
-                                                       coarse_cell, fine_cell, n, fine_macro, tau_ratio);        \
+            f2c_kernel<D2Q9, S><<<blocks, 32, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
+                                                      coarse_cell, fine_cell, n, fine_macro, tau_ratio);         \
         else                                                                                                     \
-            f2c_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,    \
-                                                        cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);   \
+            f2c_kernel<D3Q19, S><<<blocks, 32, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,     \
+                                                       cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);    \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even,      \

@@ -336,8 +336,9 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
 // the coarse level's current state (no counterpart in the reference, whose explosion is spatial
 // only); store = 0 only saves.
 // One warp per target: lane q (< Q) sums population q over the target's sources in table order
-// (so FP64 keeps its summation order); the source rows are read coalesced, and the rows' indices
-// and weights are fetched 32 at a time and broadcast by shuffle.
+// (so FP64 keeps its summation order); the source rows are read coalesced, four rows' loads in
+// flight at a time, and the rows' indices and weights are fetched 32 at a time and broadcast by
+// shuffle.
 template <class L, class S>
 __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
                                                          StepParams fp, C2FStencil st, double* __restrict__ save,
@@ -361,10 +362,23 @@ __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, Le
             wd = st.weight[kb + lane];
         }
         const int m = k1 - kb < 32 ? k1 - kb : 32;
-        for (int j = 0; j < m; ++j) {
+        int j = 0;
+        // four rows per round: their loads are issued before the sums that use them
+        for (; j + 4 <= m; j += 4) {
+            T w4[4], g4[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int sj = __shfl_sync(0xffffffffu, src, j + e);
+                w4[e] = (T)__shfl_sync(0xffffffffu, wd, j + e);
+                g4[e] = __ldg(g + (long long)sj * Q + q);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc = acc + w4[e] * g4[e];
+        }
+        for (; j < m; ++j) {
             const int sj = __shfl_sync(0xffffffffu, src, j);
             const T w = (T)__shfl_sync(0xffffffffu, wd, j);
-            acc = acc + w * g[(long long)sj * Q + q];
+            acc = acc + w * __ldg(g + (long long)sj * Q + q);
         }
     }
     if (!active) return;
