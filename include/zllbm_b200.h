@@ -284,6 +284,25 @@ int zl_ib_set_delta(zl_ctx* ctx, int level, int width);
    in FP64 (total[3], may be NULL; WriteTimeHisLagrangianForce, :596-642). */
 int zl_ib_get_forces(zl_ctx* ctx, int level, double* vertex_forces, double* total);
 
+/* ---------------------------------------------------------------- halo faces (slab sharding)
+   A level can be one slab of a lattice split across several contexts (one per GPU), the way the
+   reference splits its grid over MPI ranks (halo of one node layer per level sub-step,
+   amr_project/mpi/mpi_grid_communication.cpp:210-357).  A halo face has ZL_BC_NONE and the level
+   box on the domain face; zl_set_level_halo makes its ghost cells hold the neighbour's slots
+   (present for the lookups of the nodes next to them, never stepped).  Single-level contexts
+   without forcing.  With the single-buffer AA pattern an even step touches only a node's own
+   slots, so a pair of steps needs two exchanges per face:
+     stage 0, after an even step: zl_halo_pack(face, 0) on this context -> zl_halo_unpack(opposite
+       face, 0) on the neighbour (the boundary plane's populations that enter the neighbour);
+     stage 1, after an odd step: zl_halo_pack(face, 1) -> zl_halo_unpack(opposite face, 1) on the
+       neighbour (the populations this context's nodes wrote into its ghost plane, which belong to
+       the neighbour's boundary nodes).
+   Buffers are device buffers of zl_halo_bytes; the populations are the storage's raw elements. */
+int zl_set_level_halo(zl_ctx* ctx, int level, int faces); /* faces: bit f = face slot f */
+int zl_halo_bytes(zl_ctx* ctx, int level, int face, int64_t* bytes);
+int zl_halo_pack(zl_ctx* ctx, int level, int face, int stage, void* buf_device);
+int zl_halo_unpack(zl_ctx* ctx, int level, int face, int stage, const void* buf_device);
+
 /* ABI version of the loaded library. */
 int zl_abi_version(void);
 

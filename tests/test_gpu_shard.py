@@ -1,0 +1,141 @@
+"""Slab sharding on the device (zl_set_level_halo, zl_halo_pack / zl_halo_unpack, zllbm_b200.shard):
+a lattice split into 2 or 3 slabs of its last axis, one context per slab on one GPU, stepped by
+the sharding schedule with the halo buffers routed between the contexts, equals the same lattice
+in one context bit for bit (FP64 and FP32 storage; the step kernels' arithmetic does not depend on
+where a node lies), for periodic and wall-bounded split axes, D3Q19 and D2Q9."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _config(dims, storage, periodic_split, coll):
+    import zllbm_b200 as zl
+    n = (24, 16, 20) if dims == 3 else (40, 36)
+    kinds = [zl.BC_PERIODIC] * (2 * dims)
+    vel = [(0.0, 0.0, 0.0)] * 6
+    if not periodic_split:  # walls on the split axis, the high one moving
+        kinds[2 * dims - 2] = kinds[2 * dims - 1] = zl.BC_BOUNCE_BACK
+        vel[2 * dims - 1] = (0.05, 0.0, 0.0)
+    lo = (1,) * dims
+    hi = tuple(1 + n[a] for a in range(dims))
+    cfg = zl.SolverConfig(lattice=zl.D3Q19 if dims == 3 else zl.D2Q9, collision=coll, storage=storage,
+                          viscosity=0.02, rho0=1.0, bc_kind=tuple(kinds) + (0,) * (6 - 2 * dims),
+                          bc_velocity=tuple(vel), domain_min=lo, domain_max=hi)
+    return cfg
+
+
+def _box(cfg):
+    """(lo, n) of the context's level-0 box: unique nodes (periodic axes drop the duplicate plane)."""
+    import zllbm_b200 as zl
+    d = cfg.dims
+    lo = tuple(cfg.domain_min[:d])
+    n = tuple(cfg.domain_max[a] - cfg.domain_min[a] + (0 if cfg.bc_kind[2 * a] == zl.BC_PERIODIC else 1)
+              for a in range(d))
+    return lo, n
+
+
+def _codes(dims, lo, n):
+    import zllbm_b200 as zl
+    return zl.box_codes(dims, lo, tuple(lo[a] + n[a] - 1 for a in range(dims)))
+
+
+def _populations(cfg, codes, seed=5):
+    """Seeded perturbation of the rest state per node, a function of the node's code only."""
+    q = cfg.q
+    w = np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4) if q == 9 else np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
+    rng = np.random.default_rng(seed)
+    table = 1 + 0.05 * rng.standard_normal((int(codes.max()) + 1, q))
+    return np.ascontiguousarray(w * table[codes.astype(np.int64)])
+
+
+@pytest.mark.parametrize("storage", [0, 1])  # FP64, FP32
+@pytest.mark.parametrize("periodic_split", [True, False])
+@pytest.mark.parametrize("dims,world", [(3, 2), (3, 3), (2, 3)])
+def test_slabs_equal_single_context(dims, world, periodic_split, storage):
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, LocalRing, Ring, slab_range, split_planes
+    cfg = _config(dims, storage, periodic_split, zl.MRT)
+    glo, gn = _box(cfg)
+    gcodes = _codes(dims, glo, gn)
+    f0 = _populations(cfg, gcodes)
+    steps = 8
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, glo + (0,) * (3 - dims), gn + (1,) * (3 - dims))
+        ctx.set_populations(0, gcodes, f0)
+        ctx.advance(steps)
+        ref = ctx.get_populations(0, gcodes)
+    ref_by_code = dict(zip(gcodes.tolist(), range(gcodes.size)))
+
+    planes = split_planes(cfg)
+    slabs = []
+    try:
+        for r in range(world):
+            lo, hi = slab_range(planes, r, world)
+            slabs.append(DeviceSlab(cfg, lo, hi, Ring(r, world, periodic_split)))
+        for s in slabs:
+            codes = _codes(dims, s.box_lo, s.box_n)
+            s.ctx.set_populations(0, codes, f0[[ref_by_code[c] for c in codes.tolist()]])
+        ring = LocalRing(slabs, periodic_split, slabs[0].faces)
+        for _ in range(steps // 2):
+            ring.step_pair()
+        for s in slabs:
+            codes = _codes(dims, s.box_lo, s.box_n)
+            got = s.ctx.get_populations(0, codes)
+            want = ref[[ref_by_code[c] for c in codes.tolist()]]
+            assert np.array_equal(got, want), (s.lo, s.hi, float(np.abs(got - want).max()))
+    finally:
+        for s in slabs:
+            s.close()
+
+
+def test_slab_mid_pair_read_back():
+    """After an even step and its stage-0 swap, the populations read back (odd layout, boundary
+    nodes reading the ghost planes) equal the single context's after one step."""
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, LocalRing, Ring, slab_range, split_planes
+    cfg = _config(3, 0, True, zl.MRT)
+    glo, gn = _box(cfg)
+    gcodes = _codes(3, glo, gn)
+    f0 = _populations(cfg, gcodes)
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, glo, gn)
+        ctx.set_populations(0, gcodes, f0)
+        ctx.step_level(0)
+        ref = ctx.get_populations(0, gcodes)
+    idx = dict(zip(gcodes.tolist(), range(gcodes.size)))
+    slabs = [DeviceSlab(cfg, *slab_range(split_planes(cfg), r, 2), Ring(r, 2, True)) for r in range(2)]
+    try:
+        for s in slabs:
+            codes = _codes(3, s.box_lo, s.box_n)
+            s.ctx.set_populations(0, codes, f0[[idx[c] for c in codes.tolist()]])
+        LocalRing(slabs, True, slabs[0].faces).step()
+        for s in slabs:
+            codes = _codes(3, s.box_lo, s.box_n)
+            assert np.array_equal(s.ctx.get_populations(0, codes), ref[[idx[c] for c in codes.tolist()]])
+    finally:
+        for s in slabs:
+            s.close()
+
+
+def test_halo_errors():
+    import zllbm_b200 as zl
+    cfg = _config(3, 1, True, zl.MRT)
+    lo, n = _box(cfg)
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, lo, n)
+        with pytest.raises(zl.ZlError):
+            ctx.set_level_halo(0, 1 << 4)  # a periodic face
+        with pytest.raises(zl.ZlError):
+            ctx.halo_pack(0, 4, 0, 0)  # not a halo face
+    cfg.bc_kind = cfg.bc_kind[:4] + (zl.BC_NONE, zl.BC_NONE)
+    cfg.domain_max = cfg.domain_max[:2] + (cfg.domain_max[2] - 1,)
+    lo, n = _box(cfg)
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, lo, n)
+        ctx.set_level_halo(0, 3 << 4)
+        with pytest.raises(zl.ZlError):
+            ctx.halo_pack(0, 4, 2, 0)  # bad stage
+        with pytest.raises(zl.ZlError):
+            ctx.set_level_halo(0, 1 << 6)  # no such face
+        assert ctx.halo_bytes(0, 4) == 5 * n[0] * n[1] * 4

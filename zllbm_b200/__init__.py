@@ -109,6 +109,10 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
     dp = ctypes.POINTER(ctypes.c_double)
     sig = {
         "zl_abi_version": ([], ctypes.c_int),
+        "zl_set_level_halo": ([P, ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "zl_halo_bytes": ([P, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int64)], ctypes.c_int),
+        "zl_halo_pack": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
+        "zl_halo_unpack": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p], ctypes.c_int),
         "zl_create": ([ctypes.POINTER(ZlConfig), ctypes.POINTER(P)], ctypes.c_int),
         "zl_destroy": ([P], ctypes.c_int),
         "zl_set_level_nodes": ([P, ctypes.c_int, u64p, i64], ctypes.c_int),
@@ -332,6 +336,21 @@ class Context:
 
     def interpolate_interface(self, fine_level: int):
         self._check(self.lib.zl_interpolate_interface(self.handle, fine_level))
+
+    def set_level_halo(self, level: int, faces: int):
+        """Faces (bit f = face slot f) whose ghost cells hold a neighbouring slab's slots."""
+        self._check(self.lib.zl_set_level_halo(self.handle, level, faces))
+
+    def halo_bytes(self, level: int, face: int) -> int:
+        out = ctypes.c_int64()
+        self._check(self.lib.zl_halo_bytes(self.handle, level, face, ctypes.byref(out)))
+        return out.value
+
+    def halo_pack(self, level: int, face: int, stage: int, buf_ptr: int):
+        self._check(self.lib.zl_halo_pack(self.handle, level, face, stage, ctypes.c_void_p(buf_ptr)))
+
+    def halo_unpack(self, level: int, face: int, stage: int, buf_ptr: int):
+        self._check(self.lib.zl_halo_unpack(self.handle, level, face, stage, ctypes.c_void_p(buf_ptr)))
 
     def set_block(self, level: int, x: int, y: int = 1):
         """Step-kernel block shape; negative x: two nodes per thread (packed FP32 pairs);

@@ -68,13 +68,14 @@ struct Level {
     DeviceBuffer ib_nodes;   // every cell a vertex stencil touches, once
     // the stencils resolved when the vertices are set: per (vertex, stencil node) pair its cell and
     // delta weight; per stencil node the list of its pairs in vertex order (CSR)
-    DeviceBuffer ib_pair_cell, ib_pair_w, ib_csr_pair, ib_csr_start;
+    DeviceBuffer ib_pair_cell, ib_pair_w, ib_csr_start, ib_csr_vertex, ib_csr_share;
     int n_vertices = 0, n_ib_nodes = 0;
     int ib_width = 4;        // immersed-boundary stencil: 4 (reference) or 3 (Roma et al.)
     DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q doubles)
     bool c2f_last_valid = false;
     DeviceBuffer c_node;     // learned closure: c of the last network evaluation per cell
     DeviceBuffer sr_seed;    // stochastic rounding: the two step seeds (StepParams::sr_seed)
+    int halo_faces = 0;      // faces whose ghost cells hold a neighbour's slots (zl_set_level_halo)
 };
 
 }  // namespace
@@ -310,6 +311,7 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     const int dims = ctx->dims, q = ctx->q;
     Level& L = ctx->levels[level];
     L.active = false;
+    L.halo_faces = 0;
     // the vertex set and its node list index the old box
     L.n_vertices = 0;
     L.n_ib_nodes = 0;
@@ -1225,18 +1227,186 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     const unsigned nblocks = (unsigned)((L.n_ib_nodes + 127) / 128);
     const int* pc = (const int*)L.ib_pair_cell.ptr;
     const double* pw = (const double*)L.ib_pair_w.ptr;
-    const int *cs = (const int*)L.ib_csr_start.ptr, *cp = (const int*)L.ib_csr_pair.ptr;
+    const int *cs = (const int*)L.ib_csr_start.ptr, *cv = (const int*)L.ib_csr_vertex.ptr;
+    const double* csh = (const double*)L.ib_csr_share.ptr;
     if (ctx->dims == 2) {
         ib_force_kernel<2><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<2><<<nblocks, 128, 0, ctx->stream>>>(L.params, v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs,
-                                                              cp, pw, (double*)L.force.ptr);
+        ib_spread_kernel<2><<<nblocks, 128, 0, ctx->stream>>>(v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs, cv, csh,
+                                                              (double*)L.force.ptr);
     } else {
         ib_force_kernel<3><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<3><<<nblocks, 128, 0, ctx->stream>>>(L.params, v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs,
-                                                              cp, pw, (double*)L.force.ptr);
+        ib_spread_kernel<3><<<nblocks, 128, 0, ctx->stream>>>(v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs, cv, csh,
+                                                              (double*)L.force.ptr);
     }
     ZL_CUDA(ctx, cudaGetLastError());
     return ZL_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------- halo faces (slab sharding)
+namespace {
+
+// Cells of the plane of `face` at box coordinate `layer` on the face's axis: every cell of the
+// two other axes' allocated extents, the lower one fastest.
+struct FacePlane {
+    int axis, b, c;       // the face's axis and the two others (b fastest)
+    int nb, nc;           // allocated extents of b and c
+    int layer;            // box coordinate on `axis`
+    long long stride[3];  // cell stride per axis
+};
+
+FacePlane face_plane(const LevelGeom& geo, int dims, int face, bool ghost) {
+    FacePlane fp{};
+    fp.axis = face >> 1;
+    const bool hi = face & 1;
+    int others[2], k = 0;
+    for (int a = 0; a < 3; ++a)
+        if (a != fp.axis) others[k++] = a;
+    fp.b = others[0];
+    fp.c = others[1];
+    fp.nb = geo.a[fp.b];
+    fp.nc = dims == 3 || fp.c < 2 ? geo.a[fp.c] : 1;
+    const int g = geo.g[fp.axis], n = geo.n[fp.axis];
+    fp.layer = ghost ? (hi ? g + n : g - 1) : (hi ? g + n - 1 : g);
+    fp.stride[0] = 1;
+    fp.stride[1] = geo.a[0];
+    fp.stride[2] = (long long)geo.a[0] * geo.a[1];
+    return fp;
+}
+
+__global__ void mark_plane_present_kernel(uint32_t* info, FacePlane fp) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)fp.nb * fp.nc) return;
+    const long long cell = fp.layer * fp.stride[fp.axis] + (t % fp.nb) * fp.stride[fp.b] + (t / fp.nb) * fp.stride[fp.c];
+    info[cell] = kInfoPresent;
+}
+
+// Clear the missing-upstream bits (1 .. q - 1) of every cell before they are derived again.
+__global__ void clear_missing_kernel(uint32_t* info, long long cells, int q) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < cells) info[t] &= ~((1u << q) - 2u);
+}
+
+// Copy the planes `planes[0 .. np)` of the face plane between the population array and a packed
+// buffer [np][nc][nb] of raw storage elements (E bytes each).
+template <class E>
+__global__ void halo_copy_kernel(E* f, long long stride, FacePlane fp, int np, int4 planes_lo, int4 planes_hi,
+                                 E* buf, int pack) {
+    const long long per = (long long)fp.nb * fp.nc;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= per * np) return;
+    const int k = (int)(t / per);
+    const long long r = t % per;
+    const int pl[8] = {planes_lo.x, planes_lo.y, planes_lo.z, planes_lo.w, planes_hi.x, planes_hi.y, planes_hi.z,
+                       planes_hi.w};
+    const long long cell = fp.layer * fp.stride[fp.axis] + (r % fp.nb) * fp.stride[fp.b] + (r / fp.nb) * fp.stride[fp.c];
+    E* slot = f + pl[k] * stride + cell;
+    if (pack) buf[t] = *slot;
+    else *slot = buf[t];
+}
+
+}  // namespace
+
+extern "C" {
+
+// Population planes that cross `face` inward (toward the box) or outward.
+static int face_planes(int dims, int face, bool inward, int* planes) {
+    const int axis = face >> 1;
+    const int sign = (face & 1) ? (inward ? -1 : 1) : (inward ? 1 : -1);
+    const int q = dims == 2 ? 9 : 19;
+    int n = 0;
+    for (int k = 0; k < q; ++k)
+        if (lattice_c(dims, k, axis) == sign) planes[n++] = k;
+    return n;
+}
+
+int zl_set_level_halo(zl_ctx* ctx, int level, int faces) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    if (faces & ~((1 << (2 * ctx->dims)) - 1)) return fail(ctx, ZL_EINVAL, "halo faces 0x%x", faces);
+    for (int f = 0; f < 2 * ctx->dims; ++f) {
+        if (!((faces >> f) & 1)) continue;
+        if (ctx->cfg.bc_kind[f] != ZL_BC_NONE || !L.geo.g[f >> 1] || !((L.geo.face_on_box >> f) & 1))
+            return fail(ctx, ZL_EINVAL, "level %d: a halo face needs ZL_BC_NONE and the level box on the domain face", level);
+    }
+    if (ctx->cfg.max_level > 0 || ctx->cfg.forcing || ctx->cfg.les == ZL_LES_LEARNED)
+        return fail(ctx, ZL_ESTATE, "halo faces are for single-level contexts without forcing");
+    ZL_CUDA(ctx, cudaSetDevice(ctx->cfg.device));
+    const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
+    if (!L.info.ptr) {
+        // a full box gets its per-cell info (presence, missing-upstream and face bits)
+        if ((rc = alloc(ctx, L.info, (size_t)cells * sizeof(uint32_t)))) return rc;
+        ZL_CUDA(ctx, cudaMemsetAsync(L.info.ptr, 0, (size_t)cells * sizeof(uint32_t), ctx->stream));
+        ZL_CUDA(ctx, launch_mark_box(L.geo, (uint32_t*)L.info.ptr, ctx->stream));
+        L.geo.info = (const uint32_t*)L.info.ptr;
+    }
+    // ghost cells of a halo face hold the neighbour's slots: present for the neighbour lookups of
+    // the nodes next to them, never stepped themselves
+    for (int f = 0; f < 2 * ctx->dims; ++f) {
+        if (!((faces >> f) & 1)) continue;
+        const FacePlane fp = face_plane(L.geo, ctx->dims, f, true);
+        const long long n = (long long)fp.nb * fp.nc;
+        mark_plane_present_kernel<<<(unsigned)((n + 255) / 256), 256, 0, ctx->stream>>>((uint32_t*)L.info.ptr, fp);
+    }
+    clear_missing_kernel<<<(unsigned)((cells + 255) / 256), 256, 0, ctx->stream>>>((uint32_t*)L.info.ptr, cells, ctx->q);
+    launch_node_info(ctx->dims, L.geo, (uint32_t*)L.info.ptr, ctx->stream, L.halo_faces | faces);
+    ZL_CUDA(ctx, cudaGetLastError());
+    ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    L.halo_faces |= faces;
+    ++ctx->generation;
+    return ZL_OK;
+}
+
+int zl_halo_bytes(zl_ctx* ctx, int level, int face, int64_t* bytes) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    if (face < 0 || face >= 2 * ctx->dims || !bytes) return fail(ctx, ZL_EINVAL, "bad halo face");
+    const Level& L = ctx->levels[level];
+    const FacePlane fp = face_plane(L.geo, ctx->dims, face, true);
+    int planes[8];
+    const int np = face_planes(ctx->dims, face, true, planes);
+    *bytes = (int64_t)np * fp.nb * fp.nc * ctx->ops->elem_bytes;
+    return ZL_OK;
+}
+
+static int halo_copy(zl_ctx* ctx, int level, int face, int stage, void* buf, bool pack) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    if (face < 0 || face >= 2 * ctx->dims || !((L.halo_faces >> face) & 1) || (stage != 0 && stage != 1) || !buf)
+        return fail(ctx, ZL_EINVAL, "halo copy: face %d is not a halo face of level %d, or bad stage / buffer", face, level);
+    // stage 0 (after an even step): the boundary plane's inward planes travel to the neighbour's
+    // ghost plane (its outward planes); stage 1 (after an odd step): the ghost plane's outward
+    // planes travel back to the neighbour's boundary plane (its inward planes)
+    const bool ghost = pack ? stage == 1 : stage == 0;
+    const bool inward = pack ? stage == 0 : stage == 1;
+    const FacePlane fp = face_plane(L.geo, ctx->dims, face, ghost);
+    int planes[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int np = face_planes(ctx->dims, face, inward, planes);
+    const long long n = (long long)np * fp.nb * fp.nc;
+    const int4 lo = make_int4(planes[0], planes[1], planes[2], planes[3]);
+    const int4 hi = make_int4(planes[4], planes[5], planes[6], planes[7]);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    switch (ctx->ops->elem_bytes) {
+        case 8: halo_copy_kernel<uint64_t><<<blocks, 256, 0, ctx->stream>>>((uint64_t*)L.f.ptr, L.geo.stride, fp, np, lo,
+                                                                            hi, (uint64_t*)buf, pack); break;
+        case 4: halo_copy_kernel<uint32_t><<<blocks, 256, 0, ctx->stream>>>((uint32_t*)L.f.ptr, L.geo.stride, fp, np, lo,
+                                                                            hi, (uint32_t*)buf, pack); break;
+        default: halo_copy_kernel<uint16_t><<<blocks, 256, 0, ctx->stream>>>((uint16_t*)L.f.ptr, L.geo.stride, fp, np, lo,
+                                                                             hi, (uint16_t*)buf, pack); break;
+    }
+    ZL_CUDA(ctx, cudaGetLastError());
+    return ZL_OK;
+}
+
+int zl_halo_pack(zl_ctx* ctx, int level, int face, int stage, void* buf_device) {
+    return halo_copy(ctx, level, face, stage, buf_device, true);
+}
+
+int zl_halo_unpack(zl_ctx* ctx, int level, int face, int stage, const void* buf_device) {
+    return halo_copy(ctx, level, face, stage, const_cast<void*>(buf_device), false);
 }
 
 int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordinates, const double* velocity,
@@ -1324,11 +1494,13 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         const long long pairs = (long long)n * K;
         if (pairs >= 0x7fffffffll) return fail(ctx, ZL_ETOOLARGE, "level %d: too many vertex-node pairs", level);
         {
-            DeviceBuffer node_of_cell, key, key_sorted, id, stmp;
+            DeviceBuffer node_of_cell, key, key_sorted, id, csr_pair, stmp;
             if ((rc = alloc(ctx, node_of_cell, (size_t)cells * 4)) || (rc = alloc(ctx, key, (size_t)pairs * 4)) ||
                 (rc = alloc(ctx, key_sorted, (size_t)pairs * 4)) || (rc = alloc(ctx, id, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, csr_pair, (size_t)pairs * 4)) ||
                 (rc = alloc(ctx, L.ib_pair_cell, (size_t)pairs * 4)) || (rc = alloc(ctx, L.ib_pair_w, (size_t)pairs * 8)) ||
-                (rc = alloc(ctx, L.ib_csr_pair, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, L.ib_csr_vertex, (size_t)pairs * 4)) ||
+                (rc = alloc(ctx, L.ib_csr_share, (size_t)pairs * 8)) ||
                 (rc = alloc(ctx, L.ib_csr_start, (size_t)(nodes + 1) * 4)))
                 return rc;
             ib_index_nodes_kernel<<<(nodes + 127) / 128, 128, 0, ctx->stream>>>((const int*)L.ib_nodes.ptr, nodes,
@@ -1347,12 +1519,20 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
             while ((1ll << bits) < (long long)nodes) ++bits;
             size_t sbytes = 0;
             ZL_CUDA(ctx, sort_pairs_by_key((const int*)key.ptr, (int*)key_sorted.ptr, (const int*)id.ptr,
-                                           (int*)L.ib_csr_pair.ptr, (int)pairs, bits, nullptr, &sbytes, ctx->stream));
+                                           (int*)csr_pair.ptr, (int)pairs, bits, nullptr, &sbytes, ctx->stream));
             if ((rc = alloc(ctx, stmp, std::max<size_t>(sbytes, 1)))) return rc;
             ZL_CUDA(ctx, sort_pairs_by_key((const int*)key.ptr, (int*)key_sorted.ptr, (const int*)id.ptr,
-                                           (int*)L.ib_csr_pair.ptr, (int)pairs, bits, stmp.ptr, &sbytes, ctx->stream));
+                                           (int*)csr_pair.ptr, (int)pairs, bits, stmp.ptr, &sbytes, ctx->stream));
             ib_csr_start_kernel<<<(unsigned)((pairs + 1 + 127) / 128), 128, 0, ctx->stream>>>(
                 (const int*)key_sorted.ptr, pairs, (int*)L.ib_csr_start.ptr, nodes);
+            if (ctx->dims == 2)
+                ib_csr_fill_kernel<2><<<pblocks, 128, 0, ctx->stream>>>(v, L.params.dt, (const int*)csr_pair.ptr,
+                                                                       (const double*)L.ib_pair_w.ptr, pairs,
+                                                                       (int*)L.ib_csr_vertex.ptr, (double*)L.ib_csr_share.ptr);
+            else
+                ib_csr_fill_kernel<3><<<pblocks, 128, 0, ctx->stream>>>(v, L.params.dt, (const int*)csr_pair.ptr,
+                                                                       (const double*)L.ib_pair_w.ptr, pairs,
+                                                                       (int*)L.ib_csr_vertex.ptr, (double*)L.ib_csr_share.ptr);
             ZL_CUDA(ctx, cudaGetLastError());
             ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
         }

@@ -259,48 +259,56 @@ __global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(IbVertices v, c
     }
 }
 
-// Launch 3: a thread per stencil node sums F delta area / (dt dx^(d-1)) over its pairs, in vertex
-// order, and writes the node force (launch 1 zeroed it; no other pass adds to it).
+// Launch 3: a thread per stencil node sums F_i s_p over its pairs p (vertex i), in vertex order,
+// and writes the node force (launch 1 zeroed it; no other pass adds to it).  s_p = delta_p area_i /
+// (dt dx^(d-1)) and the vertex index come from the CSR arrays, laid out in node order.
 template <int D>
-__global__ void ib_spread_kernel(StepParams p, IbVertices v, const int* __restrict__ nodes, int n_nodes,
-                                 const int* __restrict__ csr_start, const int* __restrict__ csr_pair,
-                                 const double* __restrict__ pair_w, double* __restrict__ node_force) {
+__global__ void ib_spread_kernel(IbVertices v, const int* __restrict__ nodes, int n_nodes,
+                                 const int* __restrict__ csr_start, const int* __restrict__ csr_vertex,
+                                 const double* __restrict__ csr_share, double* __restrict__ node_force) {
     const int j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n_nodes) return;
-    const FastDiv K = FastDiv::make(D == 3 ? v.width * v.width * v.width : v.width * v.width);
     double F[3] = {0., 0., 0.};
-    auto add = [&](double w, int i, const double* f) {
-        const double area = D == 3 ? v.area[i] / p.dt / v.dx / v.dx : v.area[i] / p.dt / v.dx;
-        const double dt = w * area;
-        for (int a = 0; a < D; ++a) F[a] += f[a] * dt;
-    };
     const int s1 = csr_start[j + 1];
     int s = csr_start[j];
     // four pairs per round: their loads are issued before the sums (kept in pair order)
     for (; s + 4 <= s1; s += 4) {
-        int i4[4];
-        double w4[4], f4[4][3];
+        double sh[4], f4[4][3];
 #pragma unroll
         for (int e = 0; e < 4; ++e) {
-            const int pr = __ldg(csr_pair + s + e);
-            i4[e] = (int)K.div((uint32_t)pr);
-            w4[e] = __ldg(pair_w + pr);
+            const int i = __ldg(csr_vertex + s + e);
+            sh[e] = __ldg(csr_share + s + e);
+#pragma unroll
+            for (int a = 0; a < D; ++a) f4[e][a] = v.force[i * 3 + a];
         }
 #pragma unroll
         for (int e = 0; e < 4; ++e)
 #pragma unroll
-            for (int a = 0; a < D; ++a) f4[e][a] = v.force[i4[e] * 3 + a];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) add(w4[e], i4[e], f4[e]);
+            for (int a = 0; a < D; ++a) F[a] += f4[e][a] * sh[e];
     }
     for (; s < s1; ++s) {
-        const int pr = __ldg(csr_pair + s);
-        const int i = (int)K.div((uint32_t)pr);
-        const double f1[3] = {v.force[i * 3], v.force[i * 3 + 1], D == 3 ? v.force[i * 3 + 2] : 0.};
-        add(__ldg(pair_w + pr), i, f1);
+        const int i = __ldg(csr_vertex + s);
+        const double sh = __ldg(csr_share + s);
+        for (int a = 0; a < D; ++a) F[a] += v.force[i * 3 + a] * sh;
     }
     const long long cell = nodes[j];
     for (int a = 0; a < D; ++a) node_force[cell * 3 + a] = F[a];
+}
+
+// The spread CSR in node order: for sorted position t the vertex of pair csr_pair[t] and its share
+// delta area / (dt dx^(d-1)), with the division order of the direct formula.  Runs with the vertices.
+template <int D>
+__global__ void ib_csr_fill_kernel(IbVertices v, double dt, const int* __restrict__ csr_pair,
+                                   const double* __restrict__ pair_w, long long pairs, int* __restrict__ csr_vertex,
+                                   double* __restrict__ csr_share) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= pairs) return;
+    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+    const int pr = csr_pair[t];
+    const int i = pr / K;
+    const double area = D == 3 ? v.area[i] / dt / v.dx / v.dx : v.area[i] / dt / v.dx;
+    csr_vertex[t] = i;
+    csr_share[t] = pair_w[pr] * area;
 }
 
 // CSR row starts of the sorted pair keys (every stencil node owns at least one pair).

@@ -48,7 +48,9 @@ __global__ void count_present_kernel(const uint32_t* __restrict__ info, long lon
 
 // Missing-upstream bits and boundary-face bits of every present node.
 template <class L>
-__global__ void node_info_kernel(LevelGeom geo, uint32_t* __restrict__ info) {
+// halo: faces whose ghost plane holds a neighbouring slab's slots (upstream nodes beyond such a
+// face are missing only if their ghost cell is absent)
+__global__ void node_info_kernel(LevelGeom geo, uint32_t* __restrict__ info, int halo) {
     using Tb = Tables<L>;
     Coord c;
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
@@ -68,8 +70,11 @@ __global__ void node_info_kernel(LevelGeom geo, uint32_t* __restrict__ info) {
     for (int q = 1; q < L::kQ; ++q) {
         const int s[3] = {c.x[0] - Tb::cx(q), c.x[1] - Tb::cy(q), c.x[2] - Tb::cz(q)};
         bool missing = false;
-        for (int a = 0; a < L::kDims; ++a)
-            if (!geo.periodic[a] && (s[a] < 0 || s[a] >= geo.n[a])) missing = true;
+        for (int a = 0; a < L::kDims; ++a) {
+            if (geo.periodic[a]) continue;
+            if ((s[a] < 0 && !((halo >> (2 * a)) & 1)) || (s[a] >= geo.n[a] && !((halo >> (2 * a + 1)) & 1)))
+                missing = true;
+        }
         if (!missing) missing = !(info[cell_of(s)] & kInfoPresent);
         if (missing) v |= 1u << q;
     }
@@ -77,13 +82,13 @@ __global__ void node_info_kernel(LevelGeom geo, uint32_t* __restrict__ info) {
     info[self] = v;
 }
 
-void launch_node_info(int dims, const LevelGeom& geo, uint32_t* info, cudaStream_t s) {
+void launch_node_info(int dims, const LevelGeom& geo, uint32_t* info, cudaStream_t s, int halo_faces) {
     dim3 g, b;
     step_shape(geo, dims, g, b);
     if (dims == 2)
-        node_info_kernel<D2Q9><<<g, b, 0, s>>>(geo, info);
+        node_info_kernel<D2Q9><<<g, b, 0, s>>>(geo, info, halo_faces);
     else
-        node_info_kernel<D3Q19><<<g, b, 0, s>>>(geo, info);
+        node_info_kernel<D3Q19><<<g, b, 0, s>>>(geo, info, halo_faces);
 }
 
 template <class S>

@@ -13,7 +13,7 @@ cudaError_t launch_mark_present(const uint64_t* codes, long long n, const LevelM
                                 uint32_t* info, int* bad, cudaStream_t s);
 cudaError_t launch_count_present(const uint32_t* info, long long cells, unsigned long long* count, cudaStream_t s);
 cudaError_t launch_mark_box(const LevelGeom& geo, uint32_t* info, cudaStream_t s);
-void launch_node_info(int dims, const LevelGeom& geo, uint32_t* info, cudaStream_t s);
+void launch_node_info(int dims, const LevelGeom& geo, uint32_t* info, cudaStream_t s, int halo_faces = 0);
 cudaError_t launch_fill(int storage, void* f, long long stride, int q, const StepParams& p, const double* value,
                         cudaStream_t s);
 cudaError_t launch_morton_neighbors(const uint64_t* codes, long long n, int dims, uint64_t* out, cudaStream_t s);
