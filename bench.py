@@ -8,8 +8,10 @@ upload of the initial populations from pinned memory, K steps, read-back of dens
 velocity, all inside the timed region.  The lattice (256^3 nodes, 2.55 GB of FP32
 populations) is far larger than L2, so no flush is needed between steps.
 
-Multi-GPU runs are independent replicas (one lattice per rank, no data-path
-collective); ranks only meet at the timing barriers.
+Multi-GPU runs shard one lattice of 256 x 256 x 256N nodes into N slabs of 256^3 along z, one per
+rank (weak scaling), with the two-stage halo exchange of the AA pattern over NCCL point-to-point
+after every step (zllbm_b200.shard); ``--shard`` runs the same path at N = 1 as a one-rank periodic
+ring, ``--replicas`` gives every rank its own lattice instead (no data-path collective).
 """
 from __future__ import annotations
 
@@ -39,13 +41,14 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 # ---------------------------------------------------------------- helpers
-def tgv_nodes(cells: int):
-    """Morton codes of the reference's stored nodes (indices 1..cells+1) and TGV feq populations."""
+def tgv_nodes(cells: int, lo=(1, 1, 1), hi=None):
+    """Morton codes of the reference's stored nodes (indices lo..hi per axis, by default 1..cells+1)
+    and TGV feq populations (period `cells` on every axis), x fastest."""
     import zllbm_b200 as zl
-    n = cells + 1
-    codes = zl.box_codes(3, (1, 1, 1), (n, n, n))
-    ax = 2.0 * np.pi * (np.arange(n) % cells) / cells
-    z, y, x = np.meshgrid(ax, ax, ax, indexing="ij")
+    hi = hi or (cells + 1,) * 3
+    codes = zl.box_codes(3, lo, hi)
+    ax = [2.0 * np.pi * ((np.arange(lo[a], hi[a] + 1) - 1) % cells) / cells for a in range(3)]
+    z, y, x = np.meshgrid(ax[2], ax[1], ax[0], indexing="ij")
     x, y, z = x.ravel(), y.ravel(), z.ravel()
     ux = U0 * np.sin(x) * np.cos(y) * np.cos(z)
     uy = -U0 * np.cos(x) * np.sin(y) * np.cos(z)
@@ -177,6 +180,16 @@ def max_over_ranks(dist, value: float) -> float:
     device = "cuda" if dist.get_backend() == "nccl" else "cpu"
     t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(dist, value: float) -> float:
+    if dist is None:
+        return value
+    import torch
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -343,6 +356,8 @@ def run_ours(args):
     import zllbm_b200 as zl
     rank, world, local, dist = dist_init(args.gpus)
     torch.cuda.set_device(local)
+    if args.shard or (world > 1 and not args.replicas):
+        return run_sharded(args, rank, world, local, dist)
     storage = zl.STORAGE_NAMES[args.storage]
     elem = STORAGE_BYTES[args.storage]
     codes, f0 = tgv_nodes(CELLS)
@@ -477,6 +492,116 @@ def run_ours(args):
     return 0
 
 
+def run_sharded(args, rank: int, world: int, local: int, dist):
+    """One lattice of CELLS x CELLS x (CELLS world) nodes, periodic, split into `world` slabs of
+    CELLS planes along z (zllbm_b200.shard): each rank steps its slab and swaps halo planes with its
+    two neighbours after every step (NCCL point-to-point; at world 1 the ring routes the buffers to
+    itself).  The Taylor-Green field repeats with period CELLS along z, so every slab starts as the
+    single-GPU workload."""
+    import ctypes
+
+    import torch
+
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, LocalRing, Ring, SlabSchedule, torch_exchange
+    storage = zl.STORAGE_NAMES[args.storage]
+    elem = STORAGE_BYTES[args.storage]
+    gcfg = solver_config(storage, local)
+    gcfg.domain_max = (CELLS + 1, CELLS + 1, CELLS * world + 1)
+    ring = Ring(rank, world, True)
+    lo, hi = rank * CELLS, (rank + 1) * CELLS
+    slab = DeviceSlab(gcfg, lo, hi, ring)
+    codes, f0 = tgv_nodes(CELLS, (1, 1, 1 + lo), (CELLS + 1, CELLS + 1, hi))
+    if not np.array_equal(codes, slab.codes):
+        raise RuntimeError("slab node order")
+    nodes = CELLS ** 3
+    alg_bytes = nodes * 2 * 19 * elem
+    ctx = slab.ctx
+    ctx.set_populations(0, None, f0)
+    block = ctx.autotune(0) if args.tune else None
+    if args.tune:
+        ctx.set_populations(0, None, f0)
+    sched = LocalRing([slab], True, slab.faces) if world == 1 else SlabSchedule(slab, ring, slab.faces,
+                                                                                torch_exchange(dist))
+    barrier(dist)  # every rank's communicator is up before the first point-to-point exchange
+    for _ in range(args.warmup):
+        sched.step()
+    mass_before = sum_over_ranks(dist, ctx.conservation(0)[0])
+    stream = torch.cuda.current_stream()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier(dist)
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        start.record(stream)
+        for _ in range(args.steps):
+            sched.step()
+        end.record(stream)
+        end.synchronize()
+    torch.cuda.synchronize()
+    barrier(dist)
+    ms = max_over_ranks(dist, start.elapsed_time(end))
+    mass = sum_over_ranks(dist, ctx.conservation(0)[0])
+    ms_per_step = ms / args.steps
+    value = whole_job_mlups(world, nodes, args.steps, ms / 1e3)
+    peak, peak_kind = measured_peak()
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    halo_bytes = sum(slab.nbytes.values())
+
+    e2e = None
+    if not args.no_e2e:
+        f_h = torch.from_numpy(f0).pin_memory()
+        rho_h = torch.empty(codes.size, dtype=torch.float64).pin_memory()
+        u_h = torch.empty((codes.size, 3), dtype=torch.float64).pin_memory()
+        dp = ctypes.POINTER(ctypes.c_double)
+        lib = ctx.lib
+        barrier(dist)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx._check(lib.zl_set_populations(ctx.handle, 0, None, ctypes.cast(f_h.data_ptr(), dp), codes.size))
+        for _ in range(args.steps):
+            sched.step()
+        ctx._check(lib.zl_get_macros(ctx.handle, 0, None, ctypes.cast(rho_h.data_ptr(), dp),
+                                     ctypes.cast(u_h.data_ptr(), dp), codes.size))
+        torch.cuda.synchronize()
+        t_e2e = max_over_ranks(dist, time.perf_counter() - t0)
+        e2e = {"value": whole_job_mlups(world, nodes, args.steps, t_e2e), "unit": "MLUPS",
+               "h2d_bytes_per_step": f0.nbytes / args.steps,
+               "d2h_bytes_per_step": (rho_h.numel() + u_h.numel()) * 8 / args.steps, "seconds": t_e2e,
+               "includes": "per rank: H2D of its slab's initial populations (pinned), K steps with their halo "
+                           "exchanges, D2H of rho and u"}
+    slab.close()
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.storage, "data": "synthetic",
+            "config": {"workload": f"D3Q19 {COLLISION.upper()} Taylor-Green vortex, periodic {CELLS} x {CELLS} x "
+                                   f"{CELLS * world} (z period {CELLS}), u0={U0}, tau={TAU}, "
+                                   f"{args.storage} population storage",
+                       "block": block, "cuda_graph": False, "nodes_per_gpu": nodes, "storage": args.storage,
+                       "collision": COLLISION.upper(),
+                       "l2": f"inputs larger than L2 ({alg_bytes / 2 / 1e9:.2f} GB of populations per GPU)",
+                       "parallelism": f"slab sharding along z over {world} GPU(s), halo exchange after every step "
+                                      + ("(NCCL point-to-point)" if world > 1 else "(one-rank ring, device copies)"),
+                       "halo_bytes_per_exchange": halo_bytes},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": committed_traffic(args.storage), "peak_kind": peak_kind,
+                         "algorithmic_bytes_per_launch": alg_bytes, "kernel": kernel_name(block, args.storage),
+                         "note": "step time includes the halo packs, exchanges and unpacks"},
+            "cpu_baseline": None,
+            "e2e": e2e,
+            # per step: the step kernel, a pack per face and an unpack per face
+            "gpu_launches": args.steps * 5,
+            "clocks": clocks.summary(),
+            "mass_after": mass,
+            "mass_drift": (mass - mass_before) / mass_before,
+        }
+        print(json.dumps(out), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -492,6 +617,8 @@ def main():
     ap.add_argument("--tune", type=int, default=1, help="autotune the step kernel's block shape")
     ap.add_argument("--graph", type=int, default=1, help="replay steps as a captured CUDA graph")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shard", action="store_true", help="slab-sharded path at any N (N = 1: one-rank ring)")
+    ap.add_argument("--replicas", action="store_true", help="N > 1: independent lattices instead of slabs")
     ap.add_argument("--multilevel", type=int, default=1,
                     help="multi-level cube-flow and cylinder-flow block (reference-built grids)")
     args = ap.parse_args()

@@ -139,3 +139,66 @@ def test_halo_errors():
         with pytest.raises(zl.ZlError):
             ctx.set_level_halo(0, 1 << 6)  # no such face
         assert ctx.halo_bytes(0, 4) == 5 * n[0] * n[1] * 4
+
+
+@pytest.mark.parametrize("world", [2, 3])
+@pytest.mark.parametrize("kernel,storage", [("pair", 1), ("pair", 2), ("row", 2), ("row", 3)])
+def test_ring_slabs_take_full_box_kernels(kernel, storage, world):
+    """Slabs of a periodic box (x and y periodic, both z faces connected) run the two-nodes-per-
+    thread and one-warp-per-row kernels with z addressed through the ghost planes.  With round-to-
+    nearest storage the row kernel equals the single context running it bit for bit.  The pair
+    kernel hands the rows whose y or z neighbours wrap to the one-node update, which rounds
+    differently in FP32: the single context does so for its z = 0 and z = n - 1 rows, the slabs
+    (whose z neighbours never wrap) do not, so that case agrees to FP32 rounding only."""
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, LocalRing, Ring, slab_range, split_planes
+    n = (128, 8, 12)
+    cfg = zl.SolverConfig(lattice=zl.D3Q19, collision=zl.MRT, storage=storage, viscosity=0.02, rho0=1.0,
+                          bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(1, 1, 1), domain_max=tuple(1 + v for v in n),
+                          storage_rounding=zl.ROUND_NEAREST)
+    block = (-64, 1) if kernel == "pair" else (zl.BLOCK_ROW, 4)
+    glo, gn = _box(cfg)
+    gcodes = _codes(3, glo, gn)
+    f0 = _populations(cfg, gcodes)
+    steps = 6
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, glo, gn)
+        ctx.set_populations(0, gcodes, f0)
+        ctx.set_block(0, *block)
+        ctx.advance(steps)
+        ref = ctx.get_populations(0, gcodes)
+    idx = dict(zip(gcodes.tolist(), range(gcodes.size)))
+    slabs = []
+    try:
+        for r in range(world):
+            slabs.append(DeviceSlab(cfg, *slab_range(split_planes(cfg), r, world), Ring(r, world, True)))
+        for s in slabs:
+            codes = _codes(3, s.box_lo, s.box_n)
+            s.ctx.set_populations(0, codes, f0[[idx[c] for c in codes.tolist()]])
+            s.ctx.set_block(0, *block)  # refused unless the slab qualifies for the kernel
+        ring = LocalRing(slabs, True, slabs[0].faces)
+        for _ in range(steps // 2):
+            ring.step_pair()
+        for s in slabs:
+            codes = _codes(3, s.box_lo, s.box_n)
+            got, want = s.ctx.get_populations(0, codes), ref[[idx[c] for c in codes.tolist()]]
+            if kernel == "row":
+                assert np.array_equal(got, want), (s.lo, float(np.abs(got - want).max()))
+            else:
+                np.testing.assert_allclose(got, want, rtol=0, atol=2e-6)
+    finally:
+        for s in slabs:
+            s.close()
+
+
+def test_open_chain_slab_refuses_full_box_kernels():
+    """An end slab of a wall-bounded axis has a missing-upstream face: only the general kernel runs it."""
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, Ring, slab_range, split_planes
+    cfg = _config(3, 1, False, zl.MRT)
+    s = DeviceSlab(cfg, *slab_range(split_planes(cfg), 0, 2), Ring(0, 2, False))
+    try:
+        with pytest.raises(zl.ZlError):
+            s.ctx.set_block(0, -64, 1)
+    finally:
+        s.close()

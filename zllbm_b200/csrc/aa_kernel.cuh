@@ -48,6 +48,10 @@ struct LevelGeom {
     int face_on_box;   // bit f: box edge f lies on domain face f (non-periodic faces only)
     int block[2];      // thread-block shape of the step kernel (x, y); {0, 0}: default
     const uint32_t* info;  // per-cell info (masked levels), nullptr for full boxes
+    // 1: a full D3Q19 box, periodic along x and y, whose two z faces are halo faces (a slab of a
+    // sharded lattice): every upstream node is present, the z ones in the ghost planes, so the
+    // kernels of full periodic boxes apply with z addressed through the ghost frame
+    int ring;
 };
 
 struct StepParams {

@@ -933,7 +933,7 @@ int zl_set_block(zl_ctx* ctx, int level, int x, int y) {
     }
     const int ax = std::abs(x);
     if (ax < 32 || ax % 32 || y < 1 || ax * y > 256) return fail(ctx, ZL_EINVAL, "block shape %d x %d", x, y);
-    if (x < 0 && !pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes))
+    if (x < 0 && !pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes, L.geo))
         return fail(ctx, ZL_EINVAL, "two nodes per thread needs a full periodic D3Q19 box in reduced storage");
     L.geo.block[0] = x;
     L.geo.block[1] = y;
@@ -955,7 +955,7 @@ int zl_autotune(zl_ctx* ctx, int level, int trials, int32_t* chosen) {
     const int shapes[][2] = {{256, 1}, {128, 2}, {128, 1}, {64, 4}, {64, 2}, {32, 8}, {32, 4},
                              {-128, 1}, {-64, 2}, {-256, 1}, {-64, 1},
                              {ZL_BLOCK_ROW, 4}, {ZL_BLOCK_ROW, 2}, {ZL_BLOCK_ROW, 1}};
-    const bool pairs = pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes);
+    const bool pairs = pair_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes, L.geo);
     const bool rows = row_eligible(ctx->dims, L.bnd, L.geo.info != nullptr, L.params, ctx->ops->elem_bytes, L.geo);
     cudaEvent_t t0, t1;
     ZL_CUDA(ctx, cudaEventCreate(&t0));
@@ -1355,6 +1355,10 @@ int zl_set_level_halo(zl_ctx* ctx, int level, int faces) {
     ZL_CUDA(ctx, cudaGetLastError());
     ZL_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     L.halo_faces |= faces;
+    // a full box periodic along x and y with both z faces connected: the full-box kernels apply
+    const long long box_nodes = (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2];
+    L.geo.ring = ctx->dims == 3 && L.geo.periodic[0] && L.geo.periodic[1] && (L.halo_faces & 48) == 48 &&
+                 L.nodes == box_nodes;
     ++ctx->generation;
     return ZL_OK;
 }

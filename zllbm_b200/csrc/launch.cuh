@@ -62,17 +62,18 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
     grid = dim3((nx + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? geo.n[2] : 1);
 }
 
-// The two-nodes-per-thread kernel applies to full periodic D3Q19 boxes in deviation storage
-// without forcing or LES.
-inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, int elem_bytes) {
-    return dims == 3 && !bnd && !masked && !p.forced && !p.les && elem_bytes < 8;
+// The two-nodes-per-thread kernel applies to full periodic D3Q19 boxes (or slabs of one, geo.ring)
+// in deviation storage without forcing or LES.
+inline bool pair_eligible(int dims, bool bnd, bool masked, const StepParams& p, int elem_bytes,
+                          const LevelGeom& geo) {
+    return dims == 3 && (geo.ring || (!bnd && !masked)) && !p.forced && !p.les && elem_bytes < 8;
 }
 
 // The one-warp-per-row kernel (row_kernel.cuh): full periodic D3Q19 boxes in 16-bit storage
 // with rows of 128 or 256 nodes, no forcing or LES.
 inline bool row_eligible(int dims, bool bnd, bool masked, const StepParams& p, int elem_bytes,
                          const LevelGeom& geo) {
-    return pair_eligible(dims, bnd, masked, p, elem_bytes) && elem_bytes == 2 && row_kernel_width(geo) != 0;
+    return pair_eligible(dims, bnd, masked, p, elem_bytes, geo) && elem_bytes == 2 && row_kernel_width(geo) != 0;
 }
 
 // Fused step launchers of one (storage, lattice, collision, parity) and batched step launchers

@@ -149,8 +149,9 @@ __device__ __forceinline__ void fused_pair(const F2* d, F2* out, const StepParam
     }
 }
 
-// Nodes x0 and x0 + 1 of a row of a full periodic box with an even row length.  Rows whose y or
-// z neighbours wrap take the scalar node update twice.
+// Nodes x0 and x0 + 1 of a row of a full periodic box (or a slab of one, geo.ring: z neighbours
+// in the ghost planes) with an even row length.  Rows whose y or z neighbours wrap take the scalar
+// node update twice.
 template <class S, int Coll, bool Odd>
 __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
     using Tb = Tables<D3Q19>;
@@ -161,7 +162,8 @@ __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, Leve
     if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (x0 >= geo.n[0] || y >= geo.n[1]) return;
-    if (!(y > 0 && y < geo.n[1] - 1 && z > 0 && z < geo.n[2] - 1)) {
+    const int gz = geo.g[2];  // 1 on a slab: z rows never wrap
+    if (!(y > 0 && y < geo.n[1] - 1 && (gz || (z > 0 && z < geo.n[2] - 1)))) {
         Coord c;
         c.x[0] = x0;
         c.x[1] = y;
@@ -172,7 +174,7 @@ __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, Leve
         return;
     }
     const int n0 = geo.n[0];
-    const int row = geo.a[0] * (y + geo.a[1] * z);
+    const int row = geo.a[0] * (y + geo.a[1] * (z + gz));
     // columns x0 - 1, x0, x0 + 1, x0 + 2 of the row (x wrapped)
     S* const pc[4] = {f + (row + (x0 == 0 ? n0 - 1 : x0 - 1)), f + (row + x0), f + (row + x0 + 1),
                       f + (row + (x0 + 2 == n0 ? 0 : x0 + 2))};

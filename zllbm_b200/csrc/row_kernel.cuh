@@ -110,14 +110,17 @@ __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, Level
     if ((blockIdx.x | blockIdx.y | threadIdx.x) == 0) sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (y >= geo.n[1]) return;  // whole warp: every shuffle below has all 32 lanes
     const int n1 = geo.n[1], n2 = geo.n[2];
-    // element offsets of the rows (y + dy, z + dz), wrapped, plus this lane's first node
+    // element offsets of the rows (y + dy, z + dz), wrapped (z: through the ghost planes of a
+    // slab, geo.ring, box coordinate z + 1), plus this lane's first node
     const int ym = y == 0 ? n1 - 1 : y - 1, yp = y == n1 - 1 ? 0 : y + 1;
-    const int zm = z == 0 ? n2 - 1 : z - 1, zp = z == n2 - 1 ? 0 : z + 1;
+    const int gz = geo.g[2];
+    const int zc = z + gz;
+    const int zm = gz ? z : (z == 0 ? n2 - 1 : z - 1), zp = gz ? z + 2 : (z == n2 - 1 ? 0 : z + 1);
     const uint32_t a0 = (uint32_t)geo.a[0], a1 = (uint32_t)geo.a[1];
     const uint32_t x0 = (uint32_t)(lane * V);
     auto rowoff = [&](int dy, int dz) -> uint32_t {
         const int yy = dy < 0 ? ym : (dy > 0 ? yp : y);
-        const int zz = dz < 0 ? zm : (dz > 0 ? zp : z);
+        const int zz = dz < 0 ? zm : (dz > 0 ? zp : zc);
         return a0 * ((uint32_t)yy + a1 * (uint32_t)zz) + x0;
     };
     const long long st = geo.stride;
@@ -167,11 +170,12 @@ __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, Level
     }
 }
 
-// Full periodic D3Q19 box (no ghost frame) in 16-bit storage whose rows are 32 V nodes long and
-// whose plane stride keeps every lane's vector aligned.
+// Full periodic D3Q19 box (no ghost frame), or a slab of one (geo.ring: ghost planes in z only), in
+// 16-bit storage whose rows are 32 V nodes long and whose plane stride keeps every lane's vector
+// aligned.
 inline int row_kernel_width(const LevelGeom& geo) {
-    if (!geo.periodic[0] || !geo.periodic[1] || !geo.periodic[2]) return 0;
-    if (geo.g[0] || geo.g[1] || geo.g[2] || geo.a[0] != geo.n[0] || geo.a[1] != geo.n[1]) return 0;
+    if (!geo.periodic[0] || !geo.periodic[1] || !(geo.periodic[2] || geo.ring)) return 0;
+    if (geo.g[0] || geo.g[1] || geo.g[2] != (geo.ring ? 1 : 0) || geo.a[0] != geo.n[0] || geo.a[1] != geo.n[1]) return 0;
     const int v = geo.n[0] / 32;
     if (geo.n[0] != 32 * v || (v != 4 && v != 8)) return 0;
     if (geo.stride % 8) return 0;

@@ -56,7 +56,7 @@ cudaError_t step_lco(bool bnd, bool masked, S* f, const LevelGeom& geo, const St
     if constexpr (L::kDims == 3) {
         if (geo.block[0] == kRowKernelBlockX && row_eligible(3, bnd, masked, p, (int)sizeof(S), geo))
             return step_row<S, C, O>(f, geo, p, s);
-        if (geo.block[0] < 0 && pair_eligible(3, bnd, masked, p, (int)sizeof(S)))
+        if (geo.block[0] < 0 && pair_eligible(3, bnd, masked, p, (int)sizeof(S), geo))
             return step_pair<S, C, O>(f, geo, p, s);
     }
     if (p.forced || p.les) {

@@ -92,12 +92,16 @@ class SlabSchedule:
     def swap(self, stage: int):
         self.receive(stage, self.exchange(self.sends(stage)))
 
+    def step(self):
+        """One time step and its exchange (stage 0 after an even step, stage 1 after an odd one)."""
+        stage = self.steps & 1
+        self.slab.step()
+        self.steps += 1
+        self.swap(stage)
+
     def step_pair(self):
-        self.slab.step()
-        self.swap(0)
-        self.slab.step()
-        self.swap(1)
-        self.steps += 2
+        self.step()
+        self.step()
 
 
 class LocalRing:
@@ -186,8 +190,10 @@ def split_planes(config) -> int:
 
 class DeviceSlab:
     """One rank's slab as a library context on the current GPU: a full box over planes [lo, hi)
-    of the global configuration's last axis, halo faces where the ring has a neighbour.  Exchange
-    buffers are torch uint8 device tensors of zl_halo_bytes."""
+    of the global configuration's last axis, halo faces where the ring has a neighbour.  Its node
+    list `codes` is every node of the slab's domain the way the reference stores a level (the
+    duplicated maximum plane of a periodic axis included), so populations and fields move without
+    codes in that order.  Exchange buffers are torch uint8 device tensors of zl_halo_bytes."""
 
     def __init__(self, config, lo: int, hi: int, ring: Ring):
         import torch
@@ -207,8 +213,8 @@ class DeviceSlab:
         self.box_lo = tuple(cfg.domain_min[:dims])
         self.box_n = tuple(cfg.domain_max[a] - cfg.domain_min[a] + (0 if cfg.bc_kind[2 * a] == zl.BC_PERIODIC else 1)
                            for a in range(dims))
-        pad = (0,) * (3 - dims)
-        self.ctx.set_level_box(0, self.box_lo + pad, self.box_n + (1,) * (3 - dims))
+        self.codes = zl.box_codes(dims, cfg.domain_min[:dims], cfg.domain_max[:dims])
+        self.ctx.set_level_nodes(0, self.codes)
         below, above = ring.halo_faces
         self.ctx.set_level_halo(0, (below << self.faces[0]) | (above << self.faces[1]))
         self.nbytes = {f: self.ctx.halo_bytes(0, f) for f in self.faces}
