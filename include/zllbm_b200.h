@@ -201,6 +201,16 @@ int zl_interpolate_interface(zl_ctx* ctx, int fine_level);
    results are identical either way (those steps touch disjoint data). */
 int zl_set_batching(zl_ctx* ctx, int enabled);
 
+/* In zl_advance of a multi-level context, issue each level's steps, immersed-boundary passes,
+   face passes and transfers on a stream of that level (finer levels at higher stream priority),
+   each operation waiting only for the last operations on the levels it touches: the background
+   level's step overlaps the finer levels' sub-steps and transfers.  On by default, and then
+   zl_set_batching has no effect on zl_advance; results are identical either way.  The caller's
+   stream (zl_set_stream) waits for all of it before zl_advance returns its work.  No reference
+   counterpart (the reference advances the levels one after another,
+   amr_project/grid/grid_manager.cpp:997-1023). */
+int zl_set_level_streams(zl_ctx* ctx, int enabled);
+
 /* Replay zl_advance as a captured CUDA graph of two background steps (every launch of the
    sub-cycled order, transfers and boundary passes included).  The graph is re-captured after any
    change of levels, interfaces, vertices or tuning.  Off by default. */

@@ -87,7 +87,7 @@ def test_cube_flow_graph_matches_plain():
     from zllbm_b200 import cube_flow
     topo = os.path.join(HERE, "golden", "topo_cube_small.npz")
     fast = cube_flow.run(topo, steps=6, warmup=2, graph=True, batching=True, log=quiet)
-    plain = cube_flow.run(topo, steps=6, warmup=2, graph=False, batching=False, log=quiet)
+    plain = cube_flow.run(topo, steps=6, warmup=2, graph=False, batching=False, streams=False, log=quiet)
     check_pair(fast, plain)
 
 
@@ -96,7 +96,7 @@ def test_cylinder_flow_graph_matches_plain():
     from zllbm_b200 import cylinder_flow
     topo = os.path.join(HERE, "golden", "topo_cylinder_small.npz")
     fast = cylinder_flow.run(topo, steps=6, warmup=2, graph=True, batching=True, log=quiet)
-    plain = cylinder_flow.run(topo, steps=6, warmup=2, graph=False, batching=False, log=quiet)
+    plain = cylinder_flow.run(topo, steps=6, warmup=2, graph=False, batching=False, streams=False, log=quiet)
     check_pair(fast, plain)
 
 

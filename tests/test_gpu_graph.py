@@ -125,13 +125,16 @@ def test_graph_recaptured_after_direct_step():
 @pytest.mark.gpu
 @pytest.mark.parametrize("name", AMR)
 def test_batched_levels_match_one_launch_per_level(name):
-    """Consecutive level steps with no transfer between them share one launch (default); turning
-    batching off runs one launch per level step.  FP64 results agree bit for bit."""
+    """The sub-cycled order on one stream with one launch per level step, with consecutive
+    independent level steps sharing one launch (batching), and on per-level streams ordered by the
+    levels each operation touches (default), directly and replayed from a graph: FP64 results
+    agree bit for bit."""
     import zllbm_b200 as zl
     meta, z = load_amr(name)
     levels = meta["levels"]
     out = []
-    for batched in (False, True):
+    modes = [(False, False, False), (False, True, False), (True, False, False), (True, False, True)]
+    for streams, batched, graph in modes:
         with zl.Context(config(meta, zl.STORAGE_F64)) as ctx:
             for lv in range(levels + 1):
                 ctx.set_level_nodes(lv, z[f"codes{lv}"])
@@ -142,10 +145,13 @@ def test_batched_levels_match_one_launch_per_level(name):
             if "ib" in meta:
                 v = z["vertices_before"]
                 ctx.ib_set_vertices(levels, v[:, 0:3], v[:, 3:6], v[:, 6])
+            ctx.set_level_streams(streams)
             ctx.set_batching(batched)
+            ctx.set_graph(graph)
             ctx.advance(meta["steps"] + 1)
             out.append([ctx.get_populations(lv, z[f"codes{lv}"]) for lv in range(levels + 1)])
-    compare(out[1], out[0], "ib" in meta)
+    for o in out[1:]:
+        compare(o, out[0], "ib" in meta)
 
 
 def _amr_ctx(meta, z, storage):

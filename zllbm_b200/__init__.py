@@ -390,6 +390,9 @@ class Context:
     def set_batching(self, enabled: bool):
         self._check(self.lib.zl_set_batching(self.handle, 1 if enabled else 0))
 
+    def set_level_streams(self, enabled: bool):
+        self._check(self.lib.zl_set_level_streams(self.handle, 1 if enabled else 0))
+
     def set_graph(self, enabled: bool):
         self._check(self.lib.zl_set_graph(self.handle, 1 if enabled else 0))
 

@@ -978,17 +978,17 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
     const long long st = geo.stride;
     auto plane = [&](int q) -> S* { return f + q * st; };
 
-    uint32_t info = 0;
-    if (Masked) {
-        info = __ldg(geo.info + self);
-        if (!(info & kInfoPresent)) return;
-    }
+    // the presence bit is tested once the population loads are issued, so that they do not wait
+    // for the info word (an absent cell's slots, and those of its neighbours, are memory of the
+    // box like any other: the reads stay in bounds and their values are dropped)
+    const uint32_t info = Masked ? __ldg(geo.info + self) : 0u;
 
     // The node update, given where population q is read from and where its post-collision value goes.
     auto body = [&](auto read_slot, auto write_slot) {
         T pre[Q], post[Q];
 #pragma unroll
         for (int q = 0; q < Q; ++q) pre[q] = St::load_raw(read_slot(q));
+        if (Masked && !(info & kInfoPresent)) return;
 
         T mac[4];
         NodeForce nf;
@@ -1024,8 +1024,17 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
 #pragma unroll
             for (int q = 0; q < Q; ++q) St::store_raw(write_slot(q), post[q]);
         }
-        // a masked node with no missing upstream neighbour (bits 1 .. Q-1 clear) has nothing to patch
-        if ((Bnd || Masked) && (!Masked || (info & ((1u << Q) - 2u)))) {
+        // a masked node with no missing upstream neighbour (bits 1 .. Q-1 clear), or a node of an
+        // unmasked box off its non-periodic edges, has nothing to patch
+        bool patch = false;
+        if (Masked) {
+            patch = (info & ((1u << Q) - 2u)) != 0u;
+        } else if (Bnd) {
+#pragma unroll
+            for (int a = 0; a < L::kDims; ++a)
+                if (!geo.periodic[a] && (c.x[a] == 0 || c.x[a] == geo.n[a] - 1)) patch = true;
+        }
+        if (patch) {
             const int faces = Bnd ? (Masked ? (int)((info >> kInfoFaceShift) & 63u) : on_faces(geo, c, L::kDims)) : 0;
 #pragma unroll
             for (int q = 1; q < Q; ++q) {

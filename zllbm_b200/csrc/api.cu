@@ -101,6 +101,13 @@ struct zl_ctx {
     int closure_every = 1;      // the network runs on every closure_every-th step of a level
     DeviceBuffer params_dev;    // StepParams of every level on the device (batched steps read them)
     bool batched = true;        // independent consecutive level steps share one launch (zl_set_batching)
+    // zl_set_level_streams: zl_advance issues each level's operations on that level's stream,
+    // ordered across streams by the levels each operation touches (created on first use)
+    bool level_streams = true;
+    cudaStream_t lstream[ZL_MAX_LEVELS] = {};
+    static constexpr int kEvents = 64;
+    cudaEvent_t events[kEvents] = {};
+    int next_event = 0;
     bool temporal = false;      // time interpolation at the coarse/fine interfaces (zl_set_temporal_interpolation)
     // staging of the node I/O calls (codes, populations, macros): grown on demand and kept until
     // the context is destroyed, so repeated exchanges allocate nothing
@@ -286,6 +293,10 @@ int zl_destroy(zl_ctx* ctx) {
     }
     ctx->scratch_flag.release();
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
+    for (cudaStream_t& s : ctx->lstream)
+        if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
+    for (cudaEvent_t& e : ctx->events)
+        if (e) cudaEventDestroy(e);
     cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return ZL_OK;
@@ -795,7 +806,89 @@ static bool batchable(const zl_ctx* ctx) {
     return true;
 }
 
+// Level streams of zl_advance: one stream per level (finer levels at higher priority: their chains
+// of short launches are the critical path), created on first use, and a pool of events.
+static int ensure_level_streams(zl_ctx* ctx) {
+    if (ctx->lstream[0]) return ZL_OK;
+    int least = 0, greatest = 0;
+    ZL_CUDA(ctx, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    for (int l = 0; l <= ctx->cfg.max_level; ++l) {
+        const int prio = least - l < greatest ? greatest : least - l;
+        ZL_CUDA(ctx, cudaStreamCreateWithPriority(&ctx->lstream[l], cudaStreamNonBlocking, prio));
+    }
+    for (cudaEvent_t& e : ctx->events) ZL_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return ZL_OK;
+}
+
+// The sub-cycled order with every operation on the stream of the level it advances.  An operation
+// touches a set of levels (a step or immersed-boundary pass: its level; a transfer: the fine level
+// and the coarse one); it waits for the last operation that touched any of them, so operations on
+// disjoint levels (the background step and the fine levels' chains of steps, passes and
+// transfers) overlap, while every level sees its operations in the reference's order.  The
+// results equal the single-stream order's bit for bit.  Works under stream capture: the waits
+// become the captured graph's edges.
+static int advance_streams(zl_ctx* ctx, int steps, const std::vector<int>& order) {
+    int rc = ensure_level_streams(ctx);
+    if (rc) return rc;
+    const int nl = ctx->cfg.max_level + 1;
+    const cudaStream_t main = ctx->stream;
+    auto next_event = [&]() -> cudaEvent_t {
+        cudaEvent_t e = ctx->events[ctx->next_event];
+        ctx->next_event = (ctx->next_event + 1) % zl_ctx::kEvents;
+        return e;
+    };
+    cudaEvent_t last[ZL_MAX_LEVELS];
+    cudaStream_t last_stream[ZL_MAX_LEVELS];
+    {
+        const cudaEvent_t fork = next_event();
+        ZL_CUDA(ctx, cudaEventRecord(fork, main));
+        for (int l = 0; l < nl; ++l) {
+            last[l] = fork;
+            last_stream[l] = main;
+        }
+    }
+    // run op on the stream of level `home` after the last operations on levels lo .. hi
+    auto run = [&](int home, int lo, int hi, auto op) -> int {
+        const cudaStream_t s = ctx->lstream[home];
+        for (int l = lo; l <= hi; ++l)
+            if (last_stream[l] != s) ZL_CUDA(ctx, cudaStreamWaitEvent(s, last[l], 0));
+        ctx->stream = s;
+        const int r = op();
+        ctx->stream = main;
+        if (r) return r;
+        const cudaEvent_t e = next_event();
+        ZL_CUDA(ctx, cudaEventRecord(e, s));
+        for (int l = lo; l <= hi; ++l) {
+            last[l] = e;
+            last_stream[l] = s;
+        }
+        return ZL_OK;
+    };
+    for (int s = 0; s < steps && !rc; ++s) {
+        int count[ZL_MAX_LEVELS] = {0};
+        for (int l : order) {
+            ++count[l];
+            if (ctx->temporal && l > 0 && count[l] % 2 == 0 &&
+                (rc = run(l, l - 1, l, [&] { return interpolate_interface(ctx, l, false); })))
+                break;
+            if ((rc = run(l, l, l, [&] { return zl_step_level(ctx, l); }))) break;
+            // InformationFromGridOfDifferentLevel (lbm_solver_interface.cpp:224-238)
+            if (l > 0 && count[l] % 2 == 0 && (rc = run(l, l - 1, l, [&] { return zl_transfer_levels(ctx, l); })))
+                break;
+        }
+    }
+    // join every level stream back into the caller's stream (also on failure, so that a capture
+    // in progress can end)
+    for (int l = 0; l < nl; ++l) {
+        const cudaEvent_t e = next_event();
+        ZL_CUDA(ctx, cudaEventRecord(e, ctx->lstream[l]));
+        ZL_CUDA(ctx, cudaStreamWaitEvent(main, e, 0));
+    }
+    return rc;
+}
+
 static int advance_direct(zl_ctx* ctx, int steps, const std::vector<int>& order) {
+    if (ctx->level_streams && ctx->cfg.max_level > 0) return advance_streams(ctx, steps, order);
     const bool batch = batchable(ctx);
     std::vector<int> group;
     auto flush = [&]() -> int {
@@ -906,6 +999,13 @@ int zl_interpolate_interface(zl_ctx* ctx, int fine_level) {
 int zl_set_batching(zl_ctx* ctx, int enabled) {
     if (!ctx) return ZL_EINVAL;
     ctx->batched = enabled != 0;
+    ++ctx->generation;
+    return ZL_OK;
+}
+
+int zl_set_level_streams(zl_ctx* ctx, int enabled) {
+    if (!ctx) return ZL_EINVAL;
+    ctx->level_streams = enabled != 0;
     ++ctx->generation;
     return ZL_OK;
 }
@@ -1222,9 +1322,10 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     IbVertices v = ib_view(ctx, L, level);
     ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.params, L.even_layout, (const int*)L.ib_nodes.ptr,
                                     L.n_ib_nodes, (double*)L.force.ptr, (double*)L.ib_vel.ptr, ctx->stream));
-    // interpolation: one warp per vertex, kIbWarps vertices per block; spread: one thread per node
+    // interpolation: one warp per vertex, kIbWarps vertices per block; spread: kIbSpreadLanes
+    // lanes per node
     const unsigned blocks = (unsigned)((v.n + kIbWarps - 1) / kIbWarps), threads = 32 * kIbWarps;
-    const unsigned nblocks = (unsigned)((L.n_ib_nodes + 127) / 128);
+    const unsigned nblocks = (unsigned)(((long long)L.n_ib_nodes * kIbSpreadLanes + 127) / 128);
     const int* pc = (const int*)L.ib_pair_cell.ptr;
     const double* pw = (const double*)L.ib_pair_w.ptr;
     const int *cs = (const int*)L.ib_csr_start.ptr, *cv = (const int*)L.ib_csr_vertex.ptr;

@@ -259,38 +259,51 @@ __global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(IbVertices v, c
     }
 }
 
-// Launch 3: a thread per stencil node sums F_i s_p over its pairs p (vertex i), in vertex order,
-// and writes the node force (launch 1 zeroed it; no other pass adds to it).  s_p = delta_p area_i /
-// (dt dx^(d-1)) and the vertex index come from the CSR arrays, laid out in node order.
+// Launch 3: kIbSpreadLanes lanes per stencil node sum F_i s_p over the node's pairs p (vertex i):
+// lane k takes pairs k, k + kIbSpreadLanes, ... of the node's CSR row, two at a time with their
+// loads issued first, and the lanes' sums are combined by a fixed butterfly of shuffles
+// (deterministic).  The first lane writes the node force (launch 1 zeroed it; no other pass adds
+// to it).  s_p = delta_p area_i / (dt dx^(d-1)) and the vertex index come from the CSR arrays,
+// laid out in node order.  A node has about 16 (3D) pairs: the lanes cut the chain of dependent
+// loads per thread eightfold and give the launch eight times the threads.
+constexpr int kIbSpreadLanes = 8;
+
 template <int D>
 __global__ void ib_spread_kernel(IbVertices v, const int* __restrict__ nodes, int n_nodes,
                                  const int* __restrict__ csr_start, const int* __restrict__ csr_vertex,
                                  const double* __restrict__ csr_share, double* __restrict__ node_force) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n_nodes) return;
+    constexpr int G = kIbSpreadLanes;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int j = (int)(t / G), k = (int)(t % G);
+    const bool live = j < n_nodes;  // every lane of the warp takes part in the shuffles
     double F[3] = {0., 0., 0.};
-    const int s1 = csr_start[j + 1];
-    int s = csr_start[j];
-    // four pairs per round: their loads are issued before the sums (kept in pair order)
-    for (; s + 4 <= s1; s += 4) {
-        double sh[4], f4[4][3];
+    if (live) {
+        const int s1 = csr_start[j + 1];
+        int s = csr_start[j] + k;
+        for (; s + G < s1; s += 2 * G) {
+            const int i0 = __ldg(csr_vertex + s), i1 = __ldg(csr_vertex + s + G);
+            const double h0 = __ldg(csr_share + s), h1 = __ldg(csr_share + s + G);
+            double f0[3], f1[3];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int i = __ldg(csr_vertex + s + e);
-            sh[e] = __ldg(csr_share + s + e);
+            for (int a = 0; a < D; ++a) {
+                f0[a] = v.force[i0 * 3 + a];
+                f1[a] = v.force[i1 * 3 + a];
+            }
 #pragma unroll
-            for (int a = 0; a < D; ++a) f4[e][a] = v.force[i * 3 + a];
+            for (int a = 0; a < D; ++a) F[a] = F[a] + f0[a] * h0 + f1[a] * h1;
         }
+        if (s < s1) {
+            const int i = __ldg(csr_vertex + s);
+            const double h = __ldg(csr_share + s);
 #pragma unroll
-        for (int e = 0; e < 4; ++e)
+            for (int a = 0; a < D; ++a) F[a] += v.force[i * 3 + a] * h;
+        }
+    }
 #pragma unroll
-            for (int a = 0; a < D; ++a) F[a] += f4[e][a] * sh[e];
-    }
-    for (; s < s1; ++s) {
-        const int i = __ldg(csr_vertex + s);
-        const double sh = __ldg(csr_share + s);
-        for (int a = 0; a < D; ++a) F[a] += v.force[i * 3 + a] * sh;
-    }
+    for (int off = G / 2; off > 0; off >>= 1)
+#pragma unroll
+        for (int a = 0; a < D; ++a) F[a] += __shfl_xor_sync(0xffffffffu, F[a], off);
+    if (!live || k) return;
     const long long cell = nodes[j];
     for (int a = 0; a < D; ++a) node_force[cell * 3 + a] = F[a];
 }

@@ -2,8 +2,8 @@
 domain with two refinement levels (factor 2 each, sub-cycled 1:2:4) around a cube of 16 coarse
 cells, inflow 0.05 (non-equilibrium extrapolation), convective outflow, bounce-back side walls,
 Re = 1000 on the cube edge, FP32 storage; the cube is an immersed boundary (direct forcing, its
-surface vertices on the finest level).  All level steps run as batched launches replayed from a
-CUDA graph.
+surface vertices on the finest level).  The levels' steps, passes and transfers run on per-level
+streams (the background step overlapping the finer levels' sub-steps), replayed from a CUDA graph.
 
     python -m zllbm_b200.cube_flow [--topology cube_topology.npz] [--steps 64] [--warmup 4]
 
@@ -79,13 +79,14 @@ def build(topology: str, storage: int = zl.STORAGE_F32):
     return ctx, meta, nodes, len(xyz)
 
 
-def run(topology: str, steps: int = 64, warmup: int = 4, graph: bool = True, batching: bool = True,
+def run(topology: str, steps: int = 64, warmup: int = 4, graph: bool = True, batching: bool = True, streams: bool = True,
         log=print) -> dict:
     import torch
     ctx, meta, nodes, nv = build(topology)
     levels = meta["levels"]
     lups_per_step = sum(n * (1 << lv) for lv, n in enumerate(nodes))
     ctx.set_batching(batching)
+    ctx.set_level_streams(streams)
     ctx.set_graph(graph)
     ctx.advance(warmup)
     ctx.synchronize()
@@ -103,7 +104,7 @@ def run(topology: str, steps: int = 64, warmup: int = 4, graph: bool = True, bat
                        f"coarse {'x'.join(str(v) for v in meta['n'])}, {levels} refinement levels "
                        f"({':'.join(str(1 << lv) for lv in range(levels + 1))} sub-cycling), inflow {U_IN}, convective outflow, "
                        f"Re {RE:.0f}, FP32, immersed-boundary cube ({nv} vertices)",
-           "batched_level_steps": batching, "cuda_graph": graph,
+           "batched_level_steps": batching and not streams, "level_streams": streams, "cuda_graph": graph,
            "nodes_per_level": nodes, "lups_per_coarse_step": lups_per_step, "coarse_steps": steps,
            "ms_per_coarse_step": ms / steps, "mlups": lups_per_step * steps / (ms * 1e-3) / 1e6,
            "cube_force_total": [float(v) for v in drag], "mass_per_level": mass,
@@ -119,9 +120,10 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=4)
     ap.add_argument("--graph", type=int, default=1)
     ap.add_argument("--batching", type=int, default=1)
+    ap.add_argument("--streams", type=int, default=1, help="per-level streams (zl_set_level_streams)")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
-    run(a.topology, a.steps, a.warmup, bool(a.graph), bool(a.batching))
+    run(a.topology, a.steps, a.warmup, bool(a.graph), bool(a.batching), bool(a.streams))
     print(f"wall {time.perf_counter() - t0:.1f} s")
 
 

@@ -2,8 +2,8 @@
 levels (factor 2 each, sub-cycled 1:2:4:8) around a cylinder of diameter 40 finest cells (5 coarse
 cells), inflow 0.04 (non-equilibrium extrapolation), convective outflow, bounce-back side walls,
 Re = 200 on the diameter, FP32 storage; the cylinder is 400 immersed-boundary vertices on the
-finest level (direct forcing with the reference's four-point delta kernel).  All level steps run
-as batched launches replayed from a CUDA graph; drag and lift are the FP64 sums of the vertex
+finest level (direct forcing with the reference's four-point delta kernel).  The levels' steps,
+passes and transfers run on per-level streams, replayed from a CUDA graph; drag and lift are the FP64 sums of the vertex
 forces.
 
     python -m zllbm_b200.cylinder_flow [--topology cylinder_topology.npz] [--steps 400] [--warmup 8]
@@ -62,13 +62,14 @@ def build(topology: str, storage: int = zl.STORAGE_F32):
     return ctx, meta, nodes
 
 
-def run(topology: str, steps: int = 400, warmup: int = 8, graph: bool = True, batching: bool = True,
+def run(topology: str, steps: int = 400, warmup: int = 8, graph: bool = True, batching: bool = True, streams: bool = True,
         log=print) -> dict:
     import torch
     ctx, meta, nodes = build(topology)
     levels = meta["levels"]
     lups_per_step = sum(n * (1 << lv) for lv, n in enumerate(nodes))
     ctx.set_batching(batching)
+    ctx.set_level_streams(streams)
     ctx.set_graph(graph)
     ctx.advance(warmup)
     ctx.synchronize()
@@ -87,7 +88,7 @@ def run(topology: str, steps: int = 400, warmup: int = 8, graph: bool = True, ba
                        f"vertices), coarse {'x'.join(str(v) for v in meta['n'])}, {levels} refinement levels "
                        f"({cycles} sub-cycling), inflow {U_IN}, "
                        f"convective outflow, Re {RE:.0f}, FP32",
-           "batched_level_steps": batching, "cuda_graph": graph,
+           "batched_level_steps": batching and not streams, "level_streams": streams, "cuda_graph": graph,
            "nodes_per_level": nodes, "lups_per_coarse_step": lups_per_step, "coarse_steps": steps,
            "ms_per_coarse_step": ms / steps, "mlups": lups_per_step * steps / (ms * 1e-3) / 1e6,
            "cylinder_force_total_fp64": [float(v) for v in force],
@@ -103,9 +104,10 @@ def main(argv=None):
     ap.add_argument("--warmup", type=int, default=8)
     ap.add_argument("--graph", type=int, default=1)
     ap.add_argument("--batching", type=int, default=1)
+    ap.add_argument("--streams", type=int, default=1, help="per-level streams (zl_set_level_streams)")
     a = ap.parse_args(argv)
     t0 = time.perf_counter()
-    run(a.topology, a.steps, a.warmup, bool(a.graph), bool(a.batching))
+    run(a.topology, a.steps, a.warmup, bool(a.graph), bool(a.batching), bool(a.streams))
     print(f"wall {time.perf_counter() - t0:.1f} s")
 
 
