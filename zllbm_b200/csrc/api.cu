@@ -53,7 +53,7 @@ struct Level {
     long long n_node_codes = 0;
     // coarse/fine transfer with the next coarser level (this level is the fine side)
     DeviceBuffer macro;                                   // rho, u of transfer sources
-    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w;
+    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w, c2f_w32;
     DeviceBuffer c2f_ucell, c2f_ufine, c2f_g;  // distinct sources: cell, kind, values of a transfer
     int n_c2f = 0, n_c2f_src = 0;
     DeviceBuffer f2c_coarse, f2c_fine;
@@ -716,7 +716,7 @@ static int level_faces(zl_ctx* ctx, Level& L) {
 
 static C2FStencil c2f_stencil(const Level& F) {
     return C2FStencil{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
-                      (const double*)F.c2f_w.ptr,      F.n_c2f,
+                      (const double*)F.c2f_w.ptr,      (const float*)F.c2f_w32.ptr, F.n_c2f,
                       (const int*)F.c2f_ucell.ptr,     (const uint8_t*)F.c2f_ufine.ptr,
                       F.n_c2f_src,                     F.c2f_g.ptr};
 }
@@ -1248,6 +1248,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
     if ((rc = upload_vec(ctx, F.c2f_target, tgt)) || (rc = upload_vec(ctx, F.c2f_offset, off)) ||
         (rc = upload_vec(ctx, F.c2f_src, src)) || (rc = upload_vec(ctx, F.c2f_ucell, ucell)) ||
         (rc = upload_vec(ctx, F.c2f_ufine, ufine)) || (rc = upload_vec(ctx, F.c2f_w, wts)) ||
+        (rc = upload_vec(ctx, F.c2f_w32, std::vector<float>(wts.begin(), wts.end()))) ||
         (rc = upload_vec(ctx, F.f2c_coarse, f2c_c)) || (rc = upload_vec(ctx, F.f2c_fine, f2c_f)))
         return rc;
     F.n_c2f = (int)tgt.size();

@@ -182,7 +182,8 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
                         cudaStream_t s) {                                                                        \
         if (st.n_targets <= 0) return cudaSuccess;                                                               \
         const unsigned sblocks = (unsigned)((st.n_sources + 127) / 128);                                         \
-        const unsigned wblocks = (unsigned)(((long long)st.n_targets * 32 + kC2fThreads - 1) / kC2fThreads);     \
+        const unsigned wblocks = (unsigned)(((long long)st.n_targets * (dims == 2 ? 9 : 19) + kC2fThreads - 1) /  \
+                                            kC2fThreads);                                                        \
         if (dims == 2) {                                                                                         \
             if (st.n_sources > 0)                                                                                \
                 c2f_sources_kernel<D2Q9, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,    \

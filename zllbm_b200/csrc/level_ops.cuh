@@ -267,13 +267,14 @@ __global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParam
 // arrays, in the reference's loop order (z outer, x inner, grid/grid_interpolation.cpp:485-517).
 // Every distinct source node is evaluated once per transfer (c2f_sources_kernel) into the
 // table g; the targets then form their weighted sums from the table.
-constexpr int kC2fThreads = 128;  // explosion kernel: 4 targets (warps) per block
+constexpr int kC2fThreads = 128;  // explosion kernel block
 
 struct C2FStencil {
     const int* target;        // fine cell of every target node
     const int* offset;        // n_targets + 1
     const int* src;           // entry -> row of the source table
     const double* weight;
+    const float* weight32;    // the same weights rounded to FP32 (FP32 / FP16 / BF16 storage)
     int n_targets;
     const int* src_cell;      // per source: coarse cell (src_fine == 0) or fine cell (src_fine == 1)
     const uint8_t* src_fine;
@@ -335,10 +336,11 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
 // targets get 0.5 (prev + value) instead, the time interpolation between the last transfer and
 // the coarse level's current state (no counterpart in the reference, whose explosion is spatial
 // only); store = 0 only saves.
-// One warp per target: lane q (< Q) sums population q over the target's sources in table order
-// (so FP64 keeps its summation order); the source rows are read coalesced, four rows' loads in
-// flight at a time, and the rows' indices and weights are fetched 32 at a time and broadcast by
-// shuffle.
+// One thread per (target, population q), consecutive threads taking consecutive q of a target:
+// every lane of a warp works (Q = 19 or 9 does not divide a warp), the target's source indices
+// and weights are loads the target's lanes share, and the source rows are read coalesced.  Each
+// thread sums over the target's sources in table order (FP64 keeps its summation order), four
+// sources' loads in flight at a time.
 template <class L, class S>
 __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
                                                          StepParams fp, C2FStencil st, double* __restrict__ save,
@@ -346,45 +348,34 @@ __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, Le
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
-    const int t = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (t >= st.n_targets) return;  // whole warp
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)st.n_targets * Q) return;
+    const int t = (int)(i / Q), q = (int)(i - (long long)t * Q);
     const T* __restrict__ g = static_cast<const T*>(st.g);
-    const bool active = lane < Q;
-    const int q = active ? lane : 0;
+    auto weight = [&](int k) -> T {
+        if constexpr (sizeof(T) == 8) return __ldg(st.weight + k);
+        else return __ldg(st.weight32 + k);
+    };
     T acc = (T)0;
-    const int k0 = st.offset[t], k1 = st.offset[t + 1];
-    for (int kb = k0; kb < k1; kb += 32) {
-        int src = 0;
-        double wd = 0.;
-        if (kb + lane < k1) {
-            src = st.src[kb + lane];
-            wd = st.weight[kb + lane];
-        }
-        const int m = k1 - kb < 32 ? k1 - kb : 32;
-        int j = 0;
-        // four rows per round: their loads are issued before the sums that use them
-        for (; j + 4 <= m; j += 4) {
-            T w4[4], g4[4];
+    const int k1 = __ldg(st.offset + t + 1);
+    int k = __ldg(st.offset + t);
+    for (; k + 4 <= k1; k += 4) {
+        int s4[4];
+        T w4[4], g4[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int sj = __shfl_sync(0xffffffffu, src, j + e);
-                w4[e] = (T)__shfl_sync(0xffffffffu, wd, j + e);
-                g4[e] = __ldg(g + (long long)sj * Q + q);
-            }
+        for (int e = 0; e < 4; ++e) {
+            s4[e] = __ldg(st.src + k + e);
+            w4[e] = weight(k + e);
+        }
 #pragma unroll
-            for (int e = 0; e < 4; ++e) acc = acc + w4[e] * g4[e];
-        }
-        for (; j < m; ++j) {
-            const int sj = __shfl_sync(0xffffffffu, src, j);
-            const T w = (T)__shfl_sync(0xffffffffu, wd, j);
-            acc = acc + w * __ldg(g + (long long)sj * Q + q);
-        }
+        for (int e = 0; e < 4; ++e) g4[e] = __ldg(g + (long long)s4[e] * Q + q);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) acc = acc + w4[e] * g4[e];
     }
-    if (!active) return;
-    if (save) save[(long long)t * Q + q] = (double)acc;
+    for (; k < k1; ++k) acc = acc + weight(k) * __ldg(g + (long long)__ldg(st.src + k) * Q + q);
+    if (save) save[i] = (double)acc;
     if (!store) return;
-    if (prev) acc = (T)0.5 * ((T)prev[(long long)t * Q + q] + acc);
+    if (prev) acc = (T)0.5 * ((T)prev[i] + acc);
     const Coord c = cell_coord(fgeo, st.target[t]);
     St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), acc, fp);
 }
