@@ -586,7 +586,8 @@ constexpr uint32_t kLsSmemLaunch = kFwSmem;
 template <class S, int Coll, bool Odd>
 __global__ void __launch_bounds__(128, 5) learned_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p,
                                                            const float* __restrict__ net, float fallback_c,
-                                                           float* __restrict__ c_node, int* __restrict__ err) {
+                                                           float* __restrict__ c_node, int* __restrict__ err,
+                                                           FastDiv nx, FastDiv ny) {
     using Tb = Tables<D3Q19>;
     using St = Storage<S>;
     extern __shared__ __align__(1024) uint8_t sm[];
@@ -605,11 +606,13 @@ __global__ void __launch_bounds__(128, 5) learned_step_kernel(S* __restrict__ f,
         const bool valid = i < nn;
         Coord c;
         {
-            const long long ii = valid ? i : 0;
-            c.x[0] = (int)(ii % geo.n[0]);
-            const long long r = ii / geo.n[0];
-            c.x[1] = (int)(r % geo.n[1]);
-            c.x[2] = (int)(r / geo.n[1]);
+            // node index -> coordinates (x fastest) by multiply-shift division (the box holds
+            // fewer than 2^31 cells)
+            const uint32_t ii = valid ? (uint32_t)i : 0u;
+            const uint32_t r = nx.div(ii), zq = ny.div(r);
+            c.x[0] = (int)(ii - r * (uint32_t)geo.n[0]);
+            c.x[1] = (int)(r - zq * (uint32_t)geo.n[1]);
+            c.x[2] = (int)zq;
         }
         // periodic neighbours of the node (the level wraps on every axis)
         int bx[3], row[3][3];
@@ -696,7 +699,9 @@ static cudaError_t learned_step_s(int coll, bool odd, void* f, const LevelGeom& 
             per_sm = per_sm < kMaxCtaPerSm ? per_sm : kMaxCtaPerSm;
             grid[slot] = sms * (per_sm > 0 ? per_sm : 1);
         }
-        kernel<<<grid[slot], 128, kLsSmemLaunch, s>>>(static_cast<S*>(f), geo, p, net, fallback_c, c_node, err);
+        kernel<<<grid[slot], 128, kLsSmemLaunch, s>>>(static_cast<S*>(f), geo, p, net, fallback_c, c_node, err,
+                                                      FastDiv::make((uint32_t)geo.n[0]),
+                                                      FastDiv::make((uint32_t)geo.n[1]));
         return cudaGetLastError();
     };
     if (coll == kMrt)
