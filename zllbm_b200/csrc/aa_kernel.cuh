@@ -39,6 +39,27 @@ constexpr int kInfoFaceShift = 24;  // 6 bits: on face xmin..zmax (reference bou
 constexpr int kExtForce = 1;
 constexpr int kExtLes = 2;
 
+// Division of 31-bit unsigned integers by a fixed divisor through one widening multiply and a
+// shift (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI
+// 1994, the round-up method): with l = ceil(log2 d) and m = floor(2^(31 + l) / d) + 1,
+// floor(n / d) = floor(n m / 2^(31 + l)) for every 0 <= n < 2^31; m < 2^32 for d >= 2.
+struct FastDiv {
+    uint32_t d = 1, m = 0, shift = 0;
+    ZL_HD static FastDiv make(uint32_t divisor) {
+        FastDiv f;
+        f.d = divisor;
+        if (divisor <= 1) return f;
+        uint32_t l = 0;
+        while ((1ull << l) < divisor) ++l;
+        f.shift = 31 + l;
+        f.m = (uint32_t)((1ull << f.shift) / divisor + 1);
+        return f;
+    }
+    ZL_HD uint32_t div(uint32_t n) const {
+        return d <= 1 ? n : (uint32_t)(((unsigned long long)n * m) >> shift);
+    }
+};
+
 struct LevelGeom {
     int n[3];          // nodes per axis (periodic axes hold each plane once)
     int g[3];          // ghost frame width per axis (0 on periodic axes, 1 otherwise)
@@ -52,6 +73,7 @@ struct LevelGeom {
     // sharded lattice): every upstream node is present, the z ones in the ghost planes, so the
     // kernels of full periodic boxes apply with z addressed through the ghost frame
     int ring;
+    FastDiv fa0, fa1;  // division by a[0] and a[1] (cell index -> box coordinates)
 };
 
 struct StepParams {
@@ -558,17 +580,24 @@ __device__ __forceinline__ void mrt_d3q19_dev(const float* d, const float* n, fl
     for (int q = 0; q < 19; ++q) out[q] = fmaf(-omega, n[q], d[q]) - c[q];
 }
 
-// D3Q19 SRT without forcing, optionally with Smagorinsky, in one pass over the deviations d
-// (scaled units): the pair sums / differences of opposite directions give the density, momentum
-// and second moments; the non-equilibrium stress of the reference's second-order equilibrium
-// (lbm_solver_interface.cpp:374-435) is then Pi_ab = sum_q c_a c_b d_q - drho / 3 delta_ab - G u_a u_b
-// (G = scale rho), its diagonal sums S1 + Sxy + Sxz (x), ... and its off-diagonal S4 - S5 (xy),
-// S6 - S7 (xz), S8 - S9 (yz).  Smagorinsky: tau = tau0 + (sqrt(tau0^2 + C sqrt(2 Pi:Pi)) - tau0) / 2
+// D3Q19 SRT, optionally with Smagorinsky and with a Guo body force F (Forced), in one pass over
+// the deviations d (scaled units): the pair sums / differences of opposite directions give the
+// density, momentum and second moments; the non-equilibrium stress of the reference's second-
+// order equilibrium (lbm_solver_interface.cpp:374-435) is then
+// Pi_ab = sum_q c_a c_b d_q - drho / 3 delta_ab - G u_a u_b (G = scale rho), its diagonal sums
+// S1 + Sxy + Sxz (x), ... and its off-diagonal S4 - S5 (xy), S6 - S7 (xz), S8 - S9 (yz).
+// Smagorinsky: tau = tau0 + (sqrt(tau0^2 + C sqrt(2 Pi:Pi)) - tau0) / 2
 // (lbm_les_smagorinsky.cpp:22-94 with the increment added to tau0).  The update
-// f*_q = (1 - omega) d_q + omega feq_q is formed per opposite pair from its sum and difference:
-// feq_q = w (B + 4.5 G (c.u)^2) + 3 w (c.j), B = drho - 1.5 G u^2.
-__device__ __forceinline__ void srt_d3q19_fused(const float* d, float* out, const StepParams& p, float* mac,
-                                                bool les, float les_c) {
+// f*_q = (1 - omega) d_q + omega feq_q (+ (1 - omega / 2) dt Fq_q) is formed per opposite pair
+// from its sum and difference: feq_q = w (B + 4.5 G (c.u)^2) + 3 w (c.j), B = drho - 1.5 G u^2.
+// With a force (CalMacroForce*, CalForcingTerming3D: lbm_solver_interface.cpp:443-470, 541-592)
+// the velocity is shifted by F dt / (2 rho), j is G u, the stress gains dt (F_a u_b + F_b u_a) / 2,
+// and Fq_q = w [3 (c - u).F + 9 (c.u)(c.F)] splits into an even part w (9 (c.u)(c.F) - 3 u.F) and
+// an odd part 3 w (c.F) per pair: the same update as the general forced path (feq_neq_dev and the
+// per-direction Guo term), in another rounding order.
+template <bool Forced>
+__device__ __forceinline__ void srt_d3q19_fused_t(const float* d, float* out, const StepParams& p, float* mac,
+                                                  bool les, float les_c, const float* F) {
     const float S1 = d[1] + d[2], D1 = d[1] - d[2];
     const float S2 = d[3] + d[4], D2 = d[3] - d[4];
     const float S3 = d[5] + d[6], D3 = d[5] - d[6];
@@ -580,27 +609,53 @@ __device__ __forceinline__ void srt_d3q19_fused(const float* d, float* out, cons
     const float S9 = d[16] + d[17], D9 = d[16] - d[17];
     const float Sxy = S4 + S5, Sxz = S6 + S7, Syz = S8 + S9;
     const float drho = ((d[0] + S1) + (S2 + S3)) + ((Sxy + Sxz) + Syz);
-    const float jx = D1 + (D4 - D5) + (D6 - D7);
-    const float jy = D2 + (D4 + D5) + (D8 - D9);
-    const float jz = D3 + (D6 + D7) + (D8 + D9);
+    float jx = D1 + (D4 - D5) + (D6 - D7);
+    float jy = D2 + (D4 + D5) + (D8 - D9);
+    float jz = D3 + (D6 + D7) + (D8 + D9);
     const float rho = fmaf(drho, p.inv_scale, 1.f);
-    const float k = __fdividef(p.inv_scale, rho);  // fast reciprocal, two ulps (rho is close to 1)
-    const float ux = jx * k, uy = jy * k, uz = jz * k;
+    float ux, uy, uz;
+    if constexpr (Forced) {
+        const float k = p.inv_scale / rho, h = 0.5f * (float)p.dt / rho;
+        ux = fmaf(h, F[0], jx * k);
+        uy = fmaf(h, F[1], jy * k);
+        uz = fmaf(h, F[2], jz * k);
+    } else {
+        const float k = __fdividef(p.inv_scale, rho);  // fast reciprocal, two ulps (rho is close to 1)
+        ux = jx * k;
+        uy = jy * k;
+        uz = jz * k;
+    }
     mac[0] = rho;
     mac[1] = ux;
     mac[2] = uy;
     mac[3] = uz;
     const float ux2 = ux * ux, uy2 = uy * uy, uz2 = uz * uz;
     const float G = p.scale * rho;
+    if constexpr (Forced) {
+        // the momentum of the shifted equilibrium
+        jx = G * ux;
+        jy = G * uy;
+        jz = G * uz;
+    }
     float omega = p.omega32;
     if (les) {
         const float t = drho * (1.f / 3.f);
-        const float pxx = fmaf(-G, ux2, (S1 + Sxy + Sxz) - t);
-        const float pyy = fmaf(-G, uy2, (S2 + Sxy + Syz) - t);
-        const float pzz = fmaf(-G, uz2, (S3 + Sxz + Syz) - t);
-        const float pxy = fmaf(-G, ux * uy, S4 - S5);
-        const float pxz = fmaf(-G, ux * uz, S6 - S7);
-        const float pyz = fmaf(-G, uy * uz, S8 - S9);
+        float pxx = fmaf(-G, ux2, (S1 + Sxy + Sxz) - t);
+        float pyy = fmaf(-G, uy2, (S2 + Sxy + Syz) - t);
+        float pzz = fmaf(-G, uz2, (S3 + Sxz + Syz) - t);
+        float pxy = fmaf(-G, ux * uy, S4 - S5);
+        float pxz = fmaf(-G, ux * uz, S6 - S7);
+        float pyz = fmaf(-G, uy * uz, S8 - S9);
+        if constexpr (Forced) {
+            const float ds = (float)p.dt * p.scale;
+            const float fx = ds * F[0] * ux, fy = ds * F[1] * uy, fz = ds * F[2] * uz;
+            pxx += fx;
+            pyy += fy;
+            pzz += fz;
+            pxy += 0.5f * (fx + fy);
+            pxz += 0.5f * (fx + fz);
+            pyz += 0.5f * (fy + fz);
+        }
         const float is2 = p.inv_scale * p.inv_scale;
         const float pi2 = is2 * (pxx * pxx + pyy * pyy + pzz * pzz + 2.f * (pxy * pxy + pxz * pxz + pyz * pyz));
         const float tau0 = (float)p.tau;
@@ -612,30 +667,76 @@ __device__ __forceinline__ void srt_d3q19_fused(const float* d, float* out, cons
     const float ow0 = omega * (1.f / 3.f), ow1 = omega * (1.f / 18.f), ow2 = omega * (1.f / 36.f);
     const float K1 = 4.5f * ow1 * G, L1 = ow1 * B, o1 = 3.f * ow1;
     const float K2 = 4.5f * ow2 * G, L2 = ow2 * B, o2 = 3.f * ow2;
-    out[0] = fmaf(1.f - omega, d[0], ow0 * B);
+    // Guo term parts, scaled: gF_w = (1 - omega/2) dt scale w
+    float g1 = 0.f, g2 = 0.f, uF3 = 0.f;
+    if constexpr (Forced) {
+        const float g = (1.f - 0.5f * omega) * (float)p.dt * p.scale;
+        g1 = g * (1.f / 18.f);
+        g2 = g * (1.f / 36.f);
+        uF3 = 3.f * (ux * F[0] + uy * F[1] + uz * F[2]);
+        out[0] = fmaf(1.f - omega, d[0], fmaf(ow0, B, -(g * (1.f / 3.f)) * uF3));
+    } else {
+        out[0] = fmaf(1.f - omega, d[0], ow0 * B);
+    }
     auto pair = [&](int q, int o, float S, float D, float even, float odd) {
         const float e = fmaf(h, S, even), od = fmaf(h, D, odd);
         out[q] = e + od;
         out[o] = e - od;
     };
-    pair(1, 2, S1, D1, fmaf(K1, ux2, L1), o1 * jx);
-    pair(3, 4, S2, D2, fmaf(K1, uy2, L1), o1 * jy);
-    pair(5, 6, S3, D3, fmaf(K1, uz2, L1), o1 * jz);
+    // (even, odd) Guo parts of a pair with c.u = cu, c.F = cF and weight factor gw
+    auto force = [&](float gw, float cu, float cF, float& even, float& odd) {
+        if constexpr (Forced) {
+            even = fmaf(gw, fmaf(9.f * cu, cF, -uF3), even);
+            odd = fmaf(gw * 3.f, cF, odd);
+        }
+    };
+    {
+        float e1 = fmaf(K1, ux2, L1), od1 = o1 * jx, e2 = fmaf(K1, uy2, L1), od2 = o1 * jy;
+        float e3 = fmaf(K1, uz2, L1), od3 = o1 * jz;
+        if constexpr (Forced) {
+            force(g1, ux, F[0], e1, od1);
+            force(g1, uy, F[1], e2, od2);
+            force(g1, uz, F[2], e3, od3);
+        }
+        pair(1, 2, S1, D1, e1, od1);
+        pair(3, 4, S2, D2, e2, od2);
+        pair(5, 6, S3, D3, e3, od3);
+    }
     {
         const float a = ux + uy, b = uy - ux;
-        pair(7, 10, S4, D4, fmaf(K2, a * a, L2), o2 * (jx + jy));
-        pair(8, 9, S5, D5, fmaf(K2, b * b, L2), o2 * (jy - jx));
+        float ea = fmaf(K2, a * a, L2), oa = o2 * (jx + jy), eb = fmaf(K2, b * b, L2), ob = o2 * (jy - jx);
+        if constexpr (Forced) {
+            force(g2, a, F[0] + F[1], ea, oa);
+            force(g2, b, F[1] - F[0], eb, ob);
+        }
+        pair(7, 10, S4, D4, ea, oa);
+        pair(8, 9, S5, D5, eb, ob);
     }
     {
         const float a = ux + uz, b = uz - ux;
-        pair(11, 14, S6, D6, fmaf(K2, a * a, L2), o2 * (jx + jz));
-        pair(12, 13, S7, D7, fmaf(K2, b * b, L2), o2 * (jz - jx));
+        float ea = fmaf(K2, a * a, L2), oa = o2 * (jx + jz), eb = fmaf(K2, b * b, L2), ob = o2 * (jz - jx);
+        if constexpr (Forced) {
+            force(g2, a, F[0] + F[2], ea, oa);
+            force(g2, b, F[2] - F[0], eb, ob);
+        }
+        pair(11, 14, S6, D6, ea, oa);
+        pair(12, 13, S7, D7, eb, ob);
     }
     {
         const float a = uy + uz, b = uz - uy;
-        pair(15, 18, S8, D8, fmaf(K2, a * a, L2), o2 * (jy + jz));
-        pair(16, 17, S9, D9, fmaf(K2, b * b, L2), o2 * (jz - jy));
+        float ea = fmaf(K2, a * a, L2), oa = o2 * (jy + jz), eb = fmaf(K2, b * b, L2), ob = o2 * (jz - jy);
+        if constexpr (Forced) {
+            force(g2, a, F[1] + F[2], ea, oa);
+            force(g2, b, F[2] - F[1], eb, ob);
+        }
+        pair(15, 18, S8, D8, ea, oa);
+        pair(16, 17, S9, D9, eb, ob);
     }
+}
+
+__device__ __forceinline__ void srt_d3q19_fused(const float* d, float* out, const StepParams& p, float* mac,
+                                                bool les, float les_c) {
+    srt_d3q19_fused_t<false>(d, out, p, mac, les, les_c, nullptr);
 }
 
 // D3Q19 MRT without forcing or LES, in one pass over the deviations d (scaled units).
@@ -791,8 +892,13 @@ __device__ __forceinline__ void collide_dev(const float* d, float* out, const St
             mrt_d3q19_fused(d, out, p, mac);
             return;
         }
-        if (coll == kSrt && !nf) {
-            srt_d3q19_fused(d, out, p, mac, Les, les_c);
+        if (coll == kSrt) {
+            if (!nf) {
+                srt_d3q19_fused(d, out, p, mac, Les, les_c);
+            } else {
+                const float F[3] = {(float)nf->F[0], (float)nf->F[1], (float)nf->F[2]};
+                srt_d3q19_fused_t<true>(d, out, p, mac, Les, les_c, F);
+            }
             return;
         }
     }
@@ -1167,26 +1273,6 @@ __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>:
 }
 
 // ---------------------------------------------------------------- several levels in one launch
-// Division of 31-bit unsigned integers by a fixed divisor through one widening multiply and a
-// shift (Granlund and Montgomery, "Division by invariant integers using multiplication", PLDI
-// 1994, the round-up method): with l = ceil(log2 d) and m = floor(2^(31 + l) / d) + 1,
-// floor(n / d) = floor(n m / 2^(31 + l)) for every 0 <= n < 2^31; m < 2^32 for d >= 2.
-struct FastDiv {
-    uint32_t d = 1, m = 0, shift = 0;
-    ZL_HD static FastDiv make(uint32_t divisor) {
-        FastDiv f;
-        f.d = divisor;
-        if (divisor <= 1) return f;
-        uint32_t l = 0;
-        while ((1ull << l) < divisor) ++l;
-        f.shift = 31 + l;
-        f.m = (uint32_t)((1ull << f.shift) / divisor + 1);
-        return f;
-    }
-    ZL_HD uint32_t div(uint32_t n) const {
-        return d <= 1 ? n : (uint32_t)(((unsigned long long)n * m) >> shift);
-    }
-};
 
 // Levels whose steps follow one another with no transfer between them are independent: one
 // persistent launch sweeps all their nodes.  Node i of the batch belongs to the level whose

@@ -401,6 +401,8 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     if (cells >= (1ll << 31) - 64)
         return fail(ctx, ZL_EINVAL, "level %d box of %lld cells exceeds 2^31 (split the level)", level, cells);
     geo.stride = (cells + 63) / 64 * 64;
+    geo.fa0 = FastDiv::make((uint32_t)geo.a[0]);
+    geo.fa1 = FastDiv::make((uint32_t)geo.a[1]);
     geo.info = nullptr;
 
     // presence mask; a full box drops it and uses the coordinate-only kernels
@@ -1235,6 +1237,48 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
                 }
         tgt.push_back((int)tc);
         off.push_back((int)src.size());
+    }
+    {
+        // targets grouped by their number of sources (1, 4, 16 or 64 in 3D; a target's sum does
+        // not depend on where it sits in the list): the explosion kernel's warps, which cover
+        // consecutive targets, then loop over equal counts instead of the largest of mixed ones
+        const size_t nt = tgt.size();
+        std::vector<int> perm(nt);
+        for (size_t t = 0; t < nt; ++t) perm[t] = (int)t;
+        std::stable_sort(perm.begin(), perm.end(),
+                         [&](int a, int b) { return off[a + 1] - off[a] < off[b + 1] - off[b]; });
+        std::vector<int> tgt2(nt), off2(1, 0), src2;
+        std::vector<double> wts2;
+        src2.reserve(src.size());
+        wts2.reserve(wts.size());
+        for (size_t t = 0; t < nt; ++t) {
+            const int p = perm[t];
+            tgt2[t] = tgt[p];
+            src2.insert(src2.end(), src.begin() + off[p], src.begin() + off[p + 1]);
+            wts2.insert(wts2.end(), wts.begin() + off[p], wts.begin() + off[p + 1]);
+            off2.push_back((int)src2.size());
+        }
+        tgt.swap(tgt2);
+        off.swap(off2);
+        src.swap(src2);
+        wts.swap(wts2);
+        // source rows grouped by kind (coarse-level sources first, then fine ones): the sources
+        // kernel's warps then take one of its two paths
+        const size_t ns = ucell.size();
+        std::vector<int> row_new(ns), ucell2;
+        std::vector<uint8_t> ufine2;
+        ucell2.reserve(ns);
+        ufine2.reserve(ns);
+        for (int kind = 0; kind < 2; ++kind)
+            for (size_t r = 0; r < ns; ++r)
+                if (ufine[r] == kind) {
+                    row_new[r] = (int)ucell2.size();
+                    ucell2.push_back(ucell[r]);
+                    ufine2.push_back(ufine[r]);
+                }
+        for (int& r : src) r = row_new[r];
+        ucell.swap(ucell2);
+        ufine.swap(ufine2);
     }
     std::vector<int> f2c_c, f2c_f;
     for (int64_t i = 0; i < n_f2c; ++i) {

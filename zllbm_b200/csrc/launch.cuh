@@ -202,13 +202,13 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
                         const int* coarse_cell, const int* fine_cell, int n, const double* fine_macro,           \
                         double tau_ratio, cudaStream_t s) {                                                      \
         if (n <= 0) return cudaSuccess;                                                                          \
-        /* a few thousand targets: one-warp blocks spread them over every SM */                                  \
-        const unsigned blocks = (unsigned)((n + 31) / 32);                                                       \
+        /* one thread per (node, population), 64-thread blocks spread them over every SM */                     \
+        const unsigned blocks = (unsigned)(((long long)n * (dims == 2 ? 9 : 19) + 63) / 64);                     \
         if (dims == 2)                                                                                           \
-            f2c_kernel<D2Q9, S><<<blocks, 32, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
+            f2c_kernel<D2Q9, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
                                                       coarse_cell, fine_cell, n, fine_macro, tau_ratio);         \
         else                                                                                                     \
-            f2c_kernel<D3Q19, S><<<blocks, 32, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,     \
+            f2c_kernel<D3Q19, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,     \
                                                        cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);    \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \

@@ -53,10 +53,9 @@ __device__ __forceinline__ bool code_to_node(uint64_t code, const LevelMap& m, C
 // Node coordinates of a box cell index (inverse of the box indexing, ghost frame removed).
 __device__ __forceinline__ Coord cell_coord(const LevelGeom& geo, int cell) {
     Coord c;
-    const int bx = cell % geo.a[0];
-    const int rest = cell / geo.a[0];
-    const int by = rest % geo.a[1];
-    const int bz = rest / geo.a[1];
+    const uint32_t u = (uint32_t)cell, rest = geo.fa0.div(u), bz = geo.fa1.div(rest);
+    const int bx = (int)(u - rest * (uint32_t)geo.a[0]);
+    const int by = (int)(rest - bz * (uint32_t)geo.a[1]);
     c.x[0] = bx - geo.g[0];
     c.x[1] = by - geo.g[1];
     c.x[2] = bz - geo.g[2];
@@ -391,27 +390,33 @@ __global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even,
                            double tau_ratio) {
     using St = Storage<S>;
     constexpr int Q = L::kQ;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
+    // one thread per (node, population q): a few thousand nodes give the launch Q times the
+    // threads, and each thread has one population load in flight with the node's macros; every
+    // thread of a node forms the same feq (the same operations in the same order) and keeps its q
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= (long long)n * Q) return;
+    const int t = (int)(i / Q), q = (int)(i - (long long)t * Q);
     const Coord cf = cell_coord(fgeo, fine_cell[t]);
     const Coord cc = cell_coord(cgeo, coarse_cell[t]);
     const double* mac = fine_macro + (long long)fine_cell[t] * 4;
     if constexpr (St::kDeviation) {
+        const float v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
         float deq[Q];
         feq_dev<L>((float)mac[0], (float)mac[1], (float)mac[2], (float)mac[3], deq);
+        float e = deq[0];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const float v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
-            St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), deq[q] + (float)tau_ratio * (v - deq[q]), cp);
-        }
+        for (int k = 1; k < Q; ++k)
+            if (k == q) e = deq[k];
+        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + (float)tau_ratio * (v - e), cp);
     } else {
+        const double v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
         double feq[Q];
         feq_exact<L>(mac[0], mac[1], mac[2], mac[3], feq);
+        double e = feq[0];
 #pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const double v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
-            St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), feq[q] + tau_ratio * (v - feq[q]), cp);
-        }
+        for (int k = 1; k < Q; ++k)
+            if (k == q) e = feq[k];
+        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + tau_ratio * (v - e), cp);
     }
 }
 
