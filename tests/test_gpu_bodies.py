@@ -112,3 +112,19 @@ def test_cube_surface_vertices():
     d = np.abs(xyz - centre)
     assert np.all(np.isclose(d.max(1), edge / 2))  # on the surface
     assert area.sum() == pytest.approx(6 * edge * edge, rel=1e-12)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("flow", ["cube", "cylinder"])
+def test_level_streams_are_bit_exact(flow):
+    """The sub-cycled order on per-level streams (immersed-boundary passes beside the transfers of
+    their level) and on one stream give the same vertex forces and level masses bit for bit."""
+    from zllbm_b200 import cube_flow, cylinder_flow
+    mod = cube_flow if flow == "cube" else cylinder_flow
+    topo = os.path.join(HERE, "golden", f"topo_{flow}_small.npz")
+    a = mod.run(topo, steps=6, warmup=2, graph=True, batching=False, streams=True, log=quiet)
+    b = mod.run(topo, steps=6, warmup=2, graph=False, batching=False, streams=False, log=quiet)
+    key = "cube_force_total" if flow == "cube" else "cylinder_force_total_fp64"
+    assert a[key] == b[key]
+    if "mass_per_level" in a:
+        assert a["mass_per_level"] == b["mass_per_level"]

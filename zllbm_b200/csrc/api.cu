@@ -58,6 +58,10 @@ struct Level {
     int n_c2f = 0, n_c2f_src = 0;
     DeviceBuffer f2c_coarse, f2c_fine;
     int n_f2c = 0;
+    // the level's immersed-boundary pass may run beside its transfers (zl_advance on level
+    // streams): no cell its pass reads lies within two cells of one a transfer writes
+    bool ib_concurrent = false;
+    long long ib_concurrent_generation = -1;
     bool has_transfer = false;
     double tau_c2f = 0., tau_f2c = 0.;
     // body forces and immersed boundary
@@ -105,6 +109,7 @@ struct zl_ctx {
     // ordered across streams by the levels each operation touches (created on first use)
     bool level_streams = true;
     cudaStream_t lstream[ZL_MAX_LEVELS] = {};
+    cudaStream_t ibstream[ZL_MAX_LEVELS] = {};  // immersed-boundary passes beside their level's transfers
     static constexpr int kEvents = 64;
     cudaEvent_t events[kEvents] = {};
     int next_event = 0;
@@ -294,6 +299,8 @@ int zl_destroy(zl_ctx* ctx) {
     ctx->scratch_flag.release();
     if (ctx->graph_exec) cudaGraphExecDestroy(ctx->graph_exec);
     for (cudaStream_t& s : ctx->lstream)
+        if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
+    for (cudaStream_t& s : ctx->ibstream)
         if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
     for (cudaEvent_t& e : ctx->events)
         if (e) cudaEventDestroy(e);
@@ -653,11 +660,19 @@ int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, do
 static int ib_pass(zl_ctx* ctx, Level& L, int level);
 static int level_faces(zl_ctx* ctx, Level& L);
 
+static int step_level_body(zl_ctx* ctx, int level, bool with_ib);
+
 int zl_step_level(zl_ctx* ctx, int level) {
     int rc = check_level(ctx, level, true);
     if (rc) return rc;
+    return step_level_body(ctx, level, true);
+}
+
+// The step of a level (its immersed-boundary pass first when with_ib), then its face passes.
+static int step_level_body(zl_ctx* ctx, int level, bool with_ib) {
+    int rc;
     Level& L = ctx->levels[level];
-    if (L.n_vertices > 0 && (rc = ib_pass(ctx, L, level))) return rc;
+    if (with_ib && L.n_vertices > 0 && (rc = ib_pass(ctx, L, level))) return rc;
     const bool odd = L.even_layout == 1;
     if (ctx->cfg.les == ZL_LES_LEARNED && ctx->closure_net.ptr) {
         // the network runs inside the collision of a full periodic D3Q19 box
@@ -808,6 +823,93 @@ static bool batchable(const zl_ctx* ctx) {
     return true;
 }
 
+namespace {
+
+// Box coordinates of a cell (x fastest).
+__device__ __forceinline__ void box_coords(const LevelGeom& geo, int cell, int* b) {
+    const uint32_t u = (uint32_t)cell, rest = geo.fa0.div(u), bz = geo.fa1.div(rest);
+    b[0] = (int)(u - rest * (uint32_t)geo.a[0]);
+    b[1] = (int)(rest - bz * (uint32_t)geo.a[1]);
+    b[2] = (int)bz;
+}
+
+// Mark every cell within Chebyshev distance 2 of the listed cells (periodic axes wrap).
+__global__ void mark_near_kernel(LevelGeom geo, int dims, const int* __restrict__ cells, int n, uint8_t* mark) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    int b[3];
+    box_coords(geo, cells[t], b);
+    const int r2 = dims == 3 ? 2 : 0;
+    for (int dz = -r2; dz <= r2; ++dz)
+        for (int dy = -2; dy <= 2; ++dy)
+            for (int dx = -2; dx <= 2; ++dx) {
+                const int d[3] = {dx, dy, dz};
+                int c[3];
+                bool in = true;
+                for (int a = 0; a < 3; ++a) {
+                    c[a] = b[a] + d[a];
+                    if (geo.periodic[a]) c[a] = c[a] < 0 ? c[a] + geo.a[a] : (c[a] >= geo.a[a] ? c[a] - geo.a[a] : c[a]);
+                    in = in && c[a] >= 0 && c[a] < geo.a[a];
+                }
+                if (in) mark[c[0] + (long long)geo.a[0] * (c[1] + (long long)geo.a[1] * c[2])] = 1;
+            }
+}
+
+__global__ void any_marked_kernel(const int* __restrict__ cells, int n, const uint8_t* __restrict__ mark, int* flag) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n && mark[cells[t]]) atomicExch(flag, 1);
+}
+
+}  // namespace
+
+// Whether each level's immersed-boundary pass may overlap its transfers: the pass reads the
+// populations of its stencil nodes (slots of the node and its neighbours) and writes only forces;
+// the explosion into this level writes its targets (and their neighbours' slots), the coalescence
+// from the next finer level writes coarse nodes of this level.  With every stencil node more than
+// two cells from every such node the two touch disjoint data.  Recomputed after any change of
+// levels, interfaces or vertices (outside graph capture).
+static int refresh_ib_concurrency(zl_ctx* ctx) {
+    int rc;
+    for (int l = 0; l <= ctx->cfg.max_level; ++l) {
+        Level& L = ctx->levels[l];
+        if (L.n_vertices <= 0 || L.n_ib_nodes <= 0) {
+            L.ib_concurrent = false;
+            continue;
+        }
+        if (L.ib_concurrent_generation == ctx->generation) continue;
+        const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
+        DeviceBuffer mark;
+        if ((rc = alloc(ctx, mark, (size_t)cells))) return rc;
+        ZL_CUDA(ctx, cudaMemsetAsync(mark.ptr, 0, (size_t)cells, ctx->stream));
+        mark_near_kernel<<<(L.n_ib_nodes + 127) / 128, 128, 0, ctx->stream>>>(L.geo, ctx->dims, (const int*)L.ib_nodes.ptr,
+                                                                            L.n_ib_nodes, (uint8_t*)mark.ptr);
+        if ((rc = reset_flag(ctx))) return rc;
+        if (l >= 1 && L.has_transfer && L.n_c2f > 0)
+            any_marked_kernel<<<(L.n_c2f + 127) / 128, 128, 0, ctx->stream>>>(
+                (const int*)L.c2f_target.ptr, L.n_c2f, (const uint8_t*)mark.ptr, (int*)ctx->scratch_flag.ptr);
+        if (l < ctx->cfg.max_level && ctx->levels[l + 1].has_transfer && ctx->levels[l + 1].n_f2c > 0) {
+            const Level& F = ctx->levels[l + 1];
+            any_marked_kernel<<<(F.n_f2c + 127) / 128, 128, 0, ctx->stream>>>(
+                (const int*)F.f2c_coarse.ptr, F.n_f2c, (const uint8_t*)mark.ptr, (int*)ctx->scratch_flag.ptr);
+        }
+        ZL_CUDA(ctx, cudaGetLastError());
+        int hit = 0;
+        if ((rc = read_flag(ctx, &hit))) return rc;
+        L.ib_concurrent = hit == 0;
+        L.ib_concurrent_generation = ctx->generation;
+    }
+    return ZL_OK;
+}
+
+static int cuda_wait(zl_ctx* ctx, cudaStream_t s, cudaEvent_t e) {
+    ZL_CUDA(ctx, cudaStreamWaitEvent(s, e, 0));
+    return ZL_OK;
+}
+static int cuda_record(zl_ctx* ctx, cudaEvent_t e, cudaStream_t s) {
+    ZL_CUDA(ctx, cudaEventRecord(e, s));
+    return ZL_OK;
+}
+
 // Level streams of zl_advance: one stream per level (finer levels at higher priority: their chains
 // of short launches are the critical path), created on first use, and a pool of events.
 static int ensure_level_streams(zl_ctx* ctx) {
@@ -817,6 +919,7 @@ static int ensure_level_streams(zl_ctx* ctx) {
     for (int l = 0; l <= ctx->cfg.max_level; ++l) {
         const int prio = least - l < greatest ? greatest : least - l;
         ZL_CUDA(ctx, cudaStreamCreateWithPriority(&ctx->lstream[l], cudaStreamNonBlocking, prio));
+        ZL_CUDA(ctx, cudaStreamCreateWithPriority(&ctx->ibstream[l], cudaStreamNonBlocking, prio));
     }
     for (cudaEvent_t& e : ctx->events) ZL_CUDA(ctx, cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
     return ZL_OK;
@@ -839,21 +942,26 @@ static int advance_streams(zl_ctx* ctx, int steps, const std::vector<int>& order
         ctx->next_event = (ctx->next_event + 1) % zl_ctx::kEvents;
         return e;
     };
-    cudaEvent_t last[ZL_MAX_LEVELS];
-    cudaStream_t last_stream[ZL_MAX_LEVELS];
+    cudaEvent_t last[ZL_MAX_LEVELS], last_step[ZL_MAX_LEVELS];
+    cudaStream_t last_stream[ZL_MAX_LEVELS], last_step_stream[ZL_MAX_LEVELS];
+    // streams that joined this call's work (and, under capture, the capture): only they rejoin
+    bool lused[ZL_MAX_LEVELS] = {}, ibused[ZL_MAX_LEVELS] = {};
     {
         const cudaEvent_t fork = next_event();
         ZL_CUDA(ctx, cudaEventRecord(fork, main));
         for (int l = 0; l < nl; ++l) {
-            last[l] = fork;
-            last_stream[l] = main;
+            last[l] = last_step[l] = fork;
+            last_stream[l] = last_step_stream[l] = main;
         }
     }
-    // run op on the stream of level `home` after the last operations on levels lo .. hi
-    auto run = [&](int home, int lo, int hi, auto op) -> int {
+    // run op on the stream of level `home` after the last operations on levels lo .. hi (and
+    // after `also`, when given)
+    auto run = [&](int home, int lo, int hi, auto op, cudaEvent_t also = nullptr) -> int {
         const cudaStream_t s = ctx->lstream[home];
+        lused[home] = true;
         for (int l = lo; l <= hi; ++l)
             if (last_stream[l] != s) ZL_CUDA(ctx, cudaStreamWaitEvent(s, last[l], 0));
+        if (also) ZL_CUDA(ctx, cudaStreamWaitEvent(s, also, 0));
         ctx->stream = s;
         const int r = op();
         ctx->stream = main;
@@ -873,7 +981,25 @@ static int advance_streams(zl_ctx* ctx, int steps, const std::vector<int>& order
             if (ctx->temporal && l > 0 && count[l] % 2 == 0 &&
                 (rc = run(l, l - 1, l, [&] { return interpolate_interface(ctx, l, false); })))
                 break;
-            if ((rc = run(l, l, l, [&] { return zl_step_level(ctx, l); }))) break;
+            Level& L = ctx->levels[l];
+            if (L.ib_concurrent && L.n_vertices > 0) {
+                // the immersed-boundary pass on its own stream after the level's last step only,
+                // beside the level's transfer; the step waits for both
+                const cudaStream_t s = ctx->ibstream[l];
+                ibused[l] = true;
+                if (last_step_stream[l] != s && (rc = cuda_wait(ctx, s, last_step[l]))) break;
+                ctx->stream = s;
+                rc = ib_pass(ctx, L, l);
+                ctx->stream = main;
+                if (rc) break;
+                const cudaEvent_t ib_done = next_event();
+                if ((rc = cuda_record(ctx, ib_done, s))) break;
+                if ((rc = run(l, l, l, [&] { return step_level_body(ctx, l, false); }, ib_done))) break;
+            } else if ((rc = run(l, l, l, [&] { return zl_step_level(ctx, l); }))) {
+                break;
+            }
+            last_step[l] = last[l];
+            last_step_stream[l] = last_stream[l];
             // InformationFromGridOfDifferentLevel (lbm_solver_interface.cpp:224-238)
             if (l > 0 && count[l] % 2 == 0 && (rc = run(l, l - 1, l, [&] { return zl_transfer_levels(ctx, l); })))
                 break;
@@ -881,11 +1007,13 @@ static int advance_streams(zl_ctx* ctx, int steps, const std::vector<int>& order
     }
     // join every level stream back into the caller's stream (also on failure, so that a capture
     // in progress can end)
-    for (int l = 0; l < nl; ++l) {
-        const cudaEvent_t e = next_event();
-        ZL_CUDA(ctx, cudaEventRecord(e, ctx->lstream[l]));
-        ZL_CUDA(ctx, cudaStreamWaitEvent(main, e, 0));
-    }
+    for (int l = 0; l < nl; ++l)
+        for (int k = 0; k < 2; ++k) {
+            if (!(k ? ibused[l] : lused[l])) continue;
+            const cudaEvent_t e = next_event();
+            ZL_CUDA(ctx, cudaEventRecord(e, k ? ctx->ibstream[l] : ctx->lstream[l]));
+            ZL_CUDA(ctx, cudaStreamWaitEvent(main, e, 0));
+        }
     return rc;
 }
 
@@ -943,6 +1071,10 @@ int zl_advance(zl_ctx* ctx, int steps) {
                 const int rc = interpolate_interface(ctx, l, true);
                 if (rc) return rc;
             }
+    if (ctx->level_streams && ctx->cfg.max_level > 0) {
+        const int rc = refresh_ib_concurrency(ctx);
+        if (rc) return rc;
+    }
     // a closure evaluated every k-th step repeats with period k, not with the graph's two steps
     const bool periodic_closure = ctx->cfg.les == ZL_LES_LEARNED && ctx->closure_net.ptr && ctx->closure_every > 1;
     if (!ctx->use_graph || steps < 2 || periodic_closure) return advance_direct(ctx, steps, order);
