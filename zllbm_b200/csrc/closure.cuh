@@ -62,10 +62,17 @@ __device__ __forceinline__ float gelu(float z, float& t) {
 // Inference: the same GELU on packed BF16 pairs (the result is a BF16 operand anyway):
 // z^2, 1 + a z^2, k z, k z (1 + a z^2), tanh.approx.bf16x2, z/2, z/2 + z/2 t -- every step rounds to
 // BF16 (constants a, k rounded to BF16 too).
+// The constants are BF16 bit patterns (a = 0x3d37, k = 0x3f4c, 1 = 0x3f80, 1/2 = 0x3f00, each in
+// both halves), so that no conversion runs per call.
+__device__ __forceinline__ __nv_bfloat162 bf16x2_bits(uint32_t b) {
+    __nv_bfloat162 v;
+    memcpy(&v, &b, 4);
+    return v;
+}
 __device__ __forceinline__ uint32_t gelu_bf16x2(float z0, float z1) {
     const __nv_bfloat162 z = __floats2bfloat162_rn(z0, z1);
-    const __nv_bfloat162 a = __float2bfloat162_rn(kGeluA), k = __float2bfloat162_rn(kGeluK),
-                         one = __float2bfloat162_rn(1.f), half = __float2bfloat162_rn(0.5f);
+    const __nv_bfloat162 a = bf16x2_bits(0x3d373d37u), k = bf16x2_bits(0x3f4c3f4cu), one = bf16x2_bits(0x3f803f80u),
+                         half = bf16x2_bits(0x3f003f00u);
     const __nv_bfloat162 p = __hfma2(__hmul2(z, z), a, one);
     const __nv_bfloat162 arg = __hmul2(__hmul2(z, k), p);
     uint32_t t;
@@ -109,10 +116,13 @@ __device__ __forceinline__ void stage_weights(const float* __restrict__ net, uin
     st_row_chunk(a1s, tid, 72, kSboA1, v);
 }
 
+// One warp polls the MMA's mbarrier; the others wait at the block barrier, which issues nothing
+// while it waits (polling from every warp takes issue slots from the other resident blocks).
 __device__ __forceinline__ bool wait_mma(uint64_t* bar, uint32_t& phase, int* err) {
-    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    if (ok) phase ^= 1u;
+    bool ok = true;
+    if (threadIdx.x < 32) ok = tc::mbar_wait(bar, phase, kWaitLimit);
     const bool failed = __syncthreads_or(!ok) != 0;
+    if (!failed) phase ^= 1u;
     if (failed && threadIdx.x == 0) atomicExch(err, 1);
     tc::fence_after_sync();
     return !failed;
@@ -174,11 +184,16 @@ __device__ __forceinline__ bool infer_tile(const InferTile& it, uint32_t& phase,
         float v[16];
         tc::tmem_ld16(it.tmem + it.lane_addr + 16 * c, v);
 #pragma unroll
-        for (int i = 0; i < 16; i += 2) {
-            const uint32_t g = gelu_bf16x2(v[i], v[i + 1]);
-            const float2 a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&g));
-            acc = fmaf(a.x, it.w3[16 * c + i], acc);
-            acc = fmaf(a.y, it.w3[16 * c + i + 1], acc);
+        for (int i = 0; i < 16; i += 4) {
+            // w3 four at a time (one 128-bit shared load, the same address for every thread)
+            const float4 w = *reinterpret_cast<const float4*>(it.w3 + 16 * c + i);
+            const uint32_t g0 = gelu_bf16x2(v[i], v[i + 1]), g1 = gelu_bf16x2(v[i + 2], v[i + 3]);
+            const float2 a0 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&g0));
+            const float2 a1 = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&g1));
+            acc = fmaf(a0.x, w.x, acc);
+            acc = fmaf(a0.y, w.y, acc);
+            acc = fmaf(a1.x, w.z, acc);
+            acc = fmaf(a1.y, w.w, acc);
         }
     }
     y = acc;
