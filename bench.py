@@ -336,7 +336,7 @@ def multilevel_block(steps: int, warmup: int, peak: float):
     """The multi-level configurations on the reference-built grids (packed under
     zllbm_b200/topologies/): the cube flow (D3Q19 SRT + Smagorinsky + immersed-boundary cube,
     levels 0..2) and the cylinder flow (D2Q9 MRT + immersed-boundary cylinder, levels 0..3), FP32,
-    batched level steps replayed from a CUDA graph.  MLUPS count every node update of every level
+    per-level streams replayed from a CUDA graph.  MLUPS count every node update of every level
     (nodes x 2^level per coarse step); the HBM figure is those updates' algorithmic bytes
     (2 Q sizeof(float) each) over the event time."""
     from zllbm_b200 import cube_flow, cylinder_flow
