@@ -162,6 +162,15 @@ int zl_get_macros(zl_ctx* ctx, int level, const uint64_t* codes, double* rho, do
    for a level without coarse/fine neighbours. */
 int zl_step_level(zl_ctx* ctx, int level);
 
+/* Part of a time step of a D3Q19 level: the node updates of planes [first, first + count) of its
+   last axis, with the level's current step parity; finish != 0 then completes the step (the next
+   call steps the other parity).  Every plane once per step, in any split and order, gives the
+   whole step's result bit for bit (the single-buffer AA update of a node touches only its own
+   slot set).  A sharded slab steps its interior planes while its halo planes are in flight and its
+   boundary planes after they arrive.  For levels without ordered face passes, immersed boundary or
+   learned closure; no reference counterpart (the reference updates a level in one pass). */
+int zl_step_level_planes(zl_ctx* ctx, int level, int first, int count, int finish);
+
 /* Coarse/fine interface of refinement level `level` (>= 1) with level - 1, from the reference's
    interface layer maps (InterfaceLayerInfo, amr_project/grid/grid_info_interface.h:117-127):
      c2f_fine        fine nodes of the fine-to-coarse layers 1..2 of `level` (vec_{inner,outer}_

@@ -202,3 +202,60 @@ def test_open_chain_slab_refuses_full_box_kernels():
             s.ctx.set_block(0, -64, 1)
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("world", [1, 2, 3])
+@pytest.mark.parametrize("kernel,storage", [("scalar", 0), ("scalar", 1), ("pair", 1), ("row", 2)])
+def test_overlapped_schedule_equals_plain(kernel, storage, world):
+    """The overlapped schedule (interior planes stepped before the halo of the previous step is
+    unpacked, zl_step_level_planes) equals the plain schedule bit for bit, on every step kernel."""
+    import zllbm_b200 as zl
+    from zllbm_b200.shard import DeviceSlab, LocalRing, Ring, slab_range, split_planes
+    n = (128, 8, 21)
+    cfg = zl.SolverConfig(lattice=zl.D3Q19, collision=zl.MRT, storage=storage, viscosity=0.02, rho0=1.0,
+                          bc_kind=(zl.BC_PERIODIC,) * 6, domain_min=(1, 1, 1), domain_max=tuple(1 + v for v in n),
+                          storage_rounding=zl.ROUND_NEAREST)
+    block = {"scalar": None, "pair": (-64, 1), "row": (zl.BLOCK_ROW, 4)}[kernel]
+    glo, gn = _box(cfg)
+    gcodes = _codes(3, glo, gn)
+    f0 = _populations(cfg, gcodes)
+    idx = dict(zip(gcodes.tolist(), range(gcodes.size)))
+    out = []
+    for overlap in (False, True):
+        slabs = []
+        try:
+            for r in range(world):
+                slabs.append(DeviceSlab(cfg, *slab_range(split_planes(cfg), r, world), Ring(r, world, True)))
+            for s in slabs:
+                codes = _codes(3, s.box_lo, s.box_n)
+                s.ctx.set_populations(0, codes, f0[[idx[c] for c in codes.tolist()]])
+                if block:
+                    s.ctx.set_block(0, *block)
+            ring = LocalRing(slabs, True, slabs[0].faces, overlap=overlap)
+            assert ring.overlap == overlap
+            for _ in range(4):
+                ring.step_pair()
+            ring.flush()
+            out.append([s.ctx.get_populations(0, _codes(3, s.box_lo, s.box_n)) for s in slabs])
+        finally:
+            for s in slabs:
+                s.close()
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+
+
+def test_plane_steps_refused_where_they_do_not_apply():
+    import zllbm_b200 as zl
+    cfg = _config(2, 1, True, zl.MRT)
+    lo, n = _box(cfg)
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, lo + (0,), n + (1,))
+        with pytest.raises(zl.ZlError):
+            ctx.step_level_planes(0, 0, 1, True)  # D2Q9
+    cfg = _config(3, 1, True, zl.MRT)
+    lo, n = _box(cfg)
+    with zl.Context(cfg) as ctx:
+        ctx.set_level_box(0, lo, n)
+        with pytest.raises(zl.ZlError):
+            ctx.step_level_planes(0, n[2] - 1, 2, True)  # past the last plane
+        ctx.step_level_planes(0, 0, n[2], True)  # a whole step in one call

@@ -5,6 +5,8 @@ through the sharding schedule
 * over gloo ranks (world size 2, where both neighbours are one peer, and 3, ragged slabs), in a
   periodic ring and in an open chain;
 * in one process (LocalRing) and as a one-rank periodic ring exchanging with itself;
+* with the overlapped schedule (interior planes stepped while the halo is in flight, the rest
+  after it arrives) as well as the plain one;
 
 and compared bit for bit with the global lattice stepped by plain collide-and-stream (two
 buffers, periodic or open ends where a missing upstream node leaves the stale value, the rule of
@@ -25,6 +27,7 @@ Q = len(C)
 OPP = np.array([int(np.where((C == -c).all(1))[0][0]) for c in C])
 W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)
 SHAPE = (6, 5, 11)  # x, y, z nodes of the global lattice; z is split
+SHAPE_OVERLAP = (6, 5, 21)  # at least five planes per slab for up to four slabs
 TAU = 0.8
 STEPS = 6
 
@@ -42,10 +45,10 @@ def collide(f):
     return out
 
 
-def initial(seed=3):
+def initial(seed=3, shape=SHAPE):
     """Populations f[q, z, y, x] near rest with a seeded perturbation."""
     rng = np.random.default_rng(seed)
-    nx, ny, nz = SHAPE
+    nx, ny, nz = shape
     return W[:, None, None, None] * (1 + 0.05 * rng.standard_normal((Q, nz, ny, nx)))
 
 
@@ -91,35 +94,48 @@ class HostSlab:
             return [self.n]
         return []
 
+    @property
+    def n_planes(self):
+        return self.n
+
     def step(self):
-        F, n = self.F, self.n
+        self.step_planes(0, self.n, True)
+
+    def step_planes(self, first, count, finish):
+        """The node updates of planes [first, first + count) with the current parity (slot z = 1 +
+        plane); finish flips the parity.  Each node reads and writes only its own slot set."""
+        F = self.F
+        a, b = first + 1, first + count + 1  # slot range of the planes
         cx, cy, cz = C[:, 0], C[:, 1], C[:, 2]
-        if not self.odd:
-            pre = F[:, 1:-1].copy()
+        if count > 0 and not self.odd:
+            pre = F[:, a:b].copy()
             post = collide(pre)
             for q in range(Q):
-                F[OPP[q], 1:-1] = post[q]
+                F[OPP[q], a:b] = post[q]
             for q in range(1, Q):
                 for z in self._missing(q):  # stale value into the slot of the missing upstream cell
-                    F[OPP[q], z - cz[q]] = np.roll(pre[q, z - 1], (-cy[q], -cx[q]), axis=(0, 1))
-        else:
-            pre = np.empty((Q, n) + F.shape[2:])
+                    if a <= z < b:
+                        F[OPP[q], z - cz[q]] = np.roll(pre[q, z - a], (-cy[q], -cx[q]), axis=(0, 1))
+        elif count > 0:
+            pre = np.empty((Q, count) + F.shape[2:])
             for q in range(Q):
                 if q == 0:
-                    pre[q] = F[0, 1:-1]
+                    pre[q] = F[0, a:b]
                 else:  # f(x, q) in slot (x - c_q, opp q)
-                    src = F[OPP[q], 1 - cz[q]:n + 1 - cz[q]]
+                    src = F[OPP[q], a - cz[q]:b - cz[q]]
                     pre[q] = np.roll(src, (cy[q], cx[q]), axis=(1, 2))
             post = collide(pre)
             for q in range(Q):
                 if q == 0:
-                    F[0, 1:-1] = post[0]
+                    F[0, a:b] = post[0]
                 else:  # f*(x, q) into slot (x + c_q, q)
-                    F[q, 1 + cz[q]:n + 1 + cz[q]] = np.roll(post[q], (cy[q], cx[q]), axis=(1, 2))
+                    F[q, a + cz[q]:b + cz[q]] = np.roll(post[q], (cy[q], cx[q]), axis=(1, 2))
             for q in range(1, Q):
                 for z in self._missing(q):
-                    F[q, z] = pre[q, z - 1]
-        self.odd = not self.odd
+                    if a <= z < b:
+                        F[q, z] = pre[q, z - a]
+        if finish:
+            self.odd = not self.odd
 
     # the halo rule of zl_halo_pack / zl_halo_unpack
     def _planes(self, face, inward):
@@ -146,8 +162,8 @@ class HostSlab:
         return self.F[:, 1:-1].copy()
 
 
-def _reference(periodic):
-    return two_buffer(initial(), STEPS, periodic)
+def _reference(periodic, shape=SHAPE):
+    return two_buffer(initial(shape=shape), STEPS, periodic)
 
 
 def test_slab_range_covers_every_plane_once():
@@ -162,21 +178,24 @@ def test_slab_range_covers_every_plane_once():
         slab_range(3, 0, 4)
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("world", [1, 2, 3, 4])
-def test_local_ring_matches_global_lattice(world, periodic):
+def test_local_ring_matches_global_lattice(world, periodic, overlap):
     from zllbm_b200.shard import LocalRing, Ring, slab_range
-    f0 = initial()
-    nz = SHAPE[2]
+    shape = SHAPE_OVERLAP if overlap else SHAPE
+    f0 = initial(shape=shape)
     slabs = []
     for r in range(world):
-        lo, hi = slab_range(nz, r, world)
+        lo, hi = slab_range(shape[2], r, world)
         slabs.append(HostSlab(f0, lo, hi, Ring(r, world, periodic).halo_faces))
-    ring = LocalRing(slabs, periodic, (4, 5))
+    ring = LocalRing(slabs, periodic, (4, 5), overlap=overlap)
+    assert ring.overlap == overlap
     for _ in range(STEPS // 2):
         ring.step_pair()
+    ring.flush()
     got = np.concatenate([s.populations() for s in slabs], axis=1)
-    assert np.array_equal(got, _reference(periodic))
+    assert np.array_equal(got, _reference(periodic, shape))
 
 
 def _free_port() -> int:
@@ -185,47 +204,52 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _rank(rank, world, port, periodic, out):
+def _rank(rank, world, port, periodic, overlap, out):
     import sys
 
     import torch.distributed as dist
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
-    from test_shard_gloo import HostSlab, initial
+    from test_shard_gloo import SHAPE, SHAPE_OVERLAP, HostSlab, initial
     from zllbm_b200.shard import Ring, SlabSchedule, slab_range, torch_exchange
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
-        lo, hi = slab_range(SHAPE[2], rank, world)
+        shape = SHAPE_OVERLAP if overlap else SHAPE
+        lo, hi = slab_range(shape[2], rank, world)
         ring = Ring(rank, world, periodic)
-        slab = HostSlab(initial(), lo, hi, ring.halo_faces)
-        sched = SlabSchedule(slab, ring, (4, 5), torch_exchange(dist))
+        slab = HostSlab(initial(shape=shape), lo, hi, ring.halo_faces)
+        sched = SlabSchedule(slab, ring, (4, 5), torch_exchange(dist), overlap=overlap)
+        assert sched.overlap == overlap
         for _ in range(STEPS // 2):
             sched.step_pair()
+        sched.flush()
         out.put((rank, lo, hi, slab.populations()))
     finally:
         dist.destroy_process_group()
 
 
+@pytest.mark.parametrize("overlap", [False, True])
 @pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_match_global_lattice(world, periodic):
+def test_gloo_ranks_match_global_lattice(world, periodic, overlap):
     port = _free_port()
     ctx = mp.get_context("spawn")
     out = ctx.Queue()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, periodic, out)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, periodic, overlap, out)) for r in range(world)]
     for p in procs:
         p.start()
     results = sorted((out.get(timeout=180) for _ in range(world)), key=lambda t: t[0])
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    ref = _reference(periodic)
+    ref = _reference(periodic, SHAPE_OVERLAP if overlap else SHAPE)
     for rank, lo, hi, f in results:
         assert np.array_equal(f, ref[:, lo:hi]), rank
 
 
-def test_one_rank_ring_exchanges_with_itself():
+@pytest.mark.parametrize("overlap", [False, True])
+def test_one_rank_ring_exchanges_with_itself(overlap):
     """A periodic ring of one rank: its high face's buffers wrap onto its own low face."""
     from zllbm_b200.shard import Ring, SlabSchedule
 
@@ -236,8 +260,10 @@ def test_one_rank_ring_exchanges_with_itself():
 
     from zllbm_b200.shard import torch_exchange
     ring = Ring(0, 1, True)
-    slab = HostSlab(initial(), 0, SHAPE[2], ring.halo_faces)
-    sched = SlabSchedule(slab, ring, (4, 5), torch_exchange(Dist))
+    shape = SHAPE_OVERLAP if overlap else SHAPE
+    slab = HostSlab(initial(shape=shape), 0, shape[2], ring.halo_faces)
+    sched = SlabSchedule(slab, ring, (4, 5), torch_exchange(Dist), overlap=overlap)
     for _ in range(STEPS // 2):
         sched.step_pair()
-    assert np.array_equal(slab.populations(), _reference(True))
+    sched.flush()
+    assert np.array_equal(slab.populations(), _reference(True, shape))

@@ -120,11 +120,13 @@ def load_library(path: str = LIB_PATH) -> ctypes.CDLL:
         "zl_get_populations": ([P, ctypes.c_int, u64p, dp, i64], ctypes.c_int),
         "zl_get_macros": ([P, ctypes.c_int, u64p, dp, dp, i64], ctypes.c_int),
         "zl_step_level": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_step_level_planes": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "zl_advance": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_level_interface": ([P, ctypes.c_int, u64p, i64, u64p, i64, u64p, i64], ctypes.c_int),
         "zl_transfer_levels": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_graph": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_batching": ([P, ctypes.c_int], ctypes.c_int),
+        "zl_set_level_streams": ([P, ctypes.c_int], ctypes.c_int),
         "zl_set_block": ([P, ctypes.c_int, ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "zl_write_checkpoint_nodes": ([P, ctypes.c_char_p, ctypes.POINTER(u64p),
                                        ctypes.POINTER(ctypes.POINTER(ctypes.c_int32)), ctypes.POINTER(i64)],
@@ -403,6 +405,10 @@ class Context:
 
     def step_level(self, level: int = 0):
         self._check(self.lib.zl_step_level(self.handle, level))
+
+    def step_level_planes(self, level: int, first: int, count: int, finish: bool):
+        """Planes [first, first + count) of the level's last axis; finish completes the step."""
+        self._check(self.lib.zl_step_level_planes(self.handle, level, first, count, 1 if finish else 0))
 
     def advance(self, steps: int):
         self._check(self.lib.zl_advance(self.handle, steps))

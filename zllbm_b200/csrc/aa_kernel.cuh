@@ -74,6 +74,8 @@ struct LevelGeom {
     // kernels of full periodic boxes apply with z addressed through the ghost frame
     int ring;
     FastDiv fa0, fa1;  // division by a[0] and a[1] (cell index -> box coordinates)
+    // D3Q19 step launches: planes [z0, z0 + zn) of the last axis; zn = 0: every plane
+    int z0, zn;
 };
 
 struct StepParams {
@@ -1259,7 +1261,7 @@ __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>:
     Coord c;
     c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
     c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
-    c.x[2] = blockIdx.z;
+    c.x[2] = blockIdx.z + geo.z0;
     if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (c.x[0] >= geo.n[0] || c.x[1] >= geo.n[1]) return;

@@ -706,6 +706,31 @@ static int step_level_body(zl_ctx* ctx, int level, bool with_ib) {
     return ZL_OK;
 }
 
+int zl_step_level_planes(zl_ctx* ctx, int level, int first, int count, int finish) {
+    int rc = check_level(ctx, level, true);
+    if (rc) return rc;
+    Level& L = ctx->levels[level];
+    if (ctx->dims != 3 || L.ordered || L.n_vertices > 0 || ctx->cfg.les == ZL_LES_LEARNED)
+        return fail(ctx, ZL_EINVAL,
+                    "plane-range steps need a D3Q19 level without ordered face passes, immersed boundary "
+                    "or learned closure");
+    if (first < 0 || count < 0 || first + count > L.geo.n[2])
+        return fail(ctx, ZL_EINVAL, "planes [%d, %d) outside the level's %d", first, first + count, L.geo.n[2]);
+    if (count > 0) {
+        LevelGeom g = L.geo;
+        g.z0 = first;
+        g.zn = count;
+        ZL_CUDA(ctx, ctx->ops->step(ctx->dims, ctx->cfg.collision, L.even_layout == 1, L.bnd, L.geo.info != nullptr,
+                                    L.f.ptr, g, L.params, ctx->stream));
+    }
+    if (finish) {
+        L.even_layout ^= 1;
+        if ((rc = level_faces(ctx, L))) return rc;
+        ++L.steps;
+    }
+    return ZL_OK;
+}
+
 // Domain faces after a level's step, in the reference's order xmin, ymin, zmin, xmax, ymax, zmax
 // (lbm_grid_interface.cpp:225-314); bounce back is fused into the step kernel unless the level
 // needs every face as an ordered pass.

@@ -59,7 +59,7 @@ inline void step_shape(const LevelGeom& geo, int dims, dim3& grid, dim3& block) 
         by = 1;
     }
     block = dim3(bx, by, 1);
-    grid = dim3((nx + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? geo.n[2] : 1);
+    grid = dim3((nx + bx - 1) / bx, (geo.n[1] + by - 1) / by, dims == 3 ? (geo.zn > 0 ? geo.zn : geo.n[2]) : 1);
 }
 
 // The two-nodes-per-thread kernel applies to full periodic D3Q19 boxes (or slabs of one, geo.ring)

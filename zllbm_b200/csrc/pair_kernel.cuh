@@ -158,7 +158,7 @@ __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, Leve
     using St = Storage<S>;
     using IO = PairIO<S>;
     const int x0 = 2 * (blockIdx.x * blockDim.x + threadIdx.x);
-    const int y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z + geo.z0;
     if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (x0 >= geo.n[0] || y >= geo.n[1]) return;

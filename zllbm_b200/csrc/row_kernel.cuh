@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, Level
     constexpr int K = V / 2;
     const int lane = threadIdx.x & 31;
     const int y = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    const int z = blockIdx.y;
+    const int z = blockIdx.y + geo.z0;
     if ((blockIdx.x | blockIdx.y | threadIdx.x) == 0) sr_advance(p, Odd, sr_seed(p, Odd), true);
     if (y >= geo.n[1]) return;  // whole warp: every shuffle below has all 32 lanes
     const int n1 = geo.n[1], n2 = geo.n[2];

@@ -40,7 +40,7 @@ cudaError_t step_row(S* f, const LevelGeom& geo, const StepParams& p, cudaStream
         const int v = row_kernel_width(geo);
         const int rows = geo.block[1];
         if (v == 0 || rows < 1 || rows > 4) return cudaErrorInvalidValue;
-        const dim3 b(32 * rows), g((geo.n[1] + rows - 1) / rows, geo.n[2]);
+        const dim3 b(32 * rows), g((geo.n[1] + rows - 1) / rows, geo.zn > 0 ? geo.zn : geo.n[2]);
         if (v == 8) aa_row_kernel<S, C, O, 8><<<g, b, 0, s>>>(f, geo, p);
         else aa_row_kernel<S, C, O, 4><<<g, b, 0, s>>>(f, geo, p);
         return cudaGetLastError();

@@ -18,6 +18,20 @@ stage)`` and ``unpack(face, stage, buf)`` and any ``exchange(sends) -> recvs``: 
 library context on this rank's GPU) with ``torch_exchange`` (NCCL point-to-point), or host models
 over gloo in the CPU tests.  ``LocalRing`` runs the same schedule for several slabs held by one
 process (several contexts on one GPU), routing the buffers directly.
+
+With ``overlap`` (slabs with ``step_planes``, at least five planes) a step's exchange is left in
+flight while the next step updates the planes that do not need it, and completed before the rest:
+
+* even step: planes [2, n - 2) first (they read only slots the previous odd step's planes
+  [1, n - 1) wrote), then the stage-1 halo of the previous step is unpacked, then planes 0, 1,
+  n - 2, n - 1 (which read the unpacked boundary slots or the slots of the boundary planes'
+  previous odd update), then the stage-0 halo is packed and posted;
+* odd step: planes [1, n - 1) first (no ghost plane is read or written there), then the stage-0
+  halo is unpacked, then planes 0 and n - 1, then the stage-1 halo is packed and posted.
+
+Every plane is updated exactly once per step and no update reads a slot that a later part of the
+same step writes, so the result equals the unsplit schedule bit for bit; ``flush()`` completes the
+last exchange (before reading the populations).
 """
 from __future__ import annotations
 
@@ -65,12 +79,14 @@ class SlabSchedule:
     `exchange(sends)` takes {peer: [buffers]} and returns {peer: [buffers]}: what each peer sent
     to this rank, in the order the peer listed them."""
 
-    def __init__(self, slab, ring: Ring, faces: tuple[int, int], exchange):
+    def __init__(self, slab, ring: Ring, faces: tuple[int, int], exchange, overlap: bool = False):
         self.slab = slab
         self.ring = ring
         self.lo_face, self.hi_face = faces
         self.exchange = exchange
         self.steps = 0
+        self.overlap = overlap and plane_split_ok(slab)
+        self.pending = None  # (stage, in-flight exchange) of the last step, overlap only
 
     def sends(self, stage: int) -> dict:
         """{peer: [buffers]}: the high face's buffer first (to the rank above), then the low face's."""
@@ -95,25 +111,55 @@ class SlabSchedule:
     def step(self):
         """One time step and its exchange (stage 0 after an even step, stage 1 after an odd one)."""
         stage = self.steps & 1
-        self.slab.step()
+        if not self.overlap:
+            self.slab.step()
+            self.steps += 1
+            self.swap(stage)
+            return
+        inner, edges = plane_split(self.slab.n_planes, stage)
+        self.slab.step_planes(*inner, False)
+        self.flush()
+        for k, (first, count) in enumerate(edges):
+            self.slab.step_planes(first, count, k == len(edges) - 1)
         self.steps += 1
-        self.swap(stage)
+        self.pending = (stage, self.exchange.start(self.sends(stage)))
+
+    def flush(self):
+        """Complete the exchange still in flight (overlap only)."""
+        if self.pending is not None:
+            stage, handle = self.pending
+            self.pending = None
+            self.receive(stage, handle.wait())
 
     def step_pair(self):
         self.step()
         self.step()
 
 
+def plane_split_ok(slab) -> bool:
+    return hasattr(slab, "step_planes") and getattr(slab, "n_planes", 0) >= 5
+
+
+def plane_split(n: int, stage: int):
+    """((first, count) of the planes that do not wait for the exchange, [(first, count)] of the
+    planes that do) for a step of parity `stage` on a slab of n planes."""
+    if stage == 0:
+        return (2, n - 4), [(0, 2), (n - 2, 2)]
+    return (1, n - 2), [(0, 1), (n - 1, 1)]
+
+
 class LocalRing:
     """The slab schedule for all ranks of a ring held by one process: every slab steps, packs,
-    and unpacks what its neighbours packed (no collective; e.g. several contexts on one GPU)."""
+    and unpacks what its neighbours packed (no collective; e.g. several contexts on one GPU).
+    With overlap, the phases of the overlapped schedule run slab by slab in the same order."""
 
-    def __init__(self, slabs, periodic: bool, faces: tuple[int, int]):
+    def __init__(self, slabs, periodic: bool, faces: tuple[int, int], overlap: bool = False):
         world = len(slabs)
         self.scheds = [SlabSchedule(s, Ring(r, world, periodic), faces, None) for r, s in enumerate(slabs)]
+        self.overlap = overlap and all(plane_split_ok(s) for s in slabs)
+        self.pending = None  # (stage, sends of every slab)
 
-    def _swap(self, stage: int):
-        sends = [s.sends(stage) for s in self.scheds]
+    def _route(self, stage: int, sends):
         for r, s in enumerate(self.scheds):
             recvs = {peer: sends[peer][r] for peer in range(len(sends)) if r in sends[peer]}
             s.receive(stage, recvs)
@@ -121,24 +167,57 @@ class LocalRing:
     def step(self):
         """One time step of every slab (an even step swaps stage 0 after it, an odd one stage 1)."""
         stage = self.scheds[0].steps & 1
-        for s in self.scheds:
-            s.slab.step()
+        if not self.overlap:
+            for s in self.scheds:
+                s.slab.step()
+                s.steps += 1
+            self._route(stage, [s.sends(stage) for s in self.scheds])
+            return
+        splits = [plane_split(s.slab.n_planes, stage) for s in self.scheds]
+        for s, (inner, _) in zip(self.scheds, splits):
+            s.slab.step_planes(*inner, False)
+        self.flush()
+        for s, (_, edges) in zip(self.scheds, splits):
+            for k, (first, count) in enumerate(edges):
+                s.slab.step_planes(first, count, k == len(edges) - 1)
             s.steps += 1
-        self._swap(stage)
+        self.pending = (stage, [s.sends(stage) for s in self.scheds])
+
+    def flush(self):
+        if self.pending is not None:
+            stage, sends = self.pending
+            self.pending = None
+            self._route(stage, sends)
 
     def step_pair(self):
         self.step()
         self.step()
 
 
-def torch_exchange(dist):
+class _Posted:
+    def __init__(self, reqs, recvs):
+        self.reqs, self.recvs = reqs, recvs
+
+    def wait(self) -> dict:
+        for req in self.reqs:
+            req.wait()
+        return self.recvs
+
+
+class TorchExchange:
     """exchange(sends) over torch.distributed point-to-point calls (NCCL for device tensors, gloo
     for host tensors).  Every rank sends as many buffers to a peer as it receives from it, of equal
     sizes (the neighbouring faces have the same plane), so each send is matched by a receive of
-    the same shape posted in the same order."""
-    import torch
+    the same shape posted in the same order.  start(sends) posts the exchange and returns a handle
+    whose wait() gives the received buffers (for NCCL: the current stream then waits for the
+    transfers, the host does not)."""
 
-    def run(sends: dict) -> dict:
+    def __init__(self, dist):
+        self.dist = dist
+
+    def start(self, sends: dict) -> _Posted:
+        import torch
+        dist = self.dist
         me = dist.get_rank()
         recvs, ops = {}, []
         for peer in sorted(sends):
@@ -151,12 +230,14 @@ def torch_exchange(dist):
                 ops.append(dist.P2POp(dist.isend, b, peer))
             for r in recvs[peer]:
                 ops.append(dist.P2POp(dist.irecv, r, peer))
-        if ops:
-            for req in dist.batch_isend_irecv(ops):
-                req.wait()
-        return recvs
+        return _Posted(dist.batch_isend_irecv(ops) if ops else [], recvs)
 
-    return run
+    def __call__(self, sends: dict) -> dict:
+        return self.start(sends).wait()
+
+
+def torch_exchange(dist) -> TorchExchange:
+    return TorchExchange(dist)
 
 
 def slab_config(config, lo: int, hi: int, ring: Ring):
@@ -221,6 +302,14 @@ class DeviceSlab:
 
     def step(self):
         self.ctx.step_level(0)
+
+    @property
+    def n_planes(self) -> int:
+        """Planes of the split axis (plane-range steps are D3Q19 only)."""
+        return self.box_n[-1] if self.config.dims == 3 else 0
+
+    def step_planes(self, first: int, count: int, finish: bool):
+        self.ctx.step_level_planes(0, first, count, finish)
 
     def pack(self, face: int, stage: int):
         import torch
