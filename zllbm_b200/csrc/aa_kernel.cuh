@@ -76,6 +76,10 @@ struct LevelGeom {
     FastDiv fa0, fa1;  // division by a[0] and a[1] (cell index -> box coordinates)
     // D3Q19 step launches: planes [z0, z0 + zn) of the last axis; zn = 0: every plane
     int z0, zn;
+    // one-node step launches: 1 = threads numbered over each x-y plane (x fastest) instead of per
+    // row, so that rows whose length is not a multiple of 32 share warps; fn0 divides by n[0]
+    int flat;
+    FastDiv fn0;
 };
 
 struct StepParams {
@@ -1259,8 +1263,14 @@ template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext =
 __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>::kMinBlocks))
     aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
     Coord c;
-    c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
-    c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
+    if (geo.flat) {
+        const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, y = geo.fn0.div(t);
+        c.x[0] = (int)(t - y * (uint32_t)geo.n[0]);
+        c.x[1] = (int)y;
+    } else {
+        c.x[0] = blockIdx.x * blockDim.x + threadIdx.x;
+        c.x[1] = blockIdx.y * blockDim.y + threadIdx.y;
+    }
     c.x[2] = blockIdx.z + geo.z0;
     if (sizeof(S) == 2 && (blockIdx.x | blockIdx.y | blockIdx.z | threadIdx.x | threadIdx.y) == 0)
         sr_advance(p, Odd, sr_seed(p, Odd), true);
