@@ -1152,7 +1152,8 @@ __device__ __forceinline__ void aa_node(S* __restrict__ f, const LevelGeom& geo,
             for (int q = 1; q < Q; ++q) {
                 const bool miss = Masked ? ((info >> q) & 1u) : upstream_missing<L>(geo, c, q);
                 if (!miss) continue;
-                const T v = missing_value<L, T>(q, faces, pre, post, p);
+                // off every domain face (coarse/fine interface nodes) the value is the stale one
+                const T v = faces ? missing_value<L, T>(q, faces, pre, post, p) : pre[q];
                 if (Odd) {
                     St::store_raw(plane(q) + self, v);
                 } else {

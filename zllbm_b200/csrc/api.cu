@@ -7,6 +7,7 @@
 #include <string>
 #include <unordered_map>
 #include <algorithm>
+#include <iterator>
 #include <vector>
 #include "zllbm_b200.h"
 #include "closure_launch.cuh"
@@ -53,11 +54,12 @@ struct Level {
     long long n_node_codes = 0;
     // coarse/fine transfer with the next coarser level (this level is the fine side)
     DeviceBuffer macro;                                   // rho, u of transfer sources
-    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w, c2f_w32;
+    DeviceBuffer c2f_target, c2f_offset, c2f_src, c2f_w, c2f_sw32;
     DeviceBuffer c2f_ucell, c2f_ufine, c2f_g;  // distinct sources: cell, kind, values of a transfer
     int n_c2f = 0, n_c2f_src = 0;
     DeviceBuffer f2c_coarse, f2c_fine;
     int n_f2c = 0;
+    bool c2f_f2c_disjoint = false;  // no explosion target is a coalescence source: one launch for both
     // the level's immersed-boundary pass may run beside its transfers (zl_advance on level
     // streams): no cell its pass reads lies within two cells of one a transfer writes
     bool ib_concurrent = false;
@@ -75,7 +77,7 @@ struct Level {
     DeviceBuffer ib_pair_cell, ib_pair_w, ib_csr_start, ib_csr_vertex, ib_csr_share;
     int n_vertices = 0, n_ib_nodes = 0;
     int ib_width = 4;        // immersed-boundary stencil: 4 (reference) or 3 (Roma et al.)
-    DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q doubles)
+    DeviceBuffer c2f_last;   // explosion targets' values at the last transfer (n_c2f x q, storage arithmetic type)
     bool c2f_last_valid = false;
     DeviceBuffer c_node;     // learned closure: c of the last network evaluation per cell
     DeviceBuffer sr_seed;    // stochastic rounding: the two step seeds (StepParams::sr_seed)
@@ -758,7 +760,7 @@ static int level_faces(zl_ctx* ctx, Level& L) {
 
 static C2FStencil c2f_stencil(const Level& F) {
     return C2FStencil{(const int*)F.c2f_target.ptr, (const int*)F.c2f_offset.ptr, (const int*)F.c2f_src.ptr,
-                      (const double*)F.c2f_w.ptr,      (const float*)F.c2f_w32.ptr, F.n_c2f,
+                      (const double*)F.c2f_w.ptr,      (const int2*)F.c2f_sw32.ptr, F.n_c2f,
                       (const int*)F.c2f_ucell.ptr,     (const uint8_t*)F.c2f_ufine.ptr,
                       F.n_c2f_src,                     F.c2f_g.ptr};
 }
@@ -773,8 +775,8 @@ static int interpolate_interface(zl_ctx* ctx, int fine_level, bool save_only) {
         return fail(ctx, ZL_ESTATE, "level %d: no transfer yet to interpolate from", fine_level);
     const C2FStencil st = c2f_stencil(F);
     ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
-                               C.params, st, F.tau_c2f, save_only ? (double*)F.c2f_last.ptr : nullptr,
-                               save_only ? nullptr : (const double*)F.c2f_last.ptr, save_only ? 0 : 1, ctx->stream));
+                               C.params, st, F.tau_c2f, save_only ? F.c2f_last.ptr : nullptr,
+                               save_only ? nullptr : F.c2f_last.ptr, save_only ? 0 : 1, nullptr, ctx->stream));
     if (save_only) F.c2f_last_valid = true;
     return ZL_OK;
 }
@@ -787,12 +789,16 @@ int zl_transfer_levels(zl_ctx* ctx, int fine_level) {
     Level& C = ctx->levels[fine_level - 1];
     if (!F.has_transfer) return fail(ctx, ZL_ESTATE, "level %d: call zl_set_level_interface first", fine_level);
     const C2FStencil st = c2f_stencil(F);
+    const F2CJob job{(const int*)F.f2c_coarse.ptr, (const int*)F.f2c_fine.ptr, F.n_f2c, (const double*)F.macro.ptr,
+                     F.tau_f2c};
+    const bool fused = F.c2f_f2c_disjoint && F.n_f2c > 0;
     ZL_CUDA(ctx, ctx->ops->c2f(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
-                               C.params, st, F.tau_c2f, (double*)F.c2f_last.ptr, nullptr, 1, ctx->stream));
+                               C.params, st, F.tau_c2f, F.c2f_last.ptr, nullptr, 1, fused ? &job : nullptr,
+                               ctx->stream));
     F.c2f_last_valid = F.c2f_last.ptr != nullptr;
-    ZL_CUDA(ctx, ctx->ops->f2c(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
-                               C.params, (const int*)F.f2c_coarse.ptr, (const int*)F.f2c_fine.ptr, F.n_f2c,
-                               (const double*)F.macro.ptr, F.tau_f2c, ctx->stream));
+    if (!fused)
+        ZL_CUDA(ctx, ctx->ops->f2c(ctx->dims, F.f.ptr, F.geo, F.even_layout, C.f.ptr, C.geo, C.even_layout, F.params,
+                                   C.params, job, ctx->stream));
     return ZL_OK;
 }
 
@@ -1302,6 +1308,21 @@ __global__ void or_bits_kernel(uint32_t* info, const int* cells, int n, uint32_t
 }
 
 template <class T>
+int upload_vec(zl_ctx* ctx, DeviceBuffer& b, const std::vector<T>& v);
+
+// (source row, FP32 bits of the weight) per explosion entry.
+std::vector<int2> packed_src_w32(const std::vector<int>& src, const std::vector<double>& w) {
+    std::vector<int2> out(src.size());
+    for (size_t k = 0; k < src.size(); ++k) {
+        const float f = (float)w[k];
+        int bits;
+        std::memcpy(&bits, &f, 4);
+        out[k] = make_int2(src[k], bits);
+    }
+    return out;
+}
+
+template <class T>
 int upload_vec(zl_ctx* ctx, DeviceBuffer& b, const std::vector<T>& v) {
     int rc = alloc(ctx, b, v.size() * sizeof(T));
     if (rc) return rc;
@@ -1449,7 +1470,7 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
     if ((rc = upload_vec(ctx, F.c2f_target, tgt)) || (rc = upload_vec(ctx, F.c2f_offset, off)) ||
         (rc = upload_vec(ctx, F.c2f_src, src)) || (rc = upload_vec(ctx, F.c2f_ucell, ucell)) ||
         (rc = upload_vec(ctx, F.c2f_ufine, ufine)) || (rc = upload_vec(ctx, F.c2f_w, wts)) ||
-        (rc = upload_vec(ctx, F.c2f_w32, std::vector<float>(wts.begin(), wts.end()))) ||
+        (rc = upload_vec(ctx, F.c2f_sw32, packed_src_w32(src, wts))) ||
         (rc = upload_vec(ctx, F.f2c_coarse, f2c_c)) || (rc = upload_vec(ctx, F.f2c_fine, f2c_f)))
         return rc;
     F.n_c2f = (int)tgt.size();
@@ -1458,7 +1479,15 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
     const size_t g_elem = ctx->cfg.storage == ZL_STORAGE_F64 ? sizeof(double) : sizeof(float);
     if ((rc = alloc(ctx, F.c2f_g, (size_t)std::max(F.n_c2f_src, 1) * ctx->q * g_elem))) return rc;
     F.n_f2c = (int)f2c_c.size();
-    if ((rc = alloc(ctx, F.c2f_last, (size_t)std::max(F.n_c2f, 1) * ctx->q * sizeof(double)))) return rc;
+    {
+        std::vector<int> a(tgt), b(f2c_f);
+        std::sort(a.begin(), a.end());
+        std::sort(b.begin(), b.end());
+        std::vector<int> common;
+        std::set_intersection(a.begin(), a.end(), b.begin(), b.end(), std::back_inserter(common));
+        F.c2f_f2c_disjoint = common.empty();
+    }
+    if ((rc = alloc(ctx, F.c2f_last, (size_t)std::max(F.n_c2f, 1) * ctx->q * g_elem))) return rc;
     F.c2f_last_valid = false;
     // coalescence sources keep rho, u of their last collision
     if (F.n_f2c > 0) {

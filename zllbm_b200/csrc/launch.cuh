@@ -25,12 +25,13 @@ struct LaunchSet {
                           int* bad, cudaStream_t s);
     cudaError_t (*conservation)(int dims, const void* f, const LevelGeom& geo, const StepParams& p,
                                 int even_layout, double* partial, int nblocks, double* out, cudaStream_t s);
-    cudaError_t (*c2f)(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc, const LevelGeom& cgeo,
+    // explosion (save / prev in the storage's arithmetic type); with `with_f2c` (no target a
+    // coalescence source) the coalescence too, in the same launch
+    cudaError_t (*c2f)(int dims, void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const C2FStencil& st, double tau_ratio,
-                       double* save, const double* prev, int store, cudaStream_t s);
+                       void* save, const void* prev, int store, const F2CJob* with_f2c, cudaStream_t s);
     cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
-                       int c_even, const StepParams& fp, const StepParams& cp, const int* coarse_cell,
-                       const int* fine_cell, int n, const double* fine_macro, double tau_ratio, cudaStream_t s);
+                       int c_even, const StepParams& fp, const StepParams& cp, const F2CJob& job, cudaStream_t s);
     cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even_layout,
                             const int* nodes, int n_nodes, double* node_force, double* node_vel, cudaStream_t s);
     // ext: kExtForce / kExtLes bits of the levels in the batch
@@ -176,40 +177,52 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         conservation_final_kernel<<<1, 32, 0, s>>>(partial, nblocks, out);                                       \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
-    cudaError_t c2f_any(int dims, void* ff, const LevelGeom& fgeo, int f_even, const void* fc,                   \
-                        const LevelGeom& cgeo, int c_even, const StepParams& fp, const StepParams& cp,           \
-                        const C2FStencil& st, double tau_ratio, double* save, const double* prev, int store,     \
+    cudaError_t c2f_any(int dims, void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,     \
+                        int c_even, const StepParams& fp, const StepParams& cp, const C2FStencil& st,            \
+                        double tau_ratio, void* save, const void* prev, int store, const F2CJob* with_f2c,       \
                         cudaStream_t s) {                                                                        \
         if (st.n_targets <= 0) return cudaSuccess;                                                               \
+        using T = typename Storage<S>::T;                                                                        \
+        const int q = dims == 2 ? 9 : 19;                                                                        \
         const unsigned sblocks = (unsigned)((st.n_sources + 127) / 128);                                         \
-        const unsigned wblocks = (unsigned)(((long long)st.n_targets * (dims == 2 ? 9 : 19) + kC2fThreads - 1) /  \
-                                            kC2fThreads);                                                        \
+        const unsigned wblocks = (unsigned)(((long long)st.n_targets * q + kC2fThreads - 1) / kC2fThreads);     \
+        const unsigned fblocks = with_f2c ? (unsigned)(((long long)with_f2c->n * q + kC2fThreads - 1) /          \
+                                                       kC2fThreads) : 0u;                                        \
         if (dims == 2) {                                                                                         \
             if (st.n_sources > 0)                                                                                \
                 c2f_sources_kernel<D2Q9, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,    \
                                                                     cgeo, c_even, fp, cp, st, tau_ratio);        \
-            c2f_kernel<D2Q9, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, save, prev, store);\
+            if (with_f2c)                                                                                        \
+                c2f_f2c_kernel<D2Q9, S><<<wblocks + fblocks, kC2fThreads, 0, s>>>(                               \
+                    (S*)ff, fgeo, f_even, fp, st, (T*)save, (S*)fc, cgeo, c_even, cp, *with_f2c, wblocks);       \
+            else                                                                                                 \
+                c2f_kernel<D2Q9, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, (T*)save,      \
+                                                                     (const T*)prev, store);                     \
         } else {                                                                                                 \
             if (st.n_sources > 0)                                                                                \
                 c2f_sources_kernel<D3Q19, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,   \
                                                                      cgeo, c_even, fp, cp, st, tau_ratio);       \
-            c2f_kernel<D3Q19, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, save, prev, store);\
+            if (with_f2c)                                                                                        \
+                c2f_f2c_kernel<D3Q19, S><<<wblocks + fblocks, kC2fThreads, 0, s>>>(                              \
+                    (S*)ff, fgeo, f_even, fp, st, (T*)save, (S*)fc, cgeo, c_even, cp, *with_f2c, wblocks);       \
+            else                                                                                                 \
+                c2f_kernel<D3Q19, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, (T*)save,     \
+                                                                      (const T*)prev, store);                    \
         }                                                                                                        \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t f2c_any(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc,                   \
                         const LevelGeom& cgeo, int c_even, const StepParams& fp, const StepParams& cp,           \
-                        const int* coarse_cell, const int* fine_cell, int n, const double* fine_macro,           \
-                        double tau_ratio, cudaStream_t s) {                                                      \
-        if (n <= 0) return cudaSuccess;                                                                          \
+                        const F2CJob& job, cudaStream_t s) {                                                     \
+        if (job.n <= 0) return cudaSuccess;                                                                      \
         /* one thread per (node, population), 64-thread blocks spread them over every SM */                     \
-        const unsigned blocks = (unsigned)(((long long)n * (dims == 2 ? 9 : 19) + 63) / 64);                     \
+        const unsigned blocks = (unsigned)(((long long)job.n * (dims == 2 ? 9 : 19) + 63) / 64);                 \
         if (dims == 2)                                                                                           \
             f2c_kernel<D2Q9, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
-                                                      coarse_cell, fine_cell, n, fine_macro, tau_ratio);         \
+                                                      job);                                                      \
         else                                                                                                     \
-            f2c_kernel<D3Q19, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp,     \
-                                                       cp, coarse_cell, fine_cell, n, fine_macro, tau_ratio);    \
+            f2c_kernel<D3Q19, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp, \
+                                                       job);                                                     \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even,      \

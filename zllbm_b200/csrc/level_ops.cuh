@@ -273,7 +273,7 @@ struct C2FStencil {
     const int* offset;        // n_targets + 1
     const int* src;           // entry -> row of the source table
     const double* weight;
-    const float* weight32;    // the same weights rounded to FP32 (FP32 / FP16 / BF16 storage)
+    const int2* src_w32;      // (src, FP32 bits of the weight) per entry (FP32 / FP16 / BF16 storage)
     int n_targets;
     const int* src_cell;      // per source: coarse cell (src_fine == 0) or fine cell (src_fine == 1)
     const uint8_t* src_fine;
@@ -331,29 +331,36 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
 // (NodeInfoCoarse2fine + PostStreamCoarse2Fine, lbm_grid_interface.cpp:570-588,
 // collision_model/lbm_collision_models.cpp:244-251, or the post-stream populations of the
 // coincident fine node when the coarse node is absent or flagged).
-// save (optional) receives the targets' values (n_targets x Q, FP64); with prev (optional) the
-// targets get 0.5 (prev + value) instead, the time interpolation between the last transfer and
-// the coarse level's current state (no counterpart in the reference, whose explosion is spatial
-// only); store = 0 only saves.
+// save (optional) receives the targets' values (n_targets x Q, in the storage's arithmetic type:
+// FP64 for FP64 storage, FP32 otherwise); with prev (optional) the targets get 0.5 (prev + value)
+// instead, the time interpolation between the last transfer and the coarse level's current state
+// (no counterpart in the reference, whose explosion is spatial only); store = 0 only saves.
 // One thread per (target, population q), consecutive threads taking consecutive q of a target:
 // every lane of a warp works (Q = 19 or 9 does not divide a warp), the target's source indices
 // and weights are loads the target's lanes share, and the source rows are read coalesced.  Each
 // thread sums over the target's sources in table order (FP64 keeps its summation order), four
 // sources' loads in flight at a time.
 template <class L, class S>
-__global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
-                                                         StepParams fp, C2FStencil st, double* __restrict__ save,
-                                                         const double* __restrict__ prev, int store) {
+__device__ __forceinline__ void c2f_thread(long long i, S* __restrict__ ff, const LevelGeom& fgeo, int f_even,
+                                           const StepParams& fp, const C2FStencil& st,
+                                           typename Storage<S>::T* __restrict__ save,
+                                           const typename Storage<S>::T* __restrict__ prev, int store) {
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= (long long)st.n_targets * Q) return;
     const int t = (int)(i / Q), q = (int)(i - (long long)t * Q);
     const T* __restrict__ g = static_cast<const T*>(st.g);
-    auto weight = [&](int k) -> T {
-        if constexpr (sizeof(T) == 8) return __ldg(st.weight + k);
-        else return __ldg(st.weight32 + k);
+    // entry k: its source row and weight (FP32 storages: one 8-byte load for both)
+    auto entry = [&](int k, int& s, T& w) {
+        if constexpr (sizeof(T) == 8) {
+            s = __ldg(st.src + k);
+            w = __ldg(st.weight + k);
+        } else {
+            const int2 e = __ldg(st.src_w32 + k);
+            s = e.x;
+            w = __int_as_float(e.y);
+        }
     };
     T acc = (T)0;
     const int k1 = __ldg(st.offset + t + 1);
@@ -362,43 +369,62 @@ __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, Le
         int s4[4];
         T w4[4], g4[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            s4[e] = __ldg(st.src + k + e);
-            w4[e] = weight(k + e);
-        }
+        for (int e = 0; e < 4; ++e) entry(k + e, s4[e], w4[e]);
 #pragma unroll
         for (int e = 0; e < 4; ++e) g4[e] = __ldg(g + (long long)s4[e] * Q + q);
 #pragma unroll
         for (int e = 0; e < 4; ++e) acc = acc + w4[e] * g4[e];
     }
-    for (; k < k1; ++k) acc = acc + weight(k) * __ldg(g + (long long)__ldg(st.src + k) * Q + q);
-    if (save) save[i] = (double)acc;
+    for (; k < k1; ++k) {
+        int s;
+        T w;
+        entry(k, s, w);
+        acc = acc + w * __ldg(g + (long long)s * Q + q);
+    }
+    if (save) save[i] = acc;
     if (!store) return;
-    if (prev) acc = (T)0.5 * ((T)prev[i] + acc);
+    if (prev) acc = (T)0.5 * (prev[i] + acc);
     const Coord c = cell_coord(fgeo, st.target[t]);
     St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), acc, fp);
 }
+
+template <class L, class S>
+__global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
+                                                         StepParams fp, C2FStencil st,
+                                                         typename Storage<S>::T* __restrict__ save,
+                                                         const typename Storage<S>::T* __restrict__ prev, int store) {
+    c2f_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fp, st, save, prev, store);
+}
+
+// The coalescence nodes of a transfer: coarse cell, coincident fine cell, the fine level's saved
+// macros and the relaxation-time ratio.
+struct F2CJob {
+    const int* coarse_cell;
+    const int* fine_cell;
+    int n;
+    const double* fine_macro;
+    double tau_ratio;
+};
 
 // Coalescence (TransferInfoToCoarseGrid, lbm_grid_interface.cpp:524-564): a coarse node of the
 // inner coarse-to-fine layer takes rho, u of the coincident fine node (as stored by its last
 // collision) and f = feq + tau_f2c (f_fine - feq) (NodeInfoFine2Coarse + PostStreamFine2Coarse,
 // lbm_grid_interface.cpp:594-610, lbm_collision_models.cpp:259-267).
+// One thread per (node, population q): a few thousand nodes give the launch Q times the threads,
+// and each thread has one population load in flight with the node's macros; every thread of a node
+// forms the same feq (the same operations in the same order) and keeps its q.
 template <class L, class S>
-__global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, S* __restrict__ fc, LevelGeom cgeo,
-                           int c_even, StepParams fp, StepParams cp, const int* __restrict__ coarse_cell,
-                           const int* __restrict__ fine_cell, int n, const double* __restrict__ fine_macro,
-                           double tau_ratio) {
+__device__ __forceinline__ void f2c_thread(long long i, const S* __restrict__ ff, const LevelGeom& fgeo, int f_even,
+                                           S* __restrict__ fc, const LevelGeom& cgeo, int c_even,
+                                           const StepParams& fp, const StepParams& cp, const F2CJob& job) {
     using St = Storage<S>;
     constexpr int Q = L::kQ;
-    // one thread per (node, population q): a few thousand nodes give the launch Q times the
-    // threads, and each thread has one population load in flight with the node's macros; every
-    // thread of a node forms the same feq (the same operations in the same order) and keeps its q
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= (long long)n * Q) return;
+    if (i >= (long long)job.n * Q) return;
     const int t = (int)(i / Q), q = (int)(i - (long long)t * Q);
-    const Coord cf = cell_coord(fgeo, fine_cell[t]);
-    const Coord cc = cell_coord(cgeo, coarse_cell[t]);
-    const double* mac = fine_macro + (long long)fine_cell[t] * 4;
+    const int fcell = job.fine_cell[t];
+    const Coord cf = cell_coord(fgeo, fcell);
+    const Coord cc = cell_coord(cgeo, job.coarse_cell[t]);
+    const double* mac = job.fine_macro + (long long)fcell * 4;
     if constexpr (St::kDeviation) {
         const float v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
         float deq[Q];
@@ -407,7 +433,7 @@ __global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even,
 #pragma unroll
         for (int k = 1; k < Q; ++k)
             if (k == q) e = deq[k];
-        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + (float)tau_ratio * (v - e), cp);
+        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + (float)job.tau_ratio * (v - e), cp);
     } else {
         const double v = St::load(ff + post_stream_slot<L>(fgeo, cf, q, f_even), fp);
         double feq[Q];
@@ -416,8 +442,32 @@ __global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even,
 #pragma unroll
         for (int k = 1; k < Q; ++k)
             if (k == q) e = feq[k];
-        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + tau_ratio * (v - e), cp);
+        St::store(fc + post_stream_slot<L>(cgeo, cc, q, c_even), e + job.tau_ratio * (v - e), cp);
     }
+}
+
+template <class L, class S>
+__global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, S* __restrict__ fc, LevelGeom cgeo,
+                           int c_even, StepParams fp, StepParams cp, F2CJob job) {
+    f2c_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fc, cgeo, c_even, fp, cp, job);
+}
+
+// The explosion and the coalescence of one transfer in one launch: blocks [0, c2f_blocks) form the
+// explosion targets, the others the coalescence nodes.  Used when no explosion target is a
+// coalescence source: an explosion writes slot (t - c_q, opp q) or (t, q) of its target t, a
+// coalescence reads the same slot of its fine node, so the two meet only where a target is that
+// node, and running them side by side equals running them one after the other.
+template <class L, class S>
+__global__ void __launch_bounds__(kC2fThreads) c2f_f2c_kernel(S* __restrict__ ff, LevelGeom fgeo, int f_even,
+                                                             StepParams fp, C2FStencil st,
+                                                             typename Storage<S>::T* __restrict__ save, S* __restrict__ fc,
+                                                             LevelGeom cgeo, int c_even, StepParams cp, F2CJob job,
+                                                             unsigned c2f_blocks) {
+    if (blockIdx.x < c2f_blocks)
+        c2f_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fp, st, save, nullptr, 1);
+    else
+        f2c_thread<L, S>((blockIdx.x - c2f_blocks) * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fc, cgeo,
+                         c_even, fp, cp, job);
 }
 
 // ---------------------------------------------------------------- host exchange
