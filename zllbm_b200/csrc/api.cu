@@ -1552,10 +1552,10 @@ static IbVertices ib_view(zl_ctx* ctx, Level& L, int level) {
 static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     IbVertices v = ib_view(ctx, L, level);
     ZL_CUDA(ctx, ctx->ops->ib_touch(ctx->dims, L.f.ptr, L.geo, L.params, L.even_layout, (const int*)L.ib_nodes.ptr,
-                                    L.n_ib_nodes, (double*)L.force.ptr, (double*)L.ib_vel.ptr, ctx->stream));
-    // interpolation: one warp per vertex, kIbWarps vertices per block; spread: kIbSpreadLanes
-    // lanes per node
-    const unsigned blocks = (unsigned)((v.n + kIbWarps - 1) / kIbWarps), threads = 32 * kIbWarps;
+                                    L.n_ib_nodes, (double*)L.ib_vel.ptr, ctx->stream));
+    // interpolation: kIbForceLanes lanes per vertex; spread: kIbSpreadLanes lanes per node
+    const unsigned threads = kIbForceThreads,
+                   blocks = (unsigned)(((long long)v.n * kIbForceLanes + threads - 1) / threads);
     const unsigned nblocks = (unsigned)(((long long)L.n_ib_nodes * kIbSpreadLanes + 127) / 128);
     const int* pc = (const int*)L.ib_pair_cell.ptr;
     const double* pw = (const double*)L.ib_pair_w.ptr;

@@ -150,10 +150,10 @@ static __global__ void ib_release_kernel(const int* __restrict__ nodes, int n_no
     for (int a = 0; a < 3; ++a) node_force[cell * 3 + a] = 0.;
 }
 
+// Launch 1: the velocity of every stencil node (launch 3 then writes every stencil node's force).
 template <class L, class S>
 __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, int even_layout,
-                                const int* __restrict__ nodes, int n_nodes, double* __restrict__ node_force,
-                                double* __restrict__ node_vel) {
+                                const int* __restrict__ nodes, int n_nodes, double* __restrict__ node_vel) {
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ, D = L::kDims;
@@ -195,18 +195,7 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepPara
         u[1] = uy / rho;
         u[2] = D == 3 ? uz / rho : 0.;
     }
-    for (int a = 0; a < 3; ++a) {
-        node_force[cell * 3 + a] = 0.;
-        node_vel[cell * 3 + a] = u[a];
-    }
-}
-
-constexpr int kIbWarps = 4;  // vertices (warps) per block of the interpolation and spread kernels
-
-__device__ __forceinline__ double warp_sum_d(double x) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-    return x;
+    for (int a = 0; a < 3; ++a) node_vel[cell * 3 + a] = u[a];
 }
 
 // Every (vertex i, stencil node k) pair, k over width^D nodes x fastest: the node's cell, its
@@ -231,39 +220,60 @@ __global__ void ib_pairs_kernel(LevelGeom geo, LevelMap m, IbVertices v, const i
     pair_id[t] = (int)t;
 }
 
-// Launch 2: a warp per vertex interpolates the node velocities through its pairs.
+// Launch 2: kIbForceLanes lanes per vertex interpolate the node velocities through its pairs (a
+// vertex has 64 pairs in 3D, 16 in 2D with the four-point kernel): lane k takes pairs k,
+// k + kIbForceLanes, ..., two at a time with their loads issued first, and the lanes' sums are
+// combined by a fixed butterfly of shuffles.  The first lane writes F = 2 (U_b - sum delta u).
+constexpr int kIbForceLanes = 16;
+constexpr int kIbForceThreads = 128;
+
 template <int D>
-__global__ void __launch_bounds__(32 * kIbWarps) ib_force_kernel(IbVertices v, const int* __restrict__ pair_cell,
-                                                                 const double* __restrict__ pair_w,
-                                                                 const double* __restrict__ node_vel) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kIbWarps + w;
-    if (i >= v.n) return;
-    const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
-    const long long base = (long long)i * K;
-    double ur = 0., vr = 0., wr = 0.;
-    for (int k = lane; k < K; k += 32) {
-        const long long cell = __ldg(pair_cell + base + k);
-        const double delta = __ldg(pair_w + base + k);
-        ur += node_vel[cell * 3] * delta;
-        vr += node_vel[cell * 3 + 1] * delta;
-        if (D == 3) wr += node_vel[cell * 3 + 2] * delta;
+__global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v, const int* __restrict__ pair_cell,
+                                                                   const double* __restrict__ pair_w,
+                                                                   const double* __restrict__ node_vel) {
+    constexpr int G = kIbForceLanes;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int i = (int)(t / G), lane = (int)(t % G);
+    const bool live = i < v.n;  // every lane of the warp takes part in the shuffles
+    double u[3] = {0., 0., 0.};
+    if (live) {
+        const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
+        const long long base = (long long)i * K;
+        int k = lane;
+        for (; k + G < K; k += 2 * G) {
+            const long long c0 = __ldg(pair_cell + base + k), c1 = __ldg(pair_cell + base + k + G);
+            const double d0 = __ldg(pair_w + base + k), d1 = __ldg(pair_w + base + k + G);
+            double a0[3], a1[3];
+#pragma unroll
+            for (int a = 0; a < D; ++a) {
+                a0[a] = node_vel[c0 * 3 + a];
+                a1[a] = node_vel[c1 * 3 + a];
+            }
+#pragma unroll
+            for (int a = 0; a < D; ++a) u[a] = u[a] + a0[a] * d0 + a1[a] * d1;
+        }
+        if (k < K) {
+            const long long c = __ldg(pair_cell + base + k);
+            const double d = __ldg(pair_w + base + k);
+#pragma unroll
+            for (int a = 0; a < D; ++a) u[a] += node_vel[c * 3 + a] * d;
+        }
     }
-    ur = warp_sum_d(ur);
-    vr = warp_sum_d(vr);
-    if (D == 3) wr = warp_sum_d(wr);
-    if (lane == 0) {
-        v.force[i * 3] = 2. * (v.vel[i * 3] - ur);
-        v.force[i * 3 + 1] = 2. * (v.vel[i * 3 + 1] - vr);
-        v.force[i * 3 + 2] = D == 3 ? 2. * (v.vel[i * 3 + 2] - wr) : 0.;
-    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1)
+#pragma unroll
+        for (int a = 0; a < D; ++a) u[a] += __shfl_xor_sync(0xffffffffu, u[a], o);
+    if (!live || lane) return;
+    v.force[i * 3] = 2. * (v.vel[i * 3] - u[0]);
+    v.force[i * 3 + 1] = 2. * (v.vel[i * 3 + 1] - u[1]);
+    v.force[i * 3 + 2] = D == 3 ? 2. * (v.vel[i * 3 + 2] - u[2]) : 0.;
 }
 
 // Launch 3: kIbSpreadLanes lanes per stencil node sum F_i s_p over the node's pairs p (vertex i):
 // lane k takes pairs k, k + kIbSpreadLanes, ... of the node's CSR row, two at a time with their
 // loads issued first, and the lanes' sums are combined by a fixed butterfly of shuffles
-// (deterministic).  The first lane writes the node force (launch 1 zeroed it; no other pass adds
-// to it).  s_p = delta_p area_i / (dt dx^(d-1)) and the vertex index come from the CSR arrays,
+// (deterministic).  The first lane writes the node force (every stencil node owns at least one
+// pair, so every node of the list is written; no other pass adds to it).  s_p = delta_p area_i / (dt dx^(d-1)) and the vertex index come from the CSR arrays,
 // laid out in node order.  A node has about 16 (3D) pairs: the lanes cut the chain of dependent
 // loads per thread eightfold and give the launch eight times the threads.
 constexpr int kIbSpreadLanes = 8;

@@ -33,7 +33,7 @@ struct LaunchSet {
     cudaError_t (*f2c)(int dims, const void* ff, const LevelGeom& fgeo, int f_even, void* fc, const LevelGeom& cgeo,
                        int c_even, const StepParams& fp, const StepParams& cp, const F2CJob& job, cudaStream_t s);
     cudaError_t (*ib_touch)(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even_layout,
-                            const int* nodes, int n_nodes, double* node_force, double* node_vel, cudaStream_t s);
+                            const int* nodes, int n_nodes, double* node_vel, cudaStream_t s);
     // ext: kExtForce / kExtLes bits of the levels in the batch
     cudaError_t (*batch)(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s);
 };
@@ -226,16 +226,16 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t ib_touch_any(int dims, const void* f, const LevelGeom& geo, const StepParams& p, int even,      \
-                             const int* nodes, int n_nodes, double* node_force, double* node_vel,               \
+                             const int* nodes, int n_nodes, double* node_vel,                                   \
                              cudaStream_t s) {                                                                   \
         if (n_nodes <= 0) return cudaSuccess;                                                                    \
         const unsigned blocks = (unsigned)((n_nodes + 127) / 128);                                               \
         if (dims == 2)                                                                                           \
             ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,           \
-                                                            node_force, node_vel);                               \
+                                                            node_vel);                                           \
         else                                                                                                     \
             ib_touch_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,          \
-                                                             node_force, node_vel);                              \
+                                                             node_vel);                                          \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t batch_any(int dims, int coll, int ext, const LevelBatch& b, cudaStream_t s) {                    \
