@@ -23,6 +23,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include "lattice.cuh"
+#include "pdl.cuh"
 
 namespace zl {
 
@@ -1263,6 +1264,8 @@ struct StepOccupancy {
 template <class L, class S, int Coll, bool Odd, bool Bnd, bool Masked, int Ext = 0>
 __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>::kMinBlocks))
     aa_step_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    pdl_wait();
+    pdl_trigger();
     Coord c;
     if (geo.flat) {
         const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, y = geo.fn0.div(t);

@@ -1561,16 +1561,19 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     const double* pw = (const double*)L.ib_pair_w.ptr;
     const int *cs = (const int*)L.ib_csr_start.ptr, *cv = (const int*)L.ib_csr_vertex.ptr;
     const double* csh = (const double*)L.ib_csr_share.ptr;
+    // dependent launches: each kernel's launch overlaps the tail of the one before it
+    const double* vel = (const double*)L.ib_vel.ptr;
+    const int* nodes = (const int*)L.ib_nodes.ptr;
+    double* nf = (double*)L.force.ptr;
     if (ctx->dims == 2) {
-        ib_force_kernel<2><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<2><<<nblocks, 128, 0, ctx->stream>>>(v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs, cv, csh,
-                                                              (double*)L.force.ptr);
+        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<2>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel));
+        ZL_CUDA(ctx, launch_dependent(ib_spread_kernel<2>, dim3(nblocks), dim3(128), 0, ctx->stream, v, nodes,
+                                      L.n_ib_nodes, cs, cv, csh, nf));
     } else {
-        ib_force_kernel<3><<<blocks, threads, 0, ctx->stream>>>(v, pc, pw, (const double*)L.ib_vel.ptr);
-        ib_spread_kernel<3><<<nblocks, 128, 0, ctx->stream>>>(v, (const int*)L.ib_nodes.ptr, L.n_ib_nodes, cs, cv, csh,
-                                                              (double*)L.force.ptr);
+        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<3>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel));
+        ZL_CUDA(ctx, launch_dependent(ib_spread_kernel<3>, dim3(nblocks), dim3(128), 0, ctx->stream, v, nodes,
+                                      L.n_ib_nodes, cs, cv, csh, nf));
     }
-    ZL_CUDA(ctx, cudaGetLastError());
     return ZL_OK;
 }
 

@@ -154,6 +154,8 @@ static __global__ void ib_release_kernel(const int* __restrict__ nodes, int n_no
 template <class L, class S>
 __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, int even_layout,
                                 const int* __restrict__ nodes, int n_nodes, double* __restrict__ node_vel) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ, D = L::kDims;
@@ -231,6 +233,8 @@ template <int D>
 __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v, const int* __restrict__ pair_cell,
                                                                    const double* __restrict__ pair_w,
                                                                    const double* __restrict__ node_vel) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int G = kIbForceLanes;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int i = (int)(t / G), lane = (int)(t % G);
@@ -282,6 +286,8 @@ template <int D>
 __global__ void ib_spread_kernel(IbVertices v, const int* __restrict__ nodes, int n_nodes,
                                  const int* __restrict__ csr_start, const int* __restrict__ csr_vertex,
                                  const double* __restrict__ csr_share, double* __restrict__ node_force) {
+    pdl_wait();
+    pdl_trigger();
     constexpr int G = kIbSpreadLanes;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     const int j = (int)(t / G), k = (int)(t % G);

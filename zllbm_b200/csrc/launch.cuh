@@ -118,9 +118,9 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         const int n0 = geo.n[o0], n1 = dims == 3 ? geo.n[o1] : 1;                                                \
         dim3 b(128), g((n0 + 127) / 128, n1);                                                                    \
         if (dims == 2)                                                                                           \
-            neq_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even, feq_b);                              \
+            ZL_LAUNCH_DEP(neq_face_kernel<D2Q9, S>, g, b, 0, s, f, geo, p, face, even, feq_b);                              \
         else                                                                                                     \
-            neq_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even, feq_b);                             \
+            ZL_LAUNCH_DEP(neq_face_kernel<D3Q19, S>, g, b, 0, s, f, geo, p, face, even, feq_b);                             \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
     cudaError_t face_any(int dims, int kind, void* fv, const LevelGeom& geo, const StepParams& p, int face,     \
@@ -131,13 +131,13 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         const int n0 = geo.n[o0], n1 = dims == 3 ? geo.n[o1] : 1;                                                \
         dim3 b(128), g((n0 + 127) / 128, n1);                                                                    \
         if (dims == 2) {                                                                                         \
-            if (kind == kBcBounceBack) bb_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);           \
-            else if (kind == kBcConvective) conv_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);    \
-            else periodic_face_kernel<D2Q9, S><<<g, b, 0, s>>>(f, geo, p, face, even);                           \
+            if (kind == kBcBounceBack) ZL_LAUNCH_DEP(bb_face_kernel<D2Q9, S>, g, b, 0, s, f, geo, p, face, even);           \
+            else if (kind == kBcConvective) ZL_LAUNCH_DEP(conv_face_kernel<D2Q9, S>, g, b, 0, s, f, geo, p, face, even);    \
+            else ZL_LAUNCH_DEP(periodic_face_kernel<D2Q9, S>, g, b, 0, s, f, geo, p, face, even);                           \
         } else {                                                                                                 \
-            if (kind == kBcBounceBack) bb_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);          \
-            else if (kind == kBcConvective) conv_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);   \
-            else periodic_face_kernel<D3Q19, S><<<g, b, 0, s>>>(f, geo, p, face, even);                          \
+            if (kind == kBcBounceBack) ZL_LAUNCH_DEP(bb_face_kernel<D3Q19, S>, g, b, 0, s, f, geo, p, face, even);          \
+            else if (kind == kBcConvective) ZL_LAUNCH_DEP(conv_face_kernel<D3Q19, S>, g, b, 0, s, f, geo, p, face, even);   \
+            else ZL_LAUNCH_DEP(periodic_face_kernel<D3Q19, S>, g, b, 0, s, f, geo, p, face, even);                          \
         }                                                                                                        \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
@@ -190,23 +190,23 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
                                                        kC2fThreads) : 0u;                                        \
         if (dims == 2) {                                                                                         \
             if (st.n_sources > 0)                                                                                \
-                c2f_sources_kernel<D2Q9, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,    \
+                ZL_LAUNCH_DEP(c2f_sources_kernel<D2Q9, S>, sblocks, 128, 0, s, (const S*)ff, fgeo, f_even, (const S*)fc,    \
                                                                     cgeo, c_even, fp, cp, st, tau_ratio);        \
             if (with_f2c)                                                                                        \
-                c2f_f2c_kernel<D2Q9, S><<<wblocks + fblocks, kC2fThreads, 0, s>>>(                               \
+                ZL_LAUNCH_DEP(c2f_f2c_kernel<D2Q9, S>, wblocks + fblocks, kC2fThreads, 0, s,                                \
                     (S*)ff, fgeo, f_even, fp, st, (T*)save, (S*)fc, cgeo, c_even, cp, *with_f2c, wblocks);       \
             else                                                                                                 \
-                c2f_kernel<D2Q9, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, (T*)save,      \
+                ZL_LAUNCH_DEP(c2f_kernel<D2Q9, S>, wblocks, kC2fThreads, 0, s, (S*)ff, fgeo, f_even, fp, st, (T*)save,      \
                                                                      (const T*)prev, store);                     \
         } else {                                                                                                 \
             if (st.n_sources > 0)                                                                                \
-                c2f_sources_kernel<D3Q19, S><<<sblocks, 128, 0, s>>>((const S*)ff, fgeo, f_even, (const S*)fc,   \
+                ZL_LAUNCH_DEP(c2f_sources_kernel<D3Q19, S>, sblocks, 128, 0, s, (const S*)ff, fgeo, f_even, (const S*)fc,   \
                                                                      cgeo, c_even, fp, cp, st, tau_ratio);       \
             if (with_f2c)                                                                                        \
-                c2f_f2c_kernel<D3Q19, S><<<wblocks + fblocks, kC2fThreads, 0, s>>>(                              \
+                ZL_LAUNCH_DEP(c2f_f2c_kernel<D3Q19, S>, wblocks + fblocks, kC2fThreads, 0, s,                               \
                     (S*)ff, fgeo, f_even, fp, st, (T*)save, (S*)fc, cgeo, c_even, cp, *with_f2c, wblocks);       \
             else                                                                                                 \
-                c2f_kernel<D3Q19, S><<<wblocks, kC2fThreads, 0, s>>>((S*)ff, fgeo, f_even, fp, st, (T*)save,     \
+                ZL_LAUNCH_DEP(c2f_kernel<D3Q19, S>, wblocks, kC2fThreads, 0, s, (S*)ff, fgeo, f_even, fp, st, (T*)save,     \
                                                                       (const T*)prev, store);                    \
         }                                                                                                        \
         return cudaGetLastError();                                                                               \
@@ -218,10 +218,10 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         /* one thread per (node, population), 64-thread blocks spread them over every SM */                     \
         const unsigned blocks = (unsigned)(((long long)job.n * (dims == 2 ? 9 : 19) + 63) / 64);                 \
         if (dims == 2)                                                                                           \
-            f2c_kernel<D2Q9, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
+            ZL_LAUNCH_DEP(f2c_kernel<D2Q9, S>, blocks, 64, 0, s, (const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp,  \
                                                       job);                                                      \
         else                                                                                                     \
-            f2c_kernel<D3Q19, S><<<blocks, 64, 0, s>>>((const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp, \
+            ZL_LAUNCH_DEP(f2c_kernel<D3Q19, S>, blocks, 64, 0, s, (const S*)ff, fgeo, f_even, (S*)fc, cgeo, c_even, fp, cp, \
                                                        job);                                                     \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \
@@ -231,10 +231,10 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         if (n_nodes <= 0) return cudaSuccess;                                                                    \
         const unsigned blocks = (unsigned)((n_nodes + 127) / 128);                                               \
         if (dims == 2)                                                                                           \
-            ib_touch_kernel<D2Q9, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,           \
+            ZL_LAUNCH_DEP(ib_touch_kernel<D2Q9, S>, blocks, 128, 0, s, (const S*)f, geo, p, even, nodes, n_nodes,           \
                                                             node_vel);                                           \
         else                                                                                                     \
-            ib_touch_kernel<D3Q19, S><<<blocks, 128, 0, s>>>((const S*)f, geo, p, even, nodes, n_nodes,          \
+            ZL_LAUNCH_DEP(ib_touch_kernel<D3Q19, S>, blocks, 128, 0, s, (const S*)f, geo, p, even, nodes, n_nodes,          \
                                                              node_vel);                                          \
         return cudaGetLastError();                                                                               \
     }                                                                                                            \

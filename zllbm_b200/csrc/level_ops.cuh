@@ -98,6 +98,8 @@ __device__ __forceinline__ void feq_dev(float rho, float ux, float uy, float uz,
 template <class L, class S>
 __global__ void neq_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout,
                                 const double* __restrict__ feq_b) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
@@ -193,6 +195,8 @@ __device__ __forceinline__ FaceNode face_node(const LevelGeom& geo, int face) {
 // post-stream value.  The formula is linear, so deviation and scaled storage use it unchanged.
 template <class L, class S>
 __global__ void conv_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     using Tb = Tables<L>;
     using T = typename St::T;
@@ -225,6 +229,8 @@ __global__ void conv_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p,
 // Used when the level's faces must be applied one after another in the reference's order.
 template <class L, class S>
 __global__ void bb_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     const FaceNode fn = face_node<L>(geo, face);
     if (!fn.ok) return;
@@ -242,6 +248,8 @@ __global__ void bb_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, i
 // node with the same other coordinates on the opposite face.
 template <class L, class S>
 __global__ void periodic_face_kernel(S* __restrict__ f, LevelGeom geo, StepParams p, int face, int even_layout) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     const FaceNode fn = face_node<L>(geo, face);
     if (!fn.ok) return;
@@ -292,6 +300,8 @@ template <class L, class S>
 __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, const S* __restrict__ fc,
                                    LevelGeom cgeo, int c_even, StepParams fp, StepParams cp, C2FStencil st,
                                    double tau_ratio) {
+    pdl_wait();
+    pdl_trigger();
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
@@ -393,6 +403,8 @@ __global__ void __launch_bounds__(kC2fThreads) c2f_kernel(S* __restrict__ ff, Le
                                                          StepParams fp, C2FStencil st,
                                                          typename Storage<S>::T* __restrict__ save,
                                                          const typename Storage<S>::T* __restrict__ prev, int store) {
+    pdl_wait();
+    pdl_trigger();
     c2f_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fp, st, save, prev, store);
 }
 
@@ -449,6 +461,8 @@ __device__ __forceinline__ void f2c_thread(long long i, const S* __restrict__ ff
 template <class L, class S>
 __global__ void f2c_kernel(const S* __restrict__ ff, LevelGeom fgeo, int f_even, S* __restrict__ fc, LevelGeom cgeo,
                            int c_even, StepParams fp, StepParams cp, F2CJob job) {
+    pdl_wait();
+    pdl_trigger();
     f2c_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fc, cgeo, c_even, fp, cp, job);
 }
 
@@ -463,6 +477,8 @@ __global__ void __launch_bounds__(kC2fThreads) c2f_f2c_kernel(S* __restrict__ ff
                                                              typename Storage<S>::T* __restrict__ save, S* __restrict__ fc,
                                                              LevelGeom cgeo, int c_even, StepParams cp, F2CJob job,
                                                              unsigned c2f_blocks) {
+    pdl_wait();
+    pdl_trigger();
     if (blockIdx.x < c2f_blocks)
         c2f_thread<L, S>(blockIdx.x * (long long)blockDim.x + threadIdx.x, ff, fgeo, f_even, fp, st, save, nullptr, 1);
     else

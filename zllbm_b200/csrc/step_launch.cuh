@@ -25,11 +25,11 @@ cudaError_t step_one(S* f, const LevelGeom& geo, const StepParams& p, cudaStream
         fg.flat = 1;
         fg.fn0 = FastDiv::make((uint32_t)geo.n[0]);
         const unsigned bs = plane * g.z >= 148ll * 128 * 8 ? 128u : 32u;
-        aa_step_kernel<L, S, C, O, B, M, X>
-            <<<dim3((unsigned)((plane + bs - 1) / bs), 1, g.z), dim3(bs), 0, s>>>(f, fg, p);
+        ZL_LAUNCH_DEP(aa_step_kernel<L, S, C, O, B, M, X>, dim3((unsigned)((plane + bs - 1) / bs), 1, g.z), dim3(bs), 0, s,
+                      f, fg, p);
         return cudaGetLastError();
     }
-    aa_step_kernel<L, S, C, O, B, M, X><<<g, b, 0, s>>>(f, geo, p);
+    ZL_LAUNCH_DEP(aa_step_kernel<L, S, C, O, B, M, X>, g, b, 0, s, f, geo, p);
     return cudaGetLastError();
 }
 
