@@ -1628,6 +1628,8 @@ __global__ void clear_missing_kernel(uint32_t* info, long long cells, int q) {
 template <class E>
 __global__ void halo_copy_kernel(E* f, long long stride, FacePlane fp, int np, int4 planes_lo, int4 planes_hi,
                                  E* buf, int pack) {
+    pdl_wait();
+    pdl_trigger();
     const long long per = (long long)fp.nb * fp.nc;
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= per * np) return;
@@ -1729,12 +1731,18 @@ static int halo_copy(zl_ctx* ctx, int level, int face, int stage, void* buf, boo
     const int4 hi = make_int4(planes[4], planes[5], planes[6], planes[7]);
     const unsigned blocks = (unsigned)((n + 255) / 256);
     switch (ctx->ops->elem_bytes) {
-        case 8: halo_copy_kernel<uint64_t><<<blocks, 256, 0, ctx->stream>>>((uint64_t*)L.f.ptr, L.geo.stride, fp, np, lo,
-                                                                            hi, (uint64_t*)buf, pack); break;
-        case 4: halo_copy_kernel<uint32_t><<<blocks, 256, 0, ctx->stream>>>((uint32_t*)L.f.ptr, L.geo.stride, fp, np, lo,
-                                                                            hi, (uint32_t*)buf, pack); break;
-        default: halo_copy_kernel<uint16_t><<<blocks, 256, 0, ctx->stream>>>((uint16_t*)L.f.ptr, L.geo.stride, fp, np, lo,
-                                                                             hi, (uint16_t*)buf, pack); break;
+        case 8:
+            ZL_CUDA(ctx, launch_dependent(halo_copy_kernel<uint64_t>, dim3(blocks), dim3(256), 0, ctx->stream,
+                                          (uint64_t*)L.f.ptr, L.geo.stride, fp, np, lo, hi, (uint64_t*)buf, pack));
+            break;
+        case 4:
+            ZL_CUDA(ctx, launch_dependent(halo_copy_kernel<uint32_t>, dim3(blocks), dim3(256), 0, ctx->stream,
+                                          (uint32_t*)L.f.ptr, L.geo.stride, fp, np, lo, hi, (uint32_t*)buf, pack));
+            break;
+        default:
+            ZL_CUDA(ctx, launch_dependent(halo_copy_kernel<uint16_t>, dim3(blocks), dim3(256), 0, ctx->stream,
+                                          (uint16_t*)L.f.ptr, L.geo.stride, fp, np, lo, hi, (uint16_t*)buf, pack));
+            break;
     }
     ZL_CUDA(ctx, cudaGetLastError());
     return ZL_OK;

@@ -154,6 +154,8 @@ __device__ __forceinline__ void fused_pair(const F2* d, F2* out, const StepParam
 // node update twice.
 template <class S, int Coll, bool Odd>
 __global__ void __launch_bounds__(256, 2) aa_pair_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    pdl_wait();
+    pdl_trigger();
     using Tb = Tables<D3Q19>;
     using St = Storage<S>;
     using IO = PairIO<S>;

@@ -100,6 +100,8 @@ __device__ __forceinline__ RowVec<V> row_shift_down(const RowVec<V>& in, int lan
 
 template <class S, int Coll, bool Odd, int V>
 __global__ void __launch_bounds__(128, 3) aa_row_kernel(S* __restrict__ f, LevelGeom geo, StepParams p) {
+    pdl_wait();
+    pdl_trigger();
     static_assert(sizeof(S) == 2 && (V == 4 || V == 8), "16-bit storage, 4 or 8 nodes per lane");
     using Tb = Tables<D3Q19>;
     using IO = HalfPairIO<S>;

@@ -44,7 +44,7 @@ cudaError_t step_pair(S* f, const LevelGeom& geo, const StepParams& p, cudaStrea
         }
         dim3 g, b;
         step_shape(geo, 3, g, b);
-        aa_pair_kernel<S, C, O><<<g, b, 0, s>>>(f, geo, p);
+        ZL_LAUNCH_DEP(aa_pair_kernel<S, C, O>, g, b, 0, s, f, geo, p);
         return cudaGetLastError();
     }
     return cudaErrorInvalidValue;
@@ -57,8 +57,8 @@ cudaError_t step_row(S* f, const LevelGeom& geo, const StepParams& p, cudaStream
         const int rows = geo.block[1];
         if (v == 0 || rows < 1 || rows > 4) return cudaErrorInvalidValue;
         const dim3 b(32 * rows), g((geo.n[1] + rows - 1) / rows, geo.zn > 0 ? geo.zn : geo.n[2]);
-        if (v == 8) aa_row_kernel<S, C, O, 8><<<g, b, 0, s>>>(f, geo, p);
-        else aa_row_kernel<S, C, O, 4><<<g, b, 0, s>>>(f, geo, p);
+        if (v == 8) ZL_LAUNCH_DEP(aa_row_kernel<S, C, O, 8>, g, b, 0, s, f, geo, p);
+        else ZL_LAUNCH_DEP(aa_row_kernel<S, C, O, 4>, g, b, 0, s, f, geo, p);
         return cudaGetLastError();
     }
     return cudaErrorInvalidValue;
