@@ -1417,14 +1417,15 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
         off.push_back((int)src.size());
     }
     {
-        // targets grouped by their number of sources (1, 4, 16 or 64 in 3D; a target's sum does
-        // not depend on where it sits in the list): the explosion kernel's warps, which cover
-        // consecutive targets, then loop over equal counts instead of the largest of mixed ones
+        // targets grouped by their number of sources, most first (64, 16, 4 or 1 in 3D; a target's
+        // sum does not depend on where it sits in the list): the explosion kernel's warps, which
+        // cover consecutive targets, then loop over equal counts instead of the largest of mixed
+        // ones, and the blocks with the longest loops start first instead of forming the tail
         const size_t nt = tgt.size();
         std::vector<int> perm(nt);
         for (size_t t = 0; t < nt; ++t) perm[t] = (int)t;
         std::stable_sort(perm.begin(), perm.end(),
-                         [&](int a, int b) { return off[a + 1] - off[a] < off[b + 1] - off[b]; });
+                         [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
         std::vector<int> tgt2(nt), off2(1, 0), src2;
         std::vector<double> wts2;
         src2.reserve(src.size());
@@ -1475,9 +1476,11 @@ int zl_set_level_interface(zl_ctx* ctx, int level, const uint64_t* c2f_fine, int
         return rc;
     F.n_c2f = (int)tgt.size();
     F.n_c2f_src = (int)ucell.size();
-    // source values in the storage's arithmetic type (FP64 for FP64 storage, FP32 otherwise)
+    // source values in the storage's arithmetic type (FP64 for FP64 storage, FP32 otherwise; FP32
+    // rows padded to whole groups of four)
     const size_t g_elem = ctx->cfg.storage == ZL_STORAGE_F64 ? sizeof(double) : sizeof(float);
-    if ((rc = alloc(ctx, F.c2f_g, (size_t)std::max(F.n_c2f_src, 1) * ctx->q * g_elem))) return rc;
+    const size_t g_row = g_elem == sizeof(double) ? (size_t)ctx->q : (size_t)(ctx->q + 3) / 4 * 4;
+    if ((rc = alloc(ctx, F.c2f_g, (size_t)std::max(F.n_c2f_src, 1) * g_row * g_elem))) return rc;
     F.n_f2c = (int)f2c_c.size();
     {
         std::vector<int> a(tgt), b(f2c_f);

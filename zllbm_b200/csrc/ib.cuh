@@ -224,8 +224,9 @@ __global__ void ib_pairs_kernel(LevelGeom geo, LevelMap m, IbVertices v, const i
 
 // Launch 2: kIbForceLanes lanes per vertex interpolate the node velocities through its pairs (a
 // vertex has 64 pairs in 3D, 16 in 2D with the four-point kernel): lane k takes pairs k,
-// k + kIbForceLanes, ..., two at a time with their loads issued first, and the lanes' sums are
-// combined by a fixed butterfly of shuffles.  The first lane writes F = 2 (U_b - sum delta u).
+// k + kIbForceLanes, ..., four at a time with their loads issued first (one round of two dependent
+// loads for the 3D kernel) and summed two by two, and the lanes' sums are combined by a fixed
+// butterfly of shuffles.  The first lane writes F = 2 (U_b - sum delta u).
 constexpr int kIbForceLanes = 16;
 constexpr int kIbForceThreads = 128;
 
@@ -244,6 +245,23 @@ __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v,
         const int K = D == 3 ? v.width * v.width * v.width : v.width * v.width;
         const long long base = (long long)i * K;
         int k = lane;
+        for (; k + 3 * G < K; k += 4 * G) {
+            long long c[4];
+            double d[4], a[4][3];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                c[e] = __ldg(pair_cell + base + k + e * G);
+                d[e] = __ldg(pair_w + base + k + e * G);
+            }
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+#pragma unroll
+                for (int b = 0; b < D; ++b) a[e][b] = node_vel[c[e] * 3 + b];
+#pragma unroll
+            for (int b = 0; b < D; ++b) u[b] = u[b] + a[0][b] * d[0] + a[1][b] * d[1];
+#pragma unroll
+            for (int b = 0; b < D; ++b) u[b] = u[b] + a[2][b] * d[2] + a[3][b] * d[3];
+        }
         for (; k + G < K; k += 2 * G) {
             const long long c0 = __ldg(pair_cell + base + k), c1 = __ldg(pair_cell + base + k + G);
             const double d0 = __ldg(pair_w + base + k), d1 = __ldg(pair_w + base + k + G);

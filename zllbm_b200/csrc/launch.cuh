@@ -185,7 +185,8 @@ cudaError_t step_lc(bool odd, bool bnd, bool masked, S* f, const LevelGeom& geo,
         using T = typename Storage<S>::T;                                                                        \
         const int q = dims == 2 ? 9 : 19;                                                                        \
         const unsigned sblocks = (unsigned)((st.n_sources + 127) / 128);                                         \
-        const unsigned wblocks = (unsigned)(((long long)st.n_targets * q + kC2fThreads - 1) / kC2fThreads);     \
+        const int lanes = sizeof(T) == 8 ? q : (q + 3) / 4; /* threads per target (c2f_lanes) */                 \
+        const unsigned wblocks = (unsigned)(((long long)st.n_targets * lanes + kC2fThreads - 1) / kC2fThreads); \
         const unsigned fblocks = with_f2c ? (unsigned)(((long long)with_f2c->n * q + kC2fThreads - 1) /          \
                                                        kC2fThreads) : 0u;                                        \
         if (dims == 2) {                                                                                         \

@@ -286,8 +286,20 @@ struct C2FStencil {
     const int* src_cell;      // per source: coarse cell (src_fine == 0) or fine cell (src_fine == 1)
     const uint8_t* src_fine;
     int n_sources;
-    void* g;                  // n_sources x Q source values (the storage's arithmetic type)
+    void* g;                  // n_sources rows of c2f_row values (the storage's arithmetic type)
 };
+
+// The source table's rows: Q values in FP64; in FP32, Q values and zeros up to a whole number of
+// float4 groups, so that a lane reads four populations of a source in one 16-byte load.
+template <class L, class T>
+ZL_HD constexpr int c2f_row() {
+    return sizeof(T) == 8 ? L::kQ : 4 * ((L::kQ + 3) / 4);
+}
+// Threads per explosion target: one per population in FP64, one per float4 group in FP32.
+template <class L, class T>
+ZL_HD constexpr int c2f_lanes() {
+    return sizeof(T) == 8 ? L::kQ : (L::kQ + 3) / 4;
+}
 
 // Explosion (TransferInfoFromCoarseGrid, lbm_grid_interface.cpp:408-515): every fine ghost node
 // becomes sum_k w_k g_k with g_k = feq(rho_c, u_c) + tau_c2f (f_c - feq) for a coarse source
@@ -331,9 +343,12 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
             for (int q = 0; q < Q; ++q) g[q] = feq[q] + tau_ratio * (fcq[q] - feq[q]);
         }
     }
-    T* out = static_cast<T*>(st.g) + (long long)u * Q;
+    constexpr int R = c2f_row<L, T>();
+    T* out = static_cast<T*>(st.g) + (long long)u * R;
 #pragma unroll
     for (int q = 0; q < Q; ++q) out[q] = g[q];
+#pragma unroll
+    for (int q = Q; q < R; ++q) out[q] = (T)0;
 }
 
 // Explosion (TransferInfoFromCoarseGrid, lbm_grid_interface.cpp:408-515): every fine ghost node
@@ -345,11 +360,14 @@ __global__ void c2f_sources_kernel(const S* __restrict__ ff, LevelGeom fgeo, int
 // FP64 for FP64 storage, FP32 otherwise); with prev (optional) the targets get 0.5 (prev + value)
 // instead, the time interpolation between the last transfer and the coarse level's current state
 // (no counterpart in the reference, whose explosion is spatial only); store = 0 only saves.
-// One thread per (target, population q), consecutive threads taking consecutive q of a target:
-// every lane of a warp works (Q = 19 or 9 does not divide a warp), the target's source indices
-// and weights are loads the target's lanes share, and the source rows are read coalesced.  Each
-// thread sums over the target's sources in table order (FP64 keeps its summation order), four
-// sources' loads in flight at a time.
+// FP64: one thread per (target, population q), consecutive threads taking consecutive q of a
+// target: every lane of a warp works (Q = 19 or 9 does not divide a warp), the target's source
+// indices and weights are loads the target's lanes share, and the source rows are read coalesced.
+// FP32: one thread per (target, group of four populations), each source row read as one float4
+// per thread (a quarter of the load requests: the kernel is bound by the L1 requests of its
+// gathers).  Each thread sums over the target's sources in table order, every population in the
+// same order as the one-population form (FP64 keeps its summation order), four sources' loads in
+// flight at a time.
 template <class L, class S>
 __device__ __forceinline__ void c2f_thread(long long i, S* __restrict__ ff, const LevelGeom& fgeo, int f_even,
                                            const StepParams& fp, const C2FStencil& st,
@@ -358,6 +376,56 @@ __device__ __forceinline__ void c2f_thread(long long i, S* __restrict__ ff, cons
     using St = Storage<S>;
     using T = typename St::T;
     constexpr int Q = L::kQ;
+    if constexpr (sizeof(T) == 4) {
+        constexpr int G = c2f_lanes<L, T>();
+        if (i >= (long long)st.n_targets * G) return;
+        const int t = (int)(i / G), part = (int)(i - (long long)t * G);
+        const float4* __restrict__ g4 = static_cast<const float4*>(st.g) + part;  // row s: g4[s G]
+        float acc[4] = {0.f, 0.f, 0.f, 0.f};
+        auto add = [&](int2 e, const float4& v) {
+            const float w = __int_as_float(e.y);
+            acc[0] = acc[0] + w * v.x;
+            acc[1] = acc[1] + w * v.y;
+            acc[2] = acc[2] + w * v.z;
+            acc[3] = acc[3] + w * v.w;
+        };
+        // rounds of four entries, predicated on the target's count; the next round's entries are
+        // loaded beside this round's rows, so a round waits for one load, not two in a chain
+        const int k1 = __ldg(st.offset + t + 1);
+        int k = __ldg(st.offset + t);
+        int2 en[4];
+        auto entries = [&](int k0) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) en[e] = k0 + e < k1 ? __ldg(st.src_w32 + k0 + e) : make_int2(0, 0);
+        };
+        entries(k);
+        for (; k < k1; k += 4) {
+            int2 e4[4];
+            float4 v4[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) e4[e] = en[e];
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                v4[e] = k + e < k1 ? __ldg(g4 + (long long)e4[e].x * G) : make_float4(0.f, 0.f, 0.f, 0.f);
+            if (k + 4 < k1) entries(k + 4);
+#pragma unroll
+            for (int e = 0; e < 4; ++e)
+                if (k + e < k1) add(e4[e], v4[e]);
+        }
+        const Coord c = cell_coord(fgeo, st.target[t]);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int q = 4 * part + j;
+            if (q >= Q) break;
+            const long long iq = (long long)t * Q + q;
+            float a = acc[j];
+            if (save) save[iq] = a;
+            if (!store) continue;
+            if (prev) a = 0.5f * (prev[iq] + a);
+            St::store(ff + post_stream_slot<L>(fgeo, c, q, f_even), a, fp);
+        }
+        return;
+    }
     if (i >= (long long)st.n_targets * Q) return;
     const int t = (int)(i / Q), q = (int)(i - (long long)t * Q);
     const T* __restrict__ g = static_cast<const T*>(st.g);
