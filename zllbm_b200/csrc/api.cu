@@ -460,8 +460,15 @@ static int setup_level(zl_ctx* ctx, int level, const uint64_t* codes, int64_t n,
     p.rho0 = ctx->cfg.rho0;
     p.fuse_bb = L.ordered ? 0 : 1;
     p.dt = dt;
-    p.forced = ctx->cfg.forcing ? 1 : 0;
     for (int a = 0; a < 3; ++a) p.const_force[a] = ctx->cfg.forcing ? ctx->cfg.constant_force[a] : 0.;
+    // FP64 follows the reference, which collides every node with the forcing terms when the
+    // solver has forces; the FP32 / FP16 / BF16 step of a level whose forces are all zero (no
+    // constant force, no immersed-boundary vertices so far) takes the unforced variant, whose
+    // result differs only in rounding (zl_ib_set_vertices switches the level over)
+    p.forced = ctx->cfg.forcing && (ctx->cfg.storage == ZL_STORAGE_F64 || p.const_force[0] != 0. ||
+                                    p.const_force[1] != 0. || p.const_force[2] != 0.)
+                   ? 1
+                   : 0;
     p.les = ctx->cfg.les ? 1 : 0;
     {
         const double cs = ctx->cfg.les_cs > 0. ? ctx->cfg.les_cs : 0.16;
@@ -817,6 +824,16 @@ static void time_stepping_order(int level, int max_level, std::vector<int>* orde
 // the levels' order).
 static int step_group(zl_ctx* ctx, const std::vector<int>& group) {
     if (group.size() == 1) return zl_step_level(ctx, group[0]);
+    // one variant per launch: levels with and without forcing terms step one by one
+    int forced = 0, unforced = 0;
+    for (int l : group) (ctx->levels[l].params.forced ? forced : unforced) = 1;
+    if (forced && unforced) {
+        for (int l : group) {
+            const int rc = zl_step_level(ctx, l);
+            if (rc) return rc;
+        }
+        return ZL_OK;
+    }
     LevelBatch b{};
     b.count = (int)group.size();
     b.first[0] = 0;
@@ -836,7 +853,7 @@ static int step_group(zl_ctx* ctx, const std::vector<int>& group) {
         const long long cells = (long long)L.geo.n[0] * L.geo.n[1] * L.geo.n[2];
         b.first[i + 1] = b.first[i] + (cells + kBatchThreads - 1) / kBatchThreads * kBatchThreads;
     }
-    const int ext = (ctx->cfg.forcing ? kExtForce : 0) | (ctx->cfg.les ? kExtLes : 0);
+    const int ext = (forced ? kExtForce : 0) | (ctx->cfg.les ? kExtLes : 0);
     ZL_CUDA(ctx, ctx->ops->batch(ctx->dims, ctx->cfg.collision, ext, b, ctx->stream));
     for (int l : group) {
         Level& L = ctx->levels[l];
@@ -1776,6 +1793,11 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
     } guard{L};
     L.n_vertices = 0;
     ++ctx->generation;
+    if (n > 0 && !L.params.forced) {
+        // node forces from now on: the level's steps take the forced variant
+        L.params.forced = 1;
+        if ((rc = sync_params(ctx, level))) return rc;
+    }
     if ((rc = alloc(ctx, L.ib_coord, (size_t)n * 3 * 8)) || (rc = alloc(ctx, L.ib_uvel, (size_t)n * 3 * 8)) ||
         (rc = alloc(ctx, L.ib_area, (size_t)n * 8)) || (rc = alloc(ctx, L.ib_force, (size_t)n * 3 * 8)) ||
         (rc = alloc(ctx, L.ib_total, 3 * 8)))
