@@ -1030,7 +1030,11 @@ static int advance_streams(zl_ctx* ctx, int steps, const std::vector<int>& order
                 (rc = run(l, l - 1, l, [&] { return interpolate_interface(ctx, l, false); })))
                 break;
             Level& L = ctx->levels[l];
-            if (L.ib_concurrent && L.n_vertices > 0) {
+            // a level's odd-numbered sub-steps follow its transfer (one after every second step);
+            // the even-numbered ones follow its own step only and run their immersed-boundary
+            // pass in line on the level's stream, where the launches overlap one another
+            const bool after_transfer = l > 0 && count[l] % 2 == 1;
+            if (L.ib_concurrent && L.n_vertices > 0 && after_transfer) {
                 // the immersed-boundary pass on its own stream after the level's last step only,
                 // beside the level's transfer; the step waits for both
                 const cudaStream_t s = ctx->ibstream[l];
@@ -1803,7 +1807,7 @@ int zl_ib_set_vertices(zl_ctx* ctx, int level, int64_t n, const double* coordina
         (rc = alloc(ctx, L.ib_total, 3 * 8)))
         return rc;
     const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
-    if (!L.ib_vel.ptr && (rc = alloc(ctx, L.ib_vel, (size_t)cells * 3 * 8))) return rc;
+    if (L.ib_vel.bytes != (size_t)cells * 3 * 8 && (rc = alloc(ctx, L.ib_vel, (size_t)cells * 3 * 8))) return rc;
     if (n > 0) {
         ZL_CUDA(ctx, cudaMemcpy(L.ib_coord.ptr, coordinates, (size_t)n * 3 * 8, cudaMemcpyHostToDevice));
         ZL_CUDA(ctx, cudaMemcpy(L.ib_uvel.ptr, velocity, (size_t)n * 3 * 8, cudaMemcpyHostToDevice));
