@@ -69,7 +69,7 @@ struct Level {
     // body forces and immersed boundary
     DeviceBuffer force;      // node forces, 3 doubles per cell
     DeviceBuffer mrt64_d;    // M^-1 (I - S/2) M (FP64 forced MRT)
-    DeviceBuffer ib_vel;     // node velocities of the forcing pass, 3 doubles per cell
+    DeviceBuffer ib_vel;     // node velocities of the forcing pass: x, y, z arrays over the box cells
     DeviceBuffer ib_coord, ib_uvel, ib_area, ib_force, ib_total;
     DeviceBuffer ib_nodes;   // every cell a vertex stencil touches, once
     // the stencils resolved when the vertices are set: per (vertex, stencil node) pair its cell and
@@ -1587,14 +1587,17 @@ static int ib_pass(zl_ctx* ctx, Level& L, int level) {
     const double* csh = (const double*)L.ib_csr_share.ptr;
     // dependent launches: each kernel's launch overlaps the tail of the one before it
     const double* vel = (const double*)L.ib_vel.ptr;
+    const long long cells = (long long)L.geo.a[0] * L.geo.a[1] * L.geo.a[2];
     const int* nodes = (const int*)L.ib_nodes.ptr;
     double* nf = (double*)L.force.ptr;
     if (ctx->dims == 2) {
-        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<2>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel));
+        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<2>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel,
+                                      cells));
         ZL_CUDA(ctx, launch_dependent(ib_spread_kernel<2>, dim3(nblocks), dim3(128), 0, ctx->stream, v, nodes,
                                       L.n_ib_nodes, cs, cv, csh, nf));
     } else {
-        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<3>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel));
+        ZL_CUDA(ctx, launch_dependent(ib_force_kernel<3>, dim3(blocks), dim3(threads), 0, ctx->stream, v, pc, pw, vel,
+                                      cells));
         ZL_CUDA(ctx, launch_dependent(ib_spread_kernel<3>, dim3(nblocks), dim3(128), 0, ctx->stream, v, nodes,
                                       L.n_ib_nodes, cs, cv, csh, nf));
     }

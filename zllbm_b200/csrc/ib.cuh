@@ -150,7 +150,10 @@ static __global__ void ib_release_kernel(const int* __restrict__ nodes, int n_no
     for (int a = 0; a < 3; ++a) node_force[cell * 3 + a] = 0.;
 }
 
-// Launch 1: the velocity of every stencil node (launch 3 then writes every stencil node's force).
+// Launch 1: the velocity of every stencil node (launch 3 then writes every stencil node's force),
+// one array per component over the level's box cells (node_vel[a cells + cell]): a vertex's
+// stencil rows are runs of consecutive cells, so the interpolation's loads of one component
+// fall into few sectors.
 template <class L, class S>
 __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepParams p, int even_layout,
                                 const int* __restrict__ nodes, int n_nodes, double* __restrict__ node_vel) {
@@ -197,7 +200,8 @@ __global__ void ib_touch_kernel(const S* __restrict__ f, LevelGeom geo, StepPara
         u[1] = uy / rho;
         u[2] = D == 3 ? uz / rho : 0.;
     }
-    for (int a = 0; a < 3; ++a) node_vel[cell * 3 + a] = u[a];
+    const long long cells = (long long)geo.a[0] * geo.a[1] * geo.a[2];
+    for (int a = 0; a < 3; ++a) node_vel[a * cells + cell] = u[a];
 }
 
 // Every (vertex i, stencil node k) pair, k over width^D nodes x fastest: the node's cell, its
@@ -233,7 +237,8 @@ constexpr int kIbForceThreads = 128;
 template <int D>
 __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v, const int* __restrict__ pair_cell,
                                                                    const double* __restrict__ pair_w,
-                                                                   const double* __restrict__ node_vel) {
+                                                                   const double* __restrict__ node_vel,
+                                                                   long long cells) {
     pdl_wait();
     pdl_trigger();
     constexpr int G = kIbForceLanes;
@@ -256,7 +261,7 @@ __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v,
 #pragma unroll
             for (int e = 0; e < 4; ++e)
 #pragma unroll
-                for (int b = 0; b < D; ++b) a[e][b] = node_vel[c[e] * 3 + b];
+                for (int b = 0; b < D; ++b) a[e][b] = node_vel[b * cells + c[e]];
 #pragma unroll
             for (int b = 0; b < D; ++b) u[b] = u[b] + a[0][b] * d[0] + a[1][b] * d[1];
 #pragma unroll
@@ -268,8 +273,8 @@ __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v,
             double a0[3], a1[3];
 #pragma unroll
             for (int a = 0; a < D; ++a) {
-                a0[a] = node_vel[c0 * 3 + a];
-                a1[a] = node_vel[c1 * 3 + a];
+                a0[a] = node_vel[a * cells + c0];
+                a1[a] = node_vel[a * cells + c1];
             }
 #pragma unroll
             for (int a = 0; a < D; ++a) u[a] = u[a] + a0[a] * d0 + a1[a] * d1;
@@ -278,7 +283,7 @@ __global__ void __launch_bounds__(kIbForceThreads) ib_force_kernel(IbVertices v,
             const long long c = __ldg(pair_cell + base + k);
             const double d = __ldg(pair_w + base + k);
 #pragma unroll
-            for (int a = 0; a < D; ++a) u[a] += node_vel[c * 3 + a] * d;
+            for (int a = 0; a < D; ++a) u[a] += node_vel[a * cells + c] * d;
         }
     }
 #pragma unroll
