@@ -78,7 +78,9 @@ struct LevelGeom {
     // D3Q19 step launches: planes [z0, z0 + zn) of the last axis; zn = 0: every plane
     int z0, zn;
     // one-node step launches: 1 = threads numbered over each x-y plane (x fastest) instead of per
-    // row, so that rows whose length is not a multiple of 32 share warps; fn0 divides by n[0]
+    // row, so that rows whose length is not a multiple of 32 share warps; fn0 divides by n[0].
+    // 2 = the same with each plane's row-inner nodes (x = 1 .. n[0] - 2) first and the rows' end
+    // nodes (x = 0, n[0] - 1) last; fn0 divides by n[0] - 2
     int flat;
     FastDiv fn0;
 };
@@ -1267,7 +1269,20 @@ __global__ void __launch_bounds__(256, (StepOccupancy<S, Odd, Bnd, Masked, Ext>:
     pdl_wait();
     pdl_trigger();
     Coord c;
-    if (geo.flat) {
+    if (geo.flat == 2) {
+        // the rows' inner nodes first (fn0 divides by n0 - 2), then their two end nodes
+        const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, ni = (uint32_t)geo.n[0] - 2u,
+                       inner = ni * (uint32_t)geo.n[1];
+        if (t < inner) {
+            const uint32_t y = geo.fn0.div(t);
+            c.x[0] = 1 + (int)(t - y * ni);
+            c.x[1] = (int)y;
+        } else {
+            const uint32_t k = t - inner;
+            c.x[0] = (k & 1u) ? geo.n[0] - 1 : 0;
+            c.x[1] = (int)(k >> 1);
+        }
+    } else if (geo.flat) {
         const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x, y = geo.fn0.div(t);
         c.x[0] = (int)(t - y * (uint32_t)geo.n[0]);
         c.x[1] = (int)y;
