@@ -105,7 +105,10 @@ typedef struct zl_config {
                                   (SetDefaultVelocity, lbm_interface.h:300) */
     double storage_scale;      /* scale of FP16/BF16 deviations (0 selects the default 2^13) */
     int forcing;               /* 1: collide with Guo forcing and per-node forces (SetNumForces /
-                                  SetConstantForce, lbm_interface.h:298-319); needed by immersed boundaries */
+                                  SetConstantForce, lbm_interface.h:298-319); needed by immersed boundaries.
+                                  FP64 storage collides every node with the forcing terms, as the
+                                  reference does; FP32/FP16/BF16 levels whose forces are all zero (no
+                                  constant force, no vertex set so far) take the unforced update */
     double constant_force[3];  /* SetConstantForce */
     int les;                   /* ZL_LES_SMAGORINSKY: tau = tau0 + tau_sgs (the reference sets tau = tau_sgs,
                                   lbm_solver_interface.cpp:291-295, which this library treats as a bug);
